@@ -1,0 +1,424 @@
+#!/usr/bin/env python3
+"""Benchmark of the GMRES-IR hot path on the B200.
+
+Workload (one "step" = one drop-in solve of a new value set on an analysed
+pattern): the 3-D KKT system K = [[H, A^T], [A, -1e-6 I]] with H the 7-point
+Laplacian on 48^3 + 1e-2 I and A 27,648 x 110,592 with 6 N(0,1) entries per
+row (n = 138,240), seeded synthetic data.  Each step runs the float32
+supernodal LDL^T factorization of the scaled, permuted matrix and a float64
+GMRES-IR solve of one right-hand side to normwise backward error <= 1e-14;
+every step's backward error is checked.
+
+  value   solves/s with the values and right-hand side already in HBM
+  e2e     the same through the reference-facing C ABI with host buffers:
+          per step the values and b go host->device and x comes back
+  roofline  the dominant kernel class (CUDA events around its launches in a
+          separate profiling pass), against MEASURED_PEAKS.json
+  cpu_baseline  the reference's own CPU code (oracle/_ref) timed on bounded
+          samples on this host and extrapolated to one full solve
+
+--impl reference runs only the reference's CPU path (rank 0; other ranks
+exit 0) and prints its line.  Multi-GPU: independent replicas, one system per
+rank, no collective on the data path ("scaling": "weak").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "solves/s + p50/p99 latency @ bwd err≤1e-14: served mixed vs drop-in, 1 B200"
+UNIT = "solves/s"
+BE_TOL = 1e-14
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="mpir", choices=["mpir", "reference"])
+    ap.add_argument("--grid", type=int, default=48)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--cpu-budget", type=float, default=12.0,
+                    help="seconds of reference factor sampling for the CPU baseline")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload_name(grid):
+    n1 = grid ** 3
+    return (f"grid3d-{grid}: KKT n={n1 + n1 // 4} (7-point Laplacian {grid}^3 + 1e-2 I, "
+            f"{n1 // 4} constraint rows x 6 N(0,1), delta 1e-6); per step f32 LDL^T "
+            f"refactorization + f64 GMRES-IR solve, 1 RHS")
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}", "--format=csv,noheader",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1].split()[0]))
+                mx = float(f[2].split()[0])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------
+# CPU path of the reference (oracle/_ref), bounded samples.
+
+def reference_cpu_estimate(s, perm, counts, budget, log=print):
+    """Seconds for one drop-in solve by the reference's CPU code on P K P^T.
+
+    * factor: QDLDL_factor<float> (the reference's code) timed on the leading
+      k x k block of the scaled, permuted matrix, k chosen so the sample takes
+      about `budget` seconds; the up-looking factor computes row r from rows
+      < r only, so the sample is exactly the first k rows of the full factor.
+      Its rate (multiply-subtract updates per second, counted row by row by
+      the oracle's walk of the same tree) extrapolates to all n rows.
+    * solve: the reference's QDLDL_solve on the sampled factor gives seconds
+      per factor entry; one GMRES-IR solve applies it counts['applies'] times
+      to nnz(L) entries, plus counts['spmv'] MatrixMultiply at full size.
+    """
+    import oracle
+
+    R = oracle.Reference()
+    O = oracle.Oracle()
+    Cp, Ci, Cx = oracle.permuted_scaled_upper(O, s.n, s.Ap, s.Ai, s.Ax, perm)
+    n = s.n
+    w = O.row_work(n, Cp, Ci)
+    W = np.cumsum(w)
+    total_work = float(W[-1])
+    _, Lnz, _ = O.etree(n, Cp, Ci)
+    nnzL = float(Lnz.sum())
+    # rate guess from a cheap leading block, then the budgeted sample
+    k = int(np.searchsorted(W, min(2e8, total_work)))
+    k = max(min(k, n), 16)
+    t0 = time.perf_counter()
+    R.factor(k, Cp, Ci, Cx)
+    t = time.perf_counter() - t0
+    rate = max(W[k - 1], 1.0) / max(t, 1e-6)
+    target = rate * budget
+    k = int(np.searchsorted(W, min(target, total_work)))
+    k = max(min(k, n), 16)
+    t0 = time.perf_counter()
+    st, Lp, Li, Lx, D, Dinv = R.factor(k, Cp, Ci, Cx)
+    t_fac = time.perf_counter() - t0
+    work_k = float(W[k - 1])
+    rate = work_k / max(t_fac, 1e-9)
+    t_factor_full = total_work / rate
+    # solve rate on the sampled factor
+    nnz_k = float(Lp[k])
+    rhs = np.ones(k)
+    t0 = time.perf_counter()
+    reps = 0
+    while True:
+        R.solve(k, Lp, Li, Lx, Dinv, rhs)
+        reps += 1
+        if time.perf_counter() - t0 > 1.0 or reps >= 50:
+            break
+    t_solve_k = (time.perf_counter() - t0) / reps
+    per_entry = t_solve_k / max(2 * nnz_k + k, 1.0)
+    t_apply = per_entry * (2 * nnzL + n)
+    x = np.ones(n)
+    t0 = time.perf_counter()
+    R.matmul(n, s.Ap, s.Ai, s.Ax, x)
+    t_spmv = time.perf_counter() - t0
+    total = t_factor_full + counts["applies"] * t_apply + counts["spmv"] * t_spmv
+    log(f"cpu sample: k={k}/{n} rows, {t_fac:.2f}s for {work_k:.3e} updates "
+        f"({rate:.3e}/s); full factor {t_factor_full:.1f}s; apply {t_apply:.3f}s; "
+        f"spmv {t_spmv:.4f}s; solve total {total:.1f}s")
+    return total, {"k": k, "factor_sample_s": t_fac, "rate_updates_per_s": rate,
+                   "factor_full_s_extrapolated": t_factor_full, "apply_s": t_apply,
+                   "spmv_s": t_spmv, "work_total": total_work, "nnzL": nnzL}
+
+
+def reference_counts(grid, seed):
+    """Preconditioner applications and SpMVs per solve of the reference's
+    GMRES-IR, measured with its restated driver (bit-exact with the
+    reference) on a smaller system from the same generator."""
+    import oracle
+    from mpir_b200 import kkt
+    s = kkt.grid3d(seed=seed, grid=min(grid, 12))
+    x, st = oracle.Oracle().gmres_ir(s.n, s.Ap, s.Ai, s.Ax, s.b, form=0)
+    return {"applies": st["precond_applies"], "spmv": st["spmv"],
+            "ir_steps": st["ir_steps"], "sample_n": s.n}
+
+
+# ----------------------------------------------------------------------------
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from mpir_b200 import kkt
+    import mpir_b200 as mp
+    s = kkt.grid3d(seed=args.seed, grid=args.grid)
+    perm = mp.analyze_host(s.Ap, s.Ai, s.Ax)["perm"]
+    counts = reference_counts(args.grid, args.seed)
+    lat = []
+    for i in range(args.warmup + args.steps):
+        t, det = reference_cpu_estimate(s, perm, counts, args.cpu_budget, log=lambda *_: None)
+        if i >= args.warmup:
+            lat.append(t)
+    value = 1.0 / float(np.mean(lat))
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * float(np.mean(lat)), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 factor / f64 solve", "data": "synthetic",
+        "config": {"workload": workload_name(args.grid), "global_batch": 1},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                         "sample": "QDLDL_factor<float> on a leading block (~%.0fs) + "
+                                   "QDLDL_solve + MatrixMultiply, extrapolated to one "
+                                   "full GMRES-IR solve" % args.cpu_budget,
+                         "detail": det},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "latency_ms": {"p50": 1e3 * float(np.percentile(lat, 50)),
+                       "p99": 1e3 * float(np.percentile(lat, 99))},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_gpu(args):
+    import torch
+
+    import mpir_b200 as mp
+    from mpir_b200 import kkt
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    dev = torch.device("cuda", local)
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+
+    def max_over_ranks(v):
+        if pg is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    s = kkt.grid3d(seed=args.seed + rank, grid=args.grid)
+    solver = mp.GmresLDLIR(device=local)
+    stream = torch.cuda.current_stream(dev)
+    solver.set_stream(stream.cuda_stream)
+    solver.analyze(s.Ap, s.Ai, s.Ax)
+    info = solver.info()
+    d_Ax = torch.from_numpy(s.Ax).to(dev)
+    d_b = torch.from_numpy(s.b).to(dev)
+    d_x = torch.empty_like(d_b)
+    L = mp.lib()
+
+    def step():
+        assert solver.factor_device(d_Ax.data_ptr()) == 0
+        return solver.solve_device(d_b.data_ptr(), d_x.data_ptr())
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    # ---- device-resident timing
+    barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    time.sleep(0.3)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    t_all0, t_all1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = mp.launch_count()
+    reps = []
+    t_all0.record(stream)
+    for i in range(args.steps):
+        evs[i][0].record(stream)
+        reps.append(step())
+        evs[i][1].record(stream)
+    t_all1.record(stream)
+    torch.cuda.synchronize()
+    launches = mp.launch_count() - launches0
+    clk = clocks.stop()
+    barrier()
+    lat = [a.elapsed_time(b) for a, b in evs]
+    total_ms = max_over_ranks(t_all0.elapsed_time(t_all1))
+    value = world * args.steps / (total_ms / 1e3)
+    be = max(r["backward_error"] for r in reps)
+    assert be <= BE_TOL, f"backward error {be} above {BE_TOL}"
+
+    # ---- end to end through the C ABI with host buffers
+    h_Ax = torch.from_numpy(s.Ax).pin_memory()
+    h_b = torch.from_numpy(s.b).pin_memory()
+    h_x = torch.empty(s.n, dtype=torch.float64).pin_memory()
+    rep = mp.Report()
+
+    def step_e2e():
+        r = L.mpir_solver_factor(solver._h, h_Ax.data_ptr())
+        assert r == 0, mp.last_error()
+        r = L.mpir_solver_solve(solver._h, h_b.data_ptr(), h_x.data_ptr(), mp.C.byref(rep))
+        assert r == 0, mp.last_error()
+        return rep.backward_error
+
+    step_e2e()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    be_e2e = 0.0
+    for _ in range(args.steps):
+        be_e2e = max(be_e2e, step_e2e())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+    assert be_e2e <= BE_TOL
+    e2e_value = world * args.steps / (e2e_ms / 1e3)
+    h2d = s.Ax.nbytes + s.b.nbytes
+    d2h = s.n * 8
+
+    # ---- roofline: per-class device time in one profiled step
+    mp.kernel_timer(True)
+    step()
+    torch.cuda.synchronize()
+    kt = mp.kernel_times()
+    mp.kernel_timer(False)
+    hbm, bf16, peak_kind = load_peaks()
+    cls_ms = {k: v[0] for k, v in kt.items()}
+    dom = max(cls_ms, key=cls_ms.get)
+    rep0 = reps[-1]
+    applies = rep0["precond_applies"]
+    work = {
+        "trailing_update": ("tensor", info["update_flops"] / 1e12, "TFLOP/s", bf16),
+        "panel_solve": ("tensor", info["trsm_flops"] / 1e12, "TFLOP/s", bf16),
+        "solve_forward": ("hbm", applies * info["panel_read_bytes"] / 1e9, "GB/s", hbm),
+        "solve_backward": ("hbm", applies * info["panel_read_bytes"] / 1e9, "GB/s", hbm),
+    }
+    bound, amount, unit, peak = work.get(dom, ("hbm", float("nan"), "GB/s", hbm))
+    dom_s = cls_ms[dom] / 1e3
+    achieved = amount / dom_s if dom_s > 0 else float("nan")
+    roofline = {"bound": bound, "kernel": dom, "achieved": achieved, "peak": peak,
+                "unit": unit, "frac": achieved / peak, "peak_source": peak_kind,
+                "traffic": None,
+                "class_ms": {k: round(v, 3) for k, v in cls_ms.items() if v > 0},
+                "class_launches": {k: v[1] for k, v in kt.items() if v[1] > 0}}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 factor / f64 solve",
+        "data": "synthetic (seeded KKT generator, one system per rank)",
+        "config": {"workload": workload_name(args.grid), "global_batch": world,
+                   "seq_len": None, "parallelism": f"replicas{world}",
+                   "l2": "inputs larger than L2 (factor panels %.1f GB)" % (info["panel_bytes"] / 1e9)},
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+        "backward_error_max": be,
+        "iterations": {"ir": rep0["ir_iterations"], "gmres": rep0["gmres_iterations"],
+                       "precond_applies": applies},
+        "factor_ms": rep0["factor_ms"], "solve_ms": rep0["solve_ms"],
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "clocks": clk,
+        "roofline": roofline,
+        "info": {k: info[k] for k in ("n", "nnz_L", "supernodes", "levels", "max_front")},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            counts = {"applies": applies, "spmv": rep0["spmv_count"]}
+            perm = solver.symbolic()["perm"]
+            t, det = reference_cpu_estimate(s, perm, counts, args.cpu_budget,
+                                            log=lambda *a: print(*a, file=sys.stderr))
+            line["cpu_baseline"] = {
+                "value": 1.0 / t, "unit": UNIT, "cores": 1, "kind": "reference",
+                "sample": "reference QDLDL_factor<float> on the leading %d of %d rows of the "
+                          "scaled permuted matrix (%.1fs), QDLDL_solve on that factor, full "
+                          "MatrixMultiply; extrapolated to one solve with %d preconditioner "
+                          "applications" % (det["k"], s.n, det["factor_sample_s"], applies),
+                "detail": det}
+        except Exception as e:  # the baseline never blocks the GPU line
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 1,
+                                    "kind": "reference", "sample": f"failed: {e}"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

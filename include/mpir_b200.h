@@ -1,0 +1,210 @@
+/* mpir_b200 C ABI: GMRES-IR for sparse quasidefinite systems preconditioned
+ * by a supernodal LDL^T factor, on one NVIDIA B200 (sm_100a).
+ *
+ * The entry points replace the CPU hot path of the reference library (MPIR,
+ * header-only C++): QDLDL_etree / QDLDL_factor / QDLDL_solve in
+ * include/MPIR/qdldl.hpp and the GmresLDLIR<UF,UW,UR> solver in
+ * include/MPIR/gmres_ir.hpp.  The C++ headers include/MPIR/qdldl.hpp and
+ * include/MPIR/gmres_ir.hpp of this project keep the reference's template
+ * signatures and forward to these functions.
+ *
+ * Conventions: plain host pointers and sizes; all matrices are the upper
+ * triangle of a symmetric matrix in CSC with int64 column pointers and row
+ * indices, no duplicates.  Status codes are 0 on success and negative on
+ * failure; mpir_last_error() returns the calling thread's last message.
+ */
+#ifndef MPIR_B200_H
+#define MPIR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  -1 and -2 mean what they mean for QDLDL_etree /
+ * QDLDL_factor (qdldl.hpp:43-45, :135-138). */
+enum {
+  MPIR_OK              = 0,
+  MPIR_ERR_INPUT       = -1, /* not upper triangular, empty column, zero pivot */
+  MPIR_ERR_OVERFLOW    = -2, /* nonzero count of L overflows */
+  MPIR_ERR_CUDA        = -3, /* CUDA runtime error (message has details) */
+  MPIR_ERR_NOMEM       = -4, /* device or host allocation failed */
+  MPIR_ERR_TIMEOUT     = -5, /* a bounded device wait ran out */
+  MPIR_ERR_ARGUMENT    = -6, /* invalid argument */
+  MPIR_ERR_UNSUPPORTED = -7, /* precision combination not provided */
+  MPIR_ERR_STATE       = -8  /* call out of order (solve before factor, ...) */
+};
+
+/* Floating-point types of the factor (UF), working (UW) and residual (UR)
+ * precisions, as the reference's template parameters. */
+enum {
+  MPIR_F64  = 0,
+  MPIR_F32  = 1,
+  MPIR_BF16 = 2,
+  MPIR_F16  = 3,
+  MPIR_DD   = 4 /* double-double, the reference's dd_real residual type */
+};
+
+/* Orderings for mpir_solver_analyze. */
+enum { MPIR_ORDER_NATURAL = 0, MPIR_ORDER_AUTO = 1 };
+
+/* Outcome of one GMRES-IR solve. */
+typedef struct mpir_report {
+  int32_t status;
+  int32_t ir_iterations;    /* refinement steps (gmres_ir.hpp:561) */
+  int32_t gmres_iterations; /* inner Arnoldi steps over all PrecondGmres calls */
+  int32_t precond_applies;  /* L D L^T solves */
+  int32_t spmv_count;       /* products with K */
+  int32_t reorth_count;     /* Brown/Hindmarsh re-orthogonalisations */
+  int32_t stop_reason;      /* 0 iteration cap, 1 small update, 2 stagnation,
+                               3 zero residual */
+  int32_t pad;
+  double residual_norm;  /* ||r||_inf / ||b_scaled||_inf at exit (gmres_ir.hpp:580) */
+  double backward_error; /* ||b - Kx||_inf / (||K||_inf ||x||_inf + ||b||_inf) */
+  double factor_ms;      /* device time of the last numeric factorization */
+  double solve_ms;       /* device time of this solve */
+} mpir_report;
+
+/* Facts about an analysed pattern. */
+typedef struct mpir_info {
+  int64_t n, nnz_upper, nnz_L;   /* nnz_L = sum of QDLDL_etree's Lnz */
+  int64_t supernodes, levels;
+  int64_t panel_bytes;           /* factor storage */
+  int64_t update_bytes;          /* update-matrix arena */
+  int64_t max_front;             /* largest front height */
+  double  factor_flops;          /* sum_j Lnz_j^2: multiply-adds x 2 of the
+                                    exact elimination */
+  double  solve_bytes;           /* bytes one L D L^T solve must move: float32
+                                    L twice, Dinv, four float64 vectors */
+  double  update_flops;          /* flops of the trailing-update launches */
+  double  trsm_flops;            /* flops of the panel-solve launches */
+  double  panel_read_bytes;      /* panel bytes one forward (or backward)
+                                    sweep reads, padding included */
+} mpir_info;
+
+typedef struct mpir_solver_s *mpir_solver;
+
+int         mpir_version(void);
+const char *mpir_last_error(void);
+int         mpir_device_count(int *count);
+
+/* ---- QDLDL drop-in ------------------------------------------------------ */
+
+/* Replaces QDLDL_etree (include/MPIR/qdldl.hpp:48-105).  Host computation;
+ * Lnz and etree are equal element for element to the reference's.  `work`
+ * (n entries) is scratch, as in the reference.  Returns sum(Lnz), -1 or -2. */
+int64_t mpir_qdldl_etree(int64_t n, const int64_t *Ap, const int64_t *Ai,
+                         int64_t *work, int64_t *Lnz, int64_t *etree);
+
+/* Replaces QDLDL_factor (include/MPIR/qdldl.hpp:172-345) in natural order on
+ * device `device`.  Ax is float64 (the caller's values); the factor is
+ * computed in float32 and written to the caller's arrays (Lp: n+1, Li/Lx:
+ * sum(Lnz), D/Dinv: n) in fact_prec (MPIR_F32, or MPIR_BF16 / MPIR_F16 as
+ * raw 16-bit patterns rounded from float32).  Lnz and etree must be
+ * QDLDL_etree's output.  Li comes out in QDLDL's order (rows ascending in each
+ * column).  Returns the number of positive entries of D, or -1 on a zero
+ * pivot, or another negative status. */
+int64_t mpir_qdldl_factor(int64_t n, const int64_t *Ap, const int64_t *Ai,
+                          const double *Ax, int64_t *Lp, int64_t *Li, void *Lx,
+                          void *D, void *Dinv, int fact_prec,
+                          const int64_t *Lnz, const int64_t *etree, int device);
+
+/* Replaces QDLDL_solve (include/MPIR/qdldl.hpp:417-432): x <- (L D L^T)^{-1} x
+ * on device `device`, with L (CSC, strictly lower, rows ascending) and Dinv
+ * in fact_prec (MPIR_F32 / MPIR_BF16 / MPIR_F16) and x in x_prec (MPIR_F64 or
+ * MPIR_F32).  Accumulates in float64.  Returns a status. */
+int mpir_qdldl_solve(int64_t n, const int64_t *Lp, const int64_t *Li,
+                     const void *Lx, const void *Dinv, int fact_prec, void *x,
+                     int x_prec, int device);
+
+/* Replace QDLDL_Lsolve (qdldl.hpp:362-372, x <- (L+I)^{-1} x) and
+ * QDLDL_Ltsolve (qdldl.hpp:389-400, x <- (L+I)^{-T} x); arguments as
+ * mpir_qdldl_solve without Dinv. */
+int mpir_qdldl_lsolve(int64_t n, const int64_t *Lp, const int64_t *Li,
+                      const void *Lx, int fact_prec, void *x, int x_prec,
+                      int device);
+int mpir_qdldl_ltsolve(int64_t n, const int64_t *Lp, const int64_t *Li,
+                       const void *Lx, int fact_prec, void *x, int x_prec,
+                       int device);
+
+/* ---- GMRES-IR solver (replaces GmresLDLIR, gmres_ir.hpp:90-315) --------- */
+
+/* uf/uw/ur as MPIR_F* above.  Provided: uf = MPIR_F32, uw = MPIR_F64,
+ * ur = MPIR_F64 or MPIR_DD. */
+int mpir_solver_create(mpir_solver *out, int uf, int uw, int ur, int device);
+int mpir_solver_destroy(mpir_solver s);
+
+/* Setters of gmres_ir.hpp:291-303 (defaults 10, 10, 1e-10). */
+int mpir_solver_set_max_ir_iterations(mpir_solver s, int64_t n);
+int mpir_solver_set_max_gmres_iterations(mpir_solver s, int64_t n);
+int mpir_solver_set_tolerance(mpir_solver s, double tol);
+
+/* Compute (gmres_ir.hpp:271-278, 323-532): analyse with MPIR_ORDER_AUTO and
+ * factor.  The reference's FGPILU ILU_k pattern level has no meaning for the
+ * complete LDL^T factor and is not an argument. */
+int mpir_solver_compute(mpir_solver s, int64_t n, const int64_t *Ap,
+                        const int64_t *Ai, const double *Ax);
+/* Symbolic analysis only.  Ax (may be NULL) only supplies the signs of the
+ * diagonal, which split the ordering into the positive and the other block. */
+int mpir_solver_analyze(mpir_solver s, int64_t n, const int64_t *Ap,
+                        const int64_t *Ai, const double *Ax, int ordering);
+/* New values on the analysed pattern (host / device pointer). */
+int mpir_solver_factor(mpir_solver s, const double *Ax);
+int mpir_solver_factor_device(mpir_solver s, const double *d_Ax);
+
+/* Solve (gmres_ir.hpp:536-634): host / device vectors in the caller's
+ * order.  rep may be NULL. */
+int mpir_solver_solve(mpir_solver s, const double *b, double *x,
+                      mpir_report *rep);
+int mpir_solver_solve_device(mpir_solver s, const double *d_b, double *d_x,
+                             mpir_report *rep);
+
+/* Launch the solver's work on a caller stream (a cudaStream_t; NULL
+ * restores the solver's own stream). */
+int mpir_solver_set_stream(mpir_solver s, void *stream);
+int mpir_solver_info(mpir_solver s, mpir_info *info);
+
+/* Permutation (perm[new] = old) and the elimination tree / column counts of
+ * the permuted matrix, each n entries; Cp (n+1), Ci and Csrc (nnz_upper)
+ * describe the permuted upper CSC and the source index of each entry.  Any
+ * pointer may be NULL. */
+int mpir_solver_symbolic(mpir_solver s, int64_t *perm, int64_t *etree,
+                         int64_t *Lnz, int64_t *Cp, int64_t *Ci, int64_t *Csrc);
+
+/* Supernode partition of the analysed pattern: sfirst (supernodes+1) column
+ * ranges, srowptr (supernodes+1) and srows (srowptr[last]) the row index set
+ * of each supernode (its own columns, then the rows below, ascending).  Any
+ * pointer may be NULL; *nrows receives srowptr[last]. */
+int mpir_solver_supernodes(mpir_solver s, int64_t *sfirst, int64_t *srowptr,
+                           int32_t *srows, int64_t *nrows);
+
+/* Factor in QDLDL's CSC form for the permuted matrix (Lp: n+1, Li/Lx: nnz_L,
+ * D/Dinv: n, float32). */
+int mpir_solver_export_factor(mpir_solver s, int64_t *Lp, int64_t *Li,
+                              float *Lx, float *D, float *Dinv);
+
+/* Host-only symbolic analysis (no device needed): the permutation, the
+ * elimination tree and column counts of P K P^T, its upper CSC (Cp: n+1, Ci:
+ * nnz_upper) and the exact pattern of L in QDLDL's CSC form (Lp: n+1, Li:
+ * nnz_L; pass Li = NULL to size it first from info->nnz_L).  Any output may
+ * be NULL.  Returns a status (-1 / -2 as QDLDL_etree). */
+int mpir_analyze_host(int64_t n, const int64_t *Ap, const int64_t *Ai,
+                      const double *Ax, int ordering, int64_t *perm,
+                      int64_t *etree, int64_t *Lnz, int64_t *Cp, int64_t *Ci,
+                      int64_t *Lp, int64_t *Li, mpir_info *info);
+
+/* ---- Kernel timing (benchmark support) ----------------------------------- */
+/* Classes: 0 small fronts, 1 diagonal blocks, 2 panel solve, 3 trailing
+ * update, 4 extend-add, 5 zero fill, 6 scatter, 7 forward solve, 8 backward
+ * solve, 9 SpMV, 10 vector. */
+int mpir_kernel_timer_enable(int on);
+/* Kernel launches this library has issued in this process. */
+int64_t mpir_launch_count(void);
+int mpir_kernel_timer_collect(double *ms, int64_t *launches, int nclass);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

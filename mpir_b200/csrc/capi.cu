@@ -1,0 +1,600 @@
+// C ABI (include/mpir_b200.h).  Every entry point converts exceptions into
+// status codes and keeps the message for mpir_last_error().
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/mpir_b200.h"
+#include "solver.hpp"
+
+namespace mpir {
+
+struct StatusError : std::runtime_error {
+  int code;
+  StatusError(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+static thread_local std::string g_err;
+
+template <class F>
+static auto guard(F &&f) -> decltype(f()) {
+  try {
+    g_err.clear();
+    return f();
+  } catch (const StatusError &e) {
+    g_err = e.what();
+    return e.code;
+  } catch (const CudaError &e) {
+    g_err = e.what();
+    return e.code == cudaErrorMemoryAllocation ? MPIR_ERR_NOMEM : MPIR_ERR_CUDA;
+  } catch (const std::bad_alloc &) {
+    g_err = "host allocation failed";
+    return MPIR_ERR_NOMEM;
+  } catch (const std::invalid_argument &e) {
+    g_err = e.what();
+    return MPIR_ERR_ARGUMENT;
+  } catch (const std::logic_error &e) {
+    g_err = e.what();
+    return MPIR_ERR_STATE;
+  } catch (const std::exception &e) {
+    g_err = e.what();
+    return MPIR_ERR_CUDA;
+  }
+}
+
+// Row-by-row etree reach (the symbolic half of qdldl.hpp:228-326): row k of
+// L holds the tree paths from each i with A(i,k) != 0 up to k.  Appending k
+// to each visited column gives QDLDL's Li order (rows ascending).
+static void exact_pattern(const Symbolic &S, std::vector<int64_t> &Lp,
+                          std::vector<int64_t> &Li) {
+  const int64_t n = S.n;
+  Lp.assign(n + 1, 0);
+  for (int64_t j = 0; j < n; j++) Lp[j + 1] = Lp[j] + S.Lnz[j];
+  Li.resize(Lp[n]);
+  std::vector<int64_t> next(Lp.begin(), Lp.end() - 1), mark(n, -1);
+  for (int64_t k = 0; k < n; k++) {
+    mark[k] = k;
+    for (int64_t p = S.Cp[k]; p < S.Cp[k + 1]; p++)
+      for (int64_t i = S.Ci[p]; mark[i] != k; i = S.etree[i]) {
+        Li[next[i]++] = k;
+        mark[i]       = k;
+      }
+  }
+}
+
+// Local row of global row r in supernode J's index set.
+static int64_t local_row(const Symbolic &S, int64_t J, int64_t r) {
+  const int64_t f = S.sfirst[J], l = S.sfirst[J + 1], w = l - f;
+  if (r < l) return r - f;
+  const int32_t *b = S.srows.data() + S.srowptr[J] + w;
+  const int32_t *e = S.srows.data() + S.srowptr[J + 1];
+  const int32_t *it = std::lower_bound(b, e, static_cast<int32_t>(r));
+  if (it == e || *it != r) return -1;
+  return w + (it - b);
+}
+
+// Copy the factor out of the panels into QDLDL's CSC form.
+static void export_csc(const Plan &P, const Numeric &F, cudaStream_t s,
+                       std::vector<int64_t> &Lp, std::vector<int64_t> &Li,
+                       std::vector<float> &Lx, std::vector<float> &D,
+                       std::vector<float> &Dinv) {
+  const Symbolic    &S = P.S;
+  std::vector<float> pan(S.panel_elems);
+  D.resize(S.n);
+  Dinv.resize(S.n);
+  if (S.panel_elems)
+    MPIR_CUDA(cudaMemcpyAsync(pan.data(), F.panel.as<void>(), S.panel_elems * sizeof(float),
+                              cudaMemcpyDeviceToHost, s));
+  if (S.n) {
+    MPIR_CUDA(cudaMemcpyAsync(D.data(), F.D.as<void>(), S.n * sizeof(float),
+                              cudaMemcpyDeviceToHost, s));
+    MPIR_CUDA(cudaMemcpyAsync(Dinv.data(), F.Dinv.as<void>(), S.n * sizeof(float),
+                              cudaMemcpyDeviceToHost, s));
+  }
+  MPIR_CUDA(cudaStreamSynchronize(s));
+  exact_pattern(S, Lp, Li);
+  Lx.resize(Li.size());
+  for (int64_t J = 0; J < S.ns; J++) {
+    const int64_t f = S.sfirst[J], l = S.sfirst[J + 1], h = S.h(J);
+    for (int64_t j = f; j < l; j++)
+      for (int64_t p = Lp[j]; p < Lp[j + 1]; p++) {
+        const int64_t lr = local_row(S, J, Li[p]);
+        Lx[p] = lr < 0 ? 0.0f : pan[S.slofs[J] + (j - f) * h + lr];
+      }
+  }
+}
+
+__global__ void k_f32_to_16(int64_t n, const float *in, uint16_t *out, int bf) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (bf) {
+    const __nv_bfloat16 v = __float2bfloat16_rn(in[i]);
+    out[i]                = *reinterpret_cast<const uint16_t *>(&v);
+  } else {
+    const __half v = __float2half_rn(in[i]);
+    out[i]         = *reinterpret_cast<const uint16_t *>(&v);
+  }
+}
+
+__global__ void k_16_to_f32(int64_t n, const uint16_t *in, float *out, int bf) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint16_t b = in[i];
+  out[i] = bf ? __bfloat162float(*reinterpret_cast<const __nv_bfloat16 *>(&b))
+              : __half2float(*reinterpret_cast<const __half *>(&b));
+}
+
+// Round float32 host data to a 16-bit type through the device's conversions.
+static void to_16(const std::vector<float> &in, void *out, int prec, cudaStream_t s) {
+  const int64_t n = static_cast<int64_t>(in.size());
+  if (!n) return;
+  DeviceBuffer a(n * sizeof(float)), b(n * sizeof(uint16_t));
+  MPIR_CUDA(cudaMemcpyAsync(a.as<void>(), in.data(), n * sizeof(float), cudaMemcpyHostToDevice, s));
+  launch(k_f32_to_16, static_cast<unsigned>((n + 255) / 256), 256, 0, s, 
+      n, a.as<float>(), b.as<uint16_t>(), prec == kBF16);
+  MPIR_CUDA(cudaMemcpyAsync(out, b.as<void>(), n * sizeof(uint16_t), cudaMemcpyDeviceToHost, s));
+  MPIR_CUDA(cudaStreamSynchronize(s));
+}
+
+static void from_16(const void *in, int64_t n, int prec, std::vector<float> &out,
+                    cudaStream_t s) {
+  out.resize(n);
+  if (!n) return;
+  DeviceBuffer a(n * sizeof(uint16_t)), b(n * sizeof(float));
+  MPIR_CUDA(cudaMemcpyAsync(a.as<void>(), in, n * sizeof(uint16_t), cudaMemcpyHostToDevice, s));
+  launch(k_16_to_f32, static_cast<unsigned>((n + 255) / 256), 256, 0, s, 
+      n, a.as<uint16_t>(), b.as<float>(), prec == kBF16);
+  MPIR_CUDA(cudaMemcpyAsync(out.data(), b.as<void>(), n * sizeof(float), cudaMemcpyDeviceToHost, s));
+  MPIR_CUDA(cudaStreamSynchronize(s));
+}
+
+struct StreamGuard {
+  cudaStream_t s = nullptr;
+  explicit StreamGuard(int device) {
+    MPIR_CUDA(cudaSetDevice(device));
+    MPIR_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  }
+  ~StreamGuard() {
+    if (s) {
+      cudaStreamSynchronize(s);
+      cudaStreamDestroy(s);
+    }
+  }
+};
+
+void invert_diag_blocks(const Plan &P, Numeric &F, cudaStream_t s);
+
+}  // namespace mpir
+
+using namespace mpir;
+
+struct mpir_solver_s {
+  Solver *impl;
+};
+
+extern "C" {
+
+int mpir_version(void) { return 10000; }
+
+const char *mpir_last_error(void) { return g_err.c_str(); }
+
+int mpir_device_count(int *count) {
+  return guard([&]() -> int {
+    int c = 0;
+    MPIR_CUDA(cudaGetDeviceCount(&c));
+    if (count) *count = c;
+    return MPIR_OK;
+  });
+}
+
+int64_t mpir_qdldl_etree(int64_t n, const int64_t *Ap, const int64_t *Ai, int64_t *work,
+                         int64_t *Lnz, int64_t *etree) {
+  return guard([&]() -> int64_t {
+    if (n < 0 || (n > 0 && (!Ap || !Ai || !Lnz || !etree))) return MPIR_ERR_ARGUMENT;
+    for (int64_t i = 0; i < n; i++) {
+      if (work) work[i] = 0;
+      Lnz[i]   = 0;
+      etree[i] = -1;
+    }
+    return etree_counts(n, Ap, Ai, etree, Lnz);
+  });
+}
+
+int64_t mpir_qdldl_factor(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *Ax,
+                          int64_t *Lp, int64_t *Li, void *Lx, void *D, void *Dinv,
+                          int fact_prec, const int64_t *Lnz, const int64_t *etree,
+                          int device) {
+  return guard([&]() -> int64_t {
+    if (fact_prec != kF32 && fact_prec != kBF16 && fact_prec != kF16)
+      throw StatusError(MPIR_ERR_UNSUPPORTED, "factor type not provided (F32, BF16, F16)");
+    if (n < 0) return MPIR_ERR_ARGUMENT;
+    if (n == 0) {
+      if (Lp) Lp[0] = 0;
+      return 0;
+    }
+    Symbolic    S;
+    std::string err;
+    const int   rc = analyze(n, Ap, Ai, nullptr, Ordering::Natural, S, err);
+    if (rc != kOk) throw StatusError(rc, err);
+    for (int64_t j = 0; j < n; j++)
+      if ((Lnz && Lnz[j] != S.Lnz[j]) || (etree && etree[j] != S.etree[j]))
+        throw StatusError(MPIR_ERR_ARGUMENT, "Lnz / etree are not QDLDL_etree's output");
+    StreamGuard sg(device);
+    Plan        P;
+    P.build(std::move(S), sg.s);
+    Numeric F;
+    F.allocate(P);
+    MPIR_CUDA(cudaMemcpyAsync(F.Ax.as<void>(), Ax, P.S.nnz * sizeof(double),
+                              cudaMemcpyHostToDevice, sg.s));
+    // QDLDL_factor does not scale: an infinite threshold keeps AD = 1.
+    F.run(P, F.Ax.as<double>(), std::numeric_limits<double>::infinity(), sg.s);
+    const int64_t npos = F.result(sg.s);
+    std::vector<int64_t> lp, li;
+    std::vector<float>   lx, d, dinv;
+    export_csc(P, F, sg.s, lp, li, lx, d, dinv);
+    std::memcpy(Lp, lp.data(), (n + 1) * sizeof(int64_t));
+    if (!li.empty()) std::memcpy(Li, li.data(), li.size() * sizeof(int64_t));
+    if (fact_prec == kF32) {
+      if (!lx.empty()) std::memcpy(Lx, lx.data(), lx.size() * sizeof(float));
+      std::memcpy(D, d.data(), n * sizeof(float));
+      std::memcpy(Dinv, dinv.data(), n * sizeof(float));
+    } else {
+      to_16(lx, Lx, fact_prec, sg.s);
+      to_16(d, D, fact_prec, sg.s);
+      to_16(dinv, Dinv, fact_prec, sg.s);
+    }
+    return npos;
+  });
+}
+
+static int qdldl_solve_phases(int64_t n, const int64_t *Lp, const int64_t *Li, const void *Lx,
+                              const void *Dinv, int fact_prec, void *x, int x_prec, int device,
+                              int phases) {
+  return guard([&]() -> int {
+    if (fact_prec != kF32 && fact_prec != kBF16 && fact_prec != kF16)
+      throw StatusError(MPIR_ERR_UNSUPPORTED, "factor type not provided (F32, BF16, F16)");
+    if (x_prec != kF64 && x_prec != kF32)
+      throw StatusError(MPIR_ERR_UNSUPPORTED, "vector type not provided (F64, F32)");
+    if (n <= 0) return n < 0 ? MPIR_ERR_ARGUMENT : MPIR_OK;
+    Symbolic    S;
+    std::string err;
+    const int   rc = analyze_from_L(n, Lp, Li, S, err);
+    if (rc != kOk) throw StatusError(rc, err);
+    StreamGuard sg(device);
+    Plan        P;
+    P.build(std::move(S), sg.s);
+    const Symbolic &Sy = P.S;
+    Numeric         F;
+    F.allocate(P);
+    std::vector<float> lx, dv(n, 1.0f);
+    const int64_t      nl = Lp[n];
+    if (fact_prec == kF32) {
+      lx.assign(static_cast<const float *>(Lx), static_cast<const float *>(Lx) + nl);
+      if (Dinv) dv.assign(static_cast<const float *>(Dinv), static_cast<const float *>(Dinv) + n);
+    } else {
+      from_16(Lx, nl, fact_prec, lx, sg.s);
+      if (Dinv) from_16(Dinv, n, fact_prec, dv, sg.s);
+    }
+    std::vector<float> pan(Sy.panel_elems, 0.0f);
+    for (int64_t J = 0; J < Sy.ns; J++) {
+      const int64_t f = Sy.sfirst[J], l = Sy.sfirst[J + 1], h = Sy.h(J);
+      for (int64_t j = f; j < l; j++) {
+        pan[Sy.slofs[J] + (j - f) * h + (j - f)] = 1.0f;
+        for (int64_t p = Lp[j]; p < Lp[j + 1]; p++)
+          pan[Sy.slofs[J] + (j - f) * h + local_row(Sy, J, Li[p])] = lx[p];
+      }
+    }
+    MPIR_CUDA(cudaMemcpyAsync(F.panel.as<void>(), pan.data(), pan.size() * sizeof(float),
+                              cudaMemcpyHostToDevice, sg.s));
+    MPIR_CUDA(cudaMemcpyAsync(F.Dinv.as<void>(), dv.data(), n * sizeof(float),
+                              cudaMemcpyHostToDevice, sg.s));
+    invert_diag_blocks(P, F, sg.s);
+    SolveWorkspace ws;
+    ws.allocate(P);
+    DeviceBuffer        xd(n * sizeof(double));
+    std::vector<double> xh(n);
+    for (int64_t i = 0; i < n; i++)
+      xh[i] = x_prec == kF64 ? static_cast<const double *>(x)[i]
+                             : static_cast<double>(static_cast<const float *>(x)[i]);
+    MPIR_CUDA(cudaMemcpyAsync(xd.as<void>(), xh.data(), n * sizeof(double),
+                              cudaMemcpyHostToDevice, sg.s));
+    ldlt_solve(P, F, xd.as<double>(), ws, sg.s, phases);
+    MPIR_CUDA(cudaMemcpyAsync(xh.data(), xd.as<void>(), n * sizeof(double),
+                              cudaMemcpyDeviceToHost, sg.s));
+    MPIR_CUDA(cudaStreamSynchronize(sg.s));
+    for (int64_t i = 0; i < n; i++) {
+      if (x_prec == kF64)
+        static_cast<double *>(x)[i] = xh[i];
+      else
+        static_cast<float *>(x)[i] = static_cast<float>(xh[i]);
+    }
+    return MPIR_OK;
+  });
+}
+
+int mpir_qdldl_solve(int64_t n, const int64_t *Lp, const int64_t *Li, const void *Lx,
+                     const void *Dinv, int fact_prec, void *x, int x_prec, int device) {
+  return qdldl_solve_phases(n, Lp, Li, Lx, Dinv, fact_prec, x, x_prec, device, kAllPhases);
+}
+
+int mpir_qdldl_lsolve(int64_t n, const int64_t *Lp, const int64_t *Li, const void *Lx,
+                      int fact_prec, void *x, int x_prec, int device) {
+  return qdldl_solve_phases(n, Lp, Li, Lx, nullptr, fact_prec, x, x_prec, device, kForward);
+}
+
+int mpir_qdldl_ltsolve(int64_t n, const int64_t *Lp, const int64_t *Li, const void *Lx,
+                       int fact_prec, void *x, int x_prec, int device) {
+  return qdldl_solve_phases(n, Lp, Li, Lx, nullptr, fact_prec, x, x_prec, device, kBackward);
+}
+
+int mpir_solver_create(mpir_solver *out, int uf, int uw, int ur, int device) {
+  return guard([&]() -> int {
+    if (!out) return MPIR_ERR_ARGUMENT;
+    *out = nullptr;
+    if (uf != kF32 || uw != kF64 || (ur != kF64 && ur != kDD))
+      throw StatusError(MPIR_ERR_UNSUPPORTED,
+                        "provided precisions: UF=F32, UW=F64, UR=F64 or DD");
+    auto *h = new mpir_solver_s{nullptr};
+    try {
+      h->impl = new Solver(uf, uw, ur, device);
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    *out = h;
+    return MPIR_OK;
+  });
+}
+
+int mpir_solver_destroy(mpir_solver s) {
+  return guard([&]() -> int {
+    if (s) {
+      delete s->impl;
+      delete s;
+    }
+    return MPIR_OK;
+  });
+}
+
+#define MPIR_NEED(s)                                          \
+  if (!(s) || !(s)->impl) {                                   \
+    g_err = "null solver handle";                             \
+    return MPIR_ERR_ARGUMENT;                                 \
+  }
+
+int mpir_solver_set_max_ir_iterations(mpir_solver s, int64_t n) {
+  MPIR_NEED(s);
+  if (n < 0) return MPIR_ERR_ARGUMENT;
+  s->impl->ir_iter = n;
+  return MPIR_OK;
+}
+int mpir_solver_set_max_gmres_iterations(mpir_solver s, int64_t n) {
+  MPIR_NEED(s);
+  if (n < 0) return MPIR_ERR_ARGUMENT;
+  s->impl->gmres_iter = n;
+  return MPIR_OK;
+}
+int mpir_solver_set_tolerance(mpir_solver s, double tol) {
+  MPIR_NEED(s);
+  s->impl->tol = tol;
+  return MPIR_OK;
+}
+
+int mpir_solver_analyze(mpir_solver s, int64_t n, const int64_t *Ap, const int64_t *Ai,
+                        const double *Ax, int ordering) {
+  MPIR_NEED(s);
+  return guard([&]() -> int {
+    if (n < 0 || (n > 0 && (!Ap || !Ai))) return MPIR_ERR_ARGUMENT;
+    if (ordering != MPIR_ORDER_NATURAL && ordering != MPIR_ORDER_AUTO) return MPIR_ERR_ARGUMENT;
+    Symbolic    probe;
+    std::string err;
+    // Input errors surface with QDLDL's codes before anything is allocated.
+    for (int64_t j = 0; j < n; j++) {
+      if (Ap[j] == Ap[j + 1]) throw StatusError(MPIR_ERR_INPUT, "empty column " + std::to_string(j));
+      for (int64_t p = Ap[j]; p < Ap[j + 1]; p++)
+        if (Ai[p] > j || Ai[p] < 0)
+          throw StatusError(MPIR_ERR_INPUT, "entry below the diagonal in column " + std::to_string(j));
+    }
+    return s->impl->analyze(n, Ap, Ai, Ax, ordering);
+  });
+}
+
+int mpir_solver_factor(mpir_solver s, const double *Ax) {
+  MPIR_NEED(s);
+  return guard([&]() -> int {
+    const int rc = s->impl->factor(Ax);
+    if (rc == kBadInput) g_err = "zero pivot";
+    return rc;
+  });
+}
+
+int mpir_solver_factor_device(mpir_solver s, const double *d_Ax) {
+  MPIR_NEED(s);
+  return guard([&]() -> int {
+    const int rc = s->impl->factor_device(d_Ax);
+    if (rc == kBadInput) g_err = "zero pivot";
+    return rc;
+  });
+}
+
+int mpir_solver_compute(mpir_solver s, int64_t n, const int64_t *Ap, const int64_t *Ai,
+                        const double *Ax) {
+  const int rc = mpir_solver_analyze(s, n, Ap, Ai, Ax, MPIR_ORDER_AUTO);
+  if (rc != MPIR_OK) return rc;
+  return mpir_solver_factor(s, Ax);
+}
+
+int mpir_solver_solve(mpir_solver s, const double *b, double *x, mpir_report *rep) {
+  MPIR_NEED(s);
+  static_assert(sizeof(mpir_report) == sizeof(Report), "report layout");
+  return guard([&]() -> int {
+    return s->impl->solve(b, x, reinterpret_cast<Report *>(rep));
+  });
+}
+
+int mpir_solver_solve_device(mpir_solver s, const double *d_b, double *d_x, mpir_report *rep) {
+  MPIR_NEED(s);
+  return guard([&]() -> int {
+    return s->impl->solve_device(d_b, d_x, reinterpret_cast<Report *>(rep));
+  });
+}
+
+int mpir_solver_set_stream(mpir_solver s, void *stream) {
+  MPIR_NEED(s);
+  s->impl->set_stream(static_cast<cudaStream_t>(stream));
+  return MPIR_OK;
+}
+
+int mpir_solver_info(mpir_solver s, mpir_info *info) {
+  MPIR_NEED(s);
+  return guard([&]() -> int {
+    if (!info) return MPIR_ERR_ARGUMENT;
+    std::memset(info, 0, sizeof *info);
+    const Solver &sv = *s->impl;
+    const Plan   &P  = sv.plan();
+    const Symbolic &S = P.S;
+    info->n            = S.n;
+    info->nnz_upper    = S.nnz;
+    info->nnz_L        = S.nnzL;
+    info->supernodes   = S.ns;
+    info->levels       = S.nlevels;
+    info->panel_bytes  = S.panel_elems * 4;
+    info->update_bytes = S.uarena_elems * 4;
+    info->max_front    = S.max_h;
+    double fl = 0;
+    for (int64_t j = 0; j < S.n; j++) fl += static_cast<double>(S.Lnz[j]) * S.Lnz[j];
+    info->factor_flops     = fl;
+    info->solve_bytes      = 2.0 * 4.0 * S.nnzL + 4.0 * S.n + 4.0 * 8.0 * S.n;
+    info->update_flops     = P.update_flops;
+    info->trsm_flops       = P.trsm_flops;
+    info->panel_read_bytes = P.panel_read_bytes;
+    return MPIR_OK;
+  });
+}
+
+int mpir_solver_symbolic(mpir_solver s, int64_t *perm, int64_t *etree, int64_t *Lnz,
+                         int64_t *Cp, int64_t *Ci, int64_t *Csrc) {
+  MPIR_NEED(s);
+  return guard([&]() -> int {
+    const Symbolic &S = s->impl->plan().S;
+    auto put = [](int64_t *dst, const std::vector<int64_t> &v) {
+      if (dst && !v.empty()) std::memcpy(dst, v.data(), v.size() * sizeof(int64_t));
+    };
+    put(perm, S.perm);
+    put(etree, S.etree);
+    put(Lnz, S.Lnz);
+    put(Cp, S.Cp);
+    put(Ci, S.Ci);
+    put(Csrc, S.Csrc);
+    return MPIR_OK;
+  });
+}
+
+int mpir_solver_supernodes(mpir_solver s, int64_t *sfirst, int64_t *srowptr, int32_t *srows,
+                           int64_t *nrows) {
+  MPIR_NEED(s);
+  return guard([&]() -> int {
+    const Symbolic &S = s->impl->plan().S;
+    if (sfirst) std::memcpy(sfirst, S.sfirst.data(), S.sfirst.size() * sizeof(int64_t));
+    if (srowptr) std::memcpy(srowptr, S.srowptr.data(), S.srowptr.size() * sizeof(int64_t));
+    if (srows && !S.srows.empty())
+      std::memcpy(srows, S.srows.data(), S.srows.size() * sizeof(int32_t));
+    if (nrows) *nrows = static_cast<int64_t>(S.srows.size());
+    return MPIR_OK;
+  });
+}
+
+int mpir_solver_export_factor(mpir_solver s, int64_t *Lp, int64_t *Li, float *Lx, float *D,
+                              float *Dinv) {
+  MPIR_NEED(s);
+  return guard([&]() -> int {
+    const Solver &sv = *s->impl;
+    if (!sv.numeric().valid) throw std::logic_error("no valid factor");
+    std::vector<int64_t> lp, li;
+    std::vector<float>   lx, d, dinv;
+    export_csc(sv.plan(), sv.numeric(), sv.stream(), lp, li, lx, d, dinv);
+    const int64_t n = sv.plan().S.n;
+    if (Lp) std::memcpy(Lp, lp.data(), (n + 1) * sizeof(int64_t));
+    if (Li && !li.empty()) std::memcpy(Li, li.data(), li.size() * sizeof(int64_t));
+    if (Lx && !lx.empty()) std::memcpy(Lx, lx.data(), lx.size() * sizeof(float));
+    if (D && n) std::memcpy(D, d.data(), n * sizeof(float));
+    if (Dinv && n) std::memcpy(Dinv, dinv.data(), n * sizeof(float));
+    return MPIR_OK;
+  });
+}
+
+int mpir_analyze_host(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *Ax,
+                      int ordering, int64_t *perm, int64_t *etree, int64_t *Lnz, int64_t *Cp,
+                      int64_t *Ci, int64_t *Lp, int64_t *Li, mpir_info *info) {
+  return guard([&]() -> int {
+    if (n < 0 || (n > 0 && (!Ap || !Ai))) return MPIR_ERR_ARGUMENT;
+    std::vector<int8_t> sign;
+    if (Ax) {
+      sign.assign(n, 0);
+      for (int64_t j = 0; j < n; j++)
+        for (int64_t p = Ap[j]; p < Ap[j + 1]; p++)
+          if (Ai[p] == j && Ax[p] > 0) sign[j] = 1;
+    }
+    Symbolic    S;
+    std::string err;
+    const int   rc = analyze(n, Ap, Ai, Ax ? sign.data() : nullptr,
+                             static_cast<Ordering>(ordering), S, err);
+    if (rc != kOk) throw StatusError(rc, err);
+    auto put = [](int64_t *dst, const std::vector<int64_t> &v) {
+      if (dst && !v.empty()) std::memcpy(dst, v.data(), v.size() * sizeof(int64_t));
+    };
+    put(perm, S.perm);
+    put(etree, S.etree);
+    put(Lnz, S.Lnz);
+    put(Cp, S.Cp);
+    put(Ci, S.Ci);
+    if (Lp || Li) {
+      std::vector<int64_t> lp, li;
+      exact_pattern(S, lp, li);
+      put(Lp, lp);
+      put(Li, li);
+    }
+    if (info) {
+      std::memset(info, 0, sizeof *info);
+      info->n            = S.n;
+      info->nnz_upper    = S.nnz;
+      info->nnz_L        = S.nnzL;
+      info->supernodes   = S.ns;
+      info->levels       = S.nlevels;
+      info->panel_bytes  = S.panel_elems * 4;
+      info->update_bytes = S.uarena_elems * 4;
+      info->max_front    = S.max_h;
+      double fl = 0;
+      for (int64_t j = 0; j < S.n; j++) fl += static_cast<double>(S.Lnz[j]) * S.Lnz[j];
+      info->factor_flops = fl;
+      info->solve_bytes  = 2.0 * 4.0 * S.nnzL + 4.0 * S.n + 4.0 * 8.0 * S.n;
+    }
+    return MPIR_OK;
+  });
+}
+
+int64_t mpir_launch_count(void) { return launch_counter(); }
+
+int mpir_kernel_timer_enable(int on) {
+  KernelTimer &t = kernel_timer();
+  t.enabled      = on != 0;
+  t.reset();
+  return MPIR_OK;
+}
+
+int mpir_kernel_timer_collect(double *ms, int64_t *launches, int nclass) {
+  return guard([&]() -> int {
+    MPIR_CUDA(cudaDeviceSynchronize());
+    kernel_timer().collect(ms, launches, nclass);
+    return MPIR_OK;
+  });
+}
+
+}  // extern "C"

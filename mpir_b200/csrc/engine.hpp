@@ -1,0 +1,149 @@
+// Device-resident plan (per pattern) and numeric factor (per value set).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <vector>
+
+#include "common.cuh"
+#include "symbolic.hpp"
+
+namespace mpir {
+
+// Owning device allocation.
+class DeviceBuffer {
+ public:
+  DeviceBuffer() = default;
+  explicit DeviceBuffer(size_t bytes) { resize(bytes); }
+  ~DeviceBuffer() { release(); }
+  DeviceBuffer(const DeviceBuffer &)            = delete;
+  DeviceBuffer &operator=(const DeviceBuffer &) = delete;
+  DeviceBuffer(DeviceBuffer &&o) noexcept : p_(o.p_), bytes_(o.bytes_) {
+    o.p_     = nullptr;
+    o.bytes_ = 0;
+  }
+  DeviceBuffer &operator=(DeviceBuffer &&o) noexcept {
+    if (this != &o) {
+      release();
+      p_       = o.p_;
+      bytes_   = o.bytes_;
+      o.p_     = nullptr;
+      o.bytes_ = 0;
+    }
+    return *this;
+  }
+  void resize(size_t bytes) {
+    release();
+    if (bytes) MPIR_CUDA(cudaMalloc(&p_, bytes));
+    bytes_ = bytes;
+  }
+  void release() {
+    if (p_) cudaFree(p_);
+    p_     = nullptr;
+    bytes_ = 0;
+  }
+  template <class T>
+  T *as() const {
+    return static_cast<T *>(p_);
+  }
+  size_t bytes() const { return bytes_; }
+
+ private:
+  void  *p_     = nullptr;
+  size_t bytes_ = 0;
+};
+
+template <class T>
+DeviceBuffer upload(const std::vector<T> &v, cudaStream_t s) {
+  DeviceBuffer b(v.size() * sizeof(T));
+  if (!v.empty())
+    MPIR_CUDA(cudaMemcpyAsync(b.as<void>(), v.data(), v.size() * sizeof(T),
+                              cudaMemcpyHostToDevice, s));
+  return b;
+}
+
+// Launch lists of one etree level.
+struct LevelPlan {
+  int32_t small_begin = 0, small_count = 0;  // into small list
+  int32_t large_begin = 0, large_count = 0;  // into large list
+  int32_t zero_begin = 0, zero_count = 0;
+  int64_t zero_chunks = 0;
+  struct Round {
+    int32_t begin, count, chunks;
+  };
+  std::vector<Round> ea_rounds;
+  struct Step {
+    int32_t begin, count, trsm_tiles, upd_tiles, fsolve_tiles, bsolve_chunks;
+  };
+  std::vector<Step> steps;
+  // Solve: large fronts' gather list = large list; small fronts handled by
+  // one thread block each.
+};
+
+// Everything the kernels need about one analysed pattern.
+class Plan {
+ public:
+  Symbolic               S;
+  std::vector<LevelPlan> levels;
+  int64_t                linv_elems = 0;
+  int64_t                nnz_full   = 0;
+  int64_t                ndesc      = 0;  // step descriptors in total
+  int64_t                bpart_elems = 0; // backward partial sums (doubles)
+  double                 update_flops = 0, trsm_flops = 0, panel_read_bytes = 0;
+  // Pattern arrays on the device.
+  DeviceBuffer amap, arow, acol, diag_pos, Kp, Kj, Ksrc;
+  DeviceBuffer sfirst, srowptr, srows, srel, slofs, uofs, zofs, child_ptr,
+      child_list, perm;
+  DeviceBuffer small_list, large_list, steps, ea_tasks, zero_segs;
+  std::vector<int32_t> h_small, h_large;
+  std::vector<int64_t> linv_ofs;  // per supernode, -1 for small fronts
+
+  void build(Symbolic &&sym, cudaStream_t s);
+  bool is_large(int64_t J) const { return S.h(J) > kSmallFront; }
+};
+
+// Numeric factor of one value set on a plan.
+class Numeric {
+ public:
+  DeviceBuffer panel, uarena, linv, D, Dinv, status;
+  DeviceBuffer AD, Axs, Kval, Korig, Ax;
+  double       eps_uf = 0;
+  bool         valid  = false;
+
+  void allocate(const Plan &P);
+  // Scale the caller's values (device, caller order), assemble and factor.
+  void run(const Plan &P, const double *d_Ax, double eps_uf, cudaStream_t s);
+  // Reads the status; returns #positive D or -1 on a zero pivot.
+  int64_t result(cudaStream_t s, int32_t *zero_col = nullptr,
+                 bool *nonfinite = nullptr) const;
+};
+
+// Kernel-class timer used by the benchmark's roofline figures.
+struct KernelTimer {
+  bool                      enabled = false;
+  std::vector<cudaEvent_t>  ev;
+  std::vector<int>          cls;
+  void                      begin(int c, cudaStream_t s);
+  void                      end(cudaStream_t s);
+  void                      reset();
+  // Total milliseconds and launches per class (after a synchronize).
+  void collect(double *ms, int64_t *count, int nclass);
+};
+enum KernelClass : int {
+  kKcSmallFront = 0,
+  kKcDiag,
+  kKcTrsm,
+  kKcUpdate,
+  kKcExtendAdd,
+  kKcZero,
+  kKcScatter,
+  kKcSolveFwd,
+  kKcSolveBwd,
+  kKcSpmv,
+  kKcVec,
+  kKcCount
+};
+KernelTimer &kernel_timer();
+
+}  // namespace mpir

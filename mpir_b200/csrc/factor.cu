@@ -1,0 +1,759 @@
+// Numeric multifrontal LDL^T factorization on the GPU.
+//
+// The factor of P K P^T equals, entry for entry up to rounding, the one
+// QDLDL_factor computes row by row (qdldl.hpp:172-345); it is organised here
+// as a level-scheduled multifrontal method over the supernodal elimination
+// tree instead:
+//   * the scaled entries of K are scattered into zeroed panels;
+//   * level by level (leaves first), each front gathers its children's
+//     update matrices (extend-add), eliminates its own columns with a dense
+//     partial LDL^T and leaves its Schur complement as its update matrix;
+//   * fronts of at most kSmallFront rows are done whole in shared memory, one
+//     thread block each; larger fronts go through a blocked right-looking
+//     partial factorization whose steps are batched over all fronts of the
+//     level: diagonal-block factor + inverse, a GEMM-shaped panel solve
+//     (W = F L^{-T}, L = W D^{-1}) and a GEMM-shaped trailing update
+//     C -= (L D) L^T.
+// D is left on each panel's diagonal and copied to D / Dinv (permuted order).
+#include <algorithm>
+#include <climits>
+#include <cmath>
+
+#include "common.cuh"
+#include "engine.hpp"
+
+namespace mpir {
+
+// ---------------------------------------------------------------------------
+// Scaling and assembly of K's entries.
+
+// AD_i = 1/sqrt|k_ii| when |k_ii| > eps(UF), else 1 (gmres_ir.hpp:347-356).
+__global__ void k_scaling(int64_t n, const int64_t *diag_pos, const double *Ax,
+                          double eps, double *AD) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double        d = 1.0;
+  const int64_t p = diag_pos[i];
+  if (p >= 0) {
+    const double a = fabs(Ax[p]);
+    if (a > eps) d = 1.0 / sqrt(a);
+  }
+  AD[i] = d;
+}
+
+// a_rc *= AD_r AD_c (gmres_ir.hpp:358-363) and scatter into the panels in the
+// factor type.
+__global__ void k_scatter(int64_t nnz, const double *Ax, const double *AD,
+                          const int32_t *arow, const int32_t *acol,
+                          const int64_t *amap, double *Axs, float *panel) {
+  const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (p >= nnz) return;
+  const double v = Ax[p] * (AD[arow[p]] * AD[acol[p]]);
+  Axs[p]         = v;
+  panel[amap[p]] = static_cast<float>(v);
+}
+
+// Values of the full symmetric CSR of P K P^T: scaled and original.
+__global__ void k_csr_values(int64_t nnzf, const int64_t *Ksrc,
+                             const double *Axs, const double *Ax, double *Kval,
+                             double *Korig) {
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= nnzf) return;
+  const int64_t p = Ksrc[e];
+  Kval[e]         = Axs[p];
+  Korig[e]        = Ax[p];
+}
+
+__device__ __forceinline__ void note_pivot(FactorStatus *st, int32_t col,
+                                           float d, int *npos) {
+  if (d == 0.0f) atomicMin(&st->zero_pivot, col);
+  if (!isfinite(d)) st->nonfinite = 1;
+  if (d > 0.0f) (*npos)++;
+}
+
+// ---------------------------------------------------------------------------
+// Small fronts: whole front in shared memory.
+template <int HMAX>
+__global__ void __launch_bounds__(kSmallThreads)
+    k_small_fronts(const int32_t *list, const int64_t *sfirst,
+                   const int64_t *srowptr, const int64_t *slofs,
+                   const int64_t *uofs, const int64_t *child_ptr,
+                   const int32_t *child_list, const int32_t *srel,
+                   float *panel, float *uarena, float *D, float *Dinv,
+                   FactorStatus *st) {
+  __shared__ float F[HMAX][HMAX + 1];
+  __shared__ float wv[HMAX];
+  __shared__ int   s_npos;
+  const int        J   = list[blockIdx.x];
+  const int        tid = threadIdx.x, bd = blockDim.x;
+  const int64_t    f   = sfirst[J];
+  const int        w   = static_cast<int>(sfirst[J + 1] - f);
+  const int        h   = static_cast<int>(srowptr[J + 1] - srowptr[J]);
+  float           *P   = panel + slofs[J];
+  if (tid == 0) s_npos = 0;
+  for (int idx = tid; idx < h * h; idx += bd) {
+    const int i = idx % h, j = idx / h;
+    F[i][j]     = (j < w && i >= j) ? P[i + (int64_t)j * h] : 0.0f;
+  }
+  __syncthreads();
+  for (int64_t c = child_ptr[J]; c < child_ptr[J + 1]; c++) {
+    const int      C  = child_list[c];
+    const int      wc = static_cast<int>(sfirst[C + 1] - sfirst[C]);
+    const int      rc = static_cast<int>(srowptr[C + 1] - srowptr[C]) - wc;
+    const float   *U  = uarena + uofs[C];
+    const int32_t *rl = srel + srowptr[C] + wc;
+    for (int idx = tid; idx < rc * rc; idx += bd) {
+      const int a = idx % rc, b = idx / rc;
+      if (a >= b) F[rl[a]][rl[b]] += U[a + (int64_t)b * rc];
+    }
+    __syncthreads();
+  }
+  int npos = 0;
+  for (int k = 0; k < w; k++) {
+    const float dk = F[k][k];
+    for (int i = k + 1 + tid; i < h; i += bd) wv[i] = F[i][k];
+    __syncthreads();
+    const float dinv = 1.0f / dk;
+    const int   m    = h - k - 1;
+    for (int idx = tid; idx < m * m; idx += bd) {
+      const int ii = idx % m, jj = idx / m;
+      if (ii >= jj) {
+        const int i = k + 1 + ii, j = k + 1 + jj;
+        F[i][j] -= (wv[i] * dinv) * wv[j];
+      }
+    }
+    for (int i = k + 1 + tid; i < h; i += bd) F[i][k] = wv[i] * dinv;
+    if (tid == 0) {
+      D[f + k]    = dk;
+      Dinv[f + k] = dinv;
+      note_pivot(st, static_cast<int32_t>(f + k), dk, &npos);
+    }
+    __syncthreads();
+  }
+  if (tid == 0) atomicAdd(&st->npos, npos);
+  for (int idx = tid; idx < h * w; idx += bd) {
+    const int i = idx % h, j = idx / h;
+    if (i >= j) P[i + (int64_t)j * h] = F[i][j];
+  }
+  const int r = h - w;
+  if (r > 0) {
+    float *U = uarena + uofs[J];
+    for (int idx = tid; idx < r * r; idx += bd) {
+      const int a = idx % r, b = idx / r;
+      U[a + (int64_t)b * r] = a >= b ? F[w + a][w + b] : 0.0f;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Zero the update matrices of the level's large fronts.
+__global__ void k_zero_segments(const Segment *segs, int nseg, float *base) {
+  const int64_t t  = blockIdx.x;
+  int           lo = 0, hi = nseg - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    if (segs[mid].chunk0 <= t) lo = mid; else hi = mid - 1;
+  }
+  const Segment sg  = segs[lo];
+  const int64_t beg = (t - sg.chunk0) * kZeroChunk;
+  const int64_t end = min(beg + kZeroChunk, sg.len);
+  float        *p   = base + sg.ofs;
+  for (int64_t i = beg + threadIdx.x; i < end; i += blockDim.x) p[i] = 0.0f;
+}
+
+// Extend-add of children's update matrices into large parents.
+__global__ void k_extend_add(const EaTask *tasks, int ntasks,
+                             const int32_t *srel, float *panel,
+                             float *uarena) {
+  const int t  = blockIdx.x;
+  int       lo = 0, hi = ntasks - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    if (tasks[mid].chunk0 <= t) lo = mid; else hi = mid - 1;
+  }
+  const EaTask   tk  = tasks[lo];
+  const int      b0  = (t - tk.chunk0) * kEaChunk;
+  const int      b1  = min(b0 + kEaChunk, tk.rc);
+  const int32_t *rl  = srel + tk.rel;
+  const float   *U   = uarena + tk.child_u;
+  float         *Pp  = panel + tk.parent_panel;
+  const int      rp  = tk.hp - tk.wp;
+  for (int b = b0; b < b1; b++) {
+    const int cb = rl[b];
+    for (int a = b + threadIdx.x; a < tk.rc; a += blockDim.x) {
+      const int   ra  = rl[a];
+      const float val = U[a + (int64_t)b * tk.rc];
+      if (cb < tk.wp)
+        Pp[ra + (int64_t)cb * tk.hp] += val;
+      else
+        uarena[tk.parent_u + (ra - tk.wp) + (int64_t)(cb - tk.wp) * rp] += val;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Diagonal block of one step: LDL^T of the nbk x nbk block in shared memory,
+// together with the inverse of its unit-lower factor (right-looking forward
+// substitution on the identity, done in the same sweep).
+__global__ void __launch_bounds__(kDiagThreads)
+    k_diag_block(const StepDesc *descs, float *panel, float *linv, float *D,
+                 float *Dinv, FactorStatus *st) {
+  extern __shared__ float sm[];
+  constexpr int           LD = kNB + 1;
+  float                  *F  = sm;
+  float                  *X  = sm + kNB * LD;
+  float                  *wv = X + kNB * LD;
+  __shared__ int          s_npos;
+  const StepDesc          d   = descs[blockIdx.x];
+  const int               n   = d.nbk;
+  const int64_t           h   = d.h;
+  const int               tid = threadIdx.x, bd = blockDim.x;
+  float                  *P   = panel + d.panel + d.kb + (int64_t)d.kb * h;
+  if (tid == 0) s_npos = 0;
+  for (int idx = tid; idx < n * n; idx += bd) {
+    const int i = idx % n, j = idx / n;
+    F[i * LD + j] = i >= j ? P[i + (int64_t)j * h] : 0.0f;
+    X[i * LD + j] = i == j ? 1.0f : 0.0f;
+  }
+  __syncthreads();
+  int npos = 0;
+  for (int k = 0; k < n; k++) {
+    const float dk = F[k * LD + k];
+    for (int i = k + 1 + tid; i < n; i += bd) wv[i] = F[i * LD + k];
+    __syncthreads();
+    const float dinv = 1.0f / dk;
+    const int   m    = n - k - 1;
+    for (int idx = tid; idx < m * m; idx += bd) {
+      const int ii = idx % m, jj = idx / m;
+      if (ii >= jj) {
+        const int i = k + 1 + ii, j = k + 1 + jj;
+        F[i * LD + j] -= (wv[i] * dinv) * wv[j];
+      }
+    }
+    for (int idx = tid; idx < m * (k + 1); idx += bd) {
+      const int i = k + 1 + idx % m, j = idx / m;
+      X[i * LD + j] -= (wv[i] * dinv) * X[k * LD + j];
+    }
+    for (int i = k + 1 + tid; i < n; i += bd) F[i * LD + k] = wv[i] * dinv;
+    if (tid == 0) {
+      const int64_t col = (int64_t)d.col0 + d.kb + k;
+      D[col]            = dk;
+      Dinv[col]         = dinv;
+      note_pivot(st, static_cast<int32_t>(col), dk, &npos);
+    }
+    __syncthreads();
+  }
+  if (tid == 0) atomicAdd(&st->npos, npos);
+  float *Lv = linv + d.linv;
+  for (int idx = tid; idx < kNB * kNB; idx += bd) {
+    const int i = idx % kNB, j = idx / kNB;
+    if (i < n && j < n) {
+      if (i >= j) P[i + (int64_t)j * h] = F[i * LD + j];
+      Lv[i + j * kNB] = X[i * LD + j];
+    } else {
+      Lv[i + j * kNB] = 0.0f;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// GEMM-shaped kernels of a step (FP32 SIMT, 128x128 tiles, K in slices of 16).
+//   TRSM:   C = (A B^T) .* dinv(cols), in place over A's block column;
+//           A = panel rows below the block, B = Linv of the block.
+//   UPDATE: C -= (A .* d(k)) B^T on the lower part; A = B = the eliminated
+//           block column (rows below), C = trailing panel or update matrix.
+constexpr int kBM = 128, kBN = 128, kBK = 16;
+
+template <bool TRSM>
+__global__ void __launch_bounds__(kGemmThreads)
+    k_step_gemm(const StepDesc *descs, int ndesc, float *panel, float *uarena,
+                const float *linv, const float *Dinv) {
+  __shared__ float As[kBK][kBM];
+  __shared__ float Bs[kBK][kBN];
+  __shared__ float sd[kNB];
+  const int        t  = blockIdx.x;
+  int              lo = 0, hi = ndesc - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    const int t0  = TRSM ? descs[mid].trsm_tile0 : descs[mid].upd_tile0;
+    if (t0 <= t) lo = mid; else hi = mid - 1;
+  }
+  const StepDesc d     = descs[lo];
+  int            local = t - (TRSM ? d.trsm_tile0 : d.upd_tile0);
+  const int64_t  h     = d.h;
+  const int      kb = d.kb, nbk = d.nbk, w = d.w;
+  const float   *A, *B;
+  float         *C;
+  int64_t        lda, ldb, ldc;
+  int            M, N, m0, n0;
+  const int      K = nbk;
+  float         *Pp = panel + d.panel;
+  if (TRSM) {
+    M   = static_cast<int>(h) - kb - nbk;
+    N   = nbk;
+    A   = Pp + (kb + nbk) + (int64_t)kb * h;
+    lda = h;
+    B   = linv + d.linv;
+    ldb = kNB;
+    C   = Pp + (kb + nbk) + (int64_t)kb * h;
+    ldc = h;
+    m0  = local * kBM;
+    n0  = 0;
+  } else {
+    if (local < d.upd_panel_tiles) {
+      M = static_cast<int>(h) - kb - nbk;
+      N = w - kb - nbk;
+      A = Pp + (kb + nbk) + (int64_t)kb * h;
+      C = Pp + (kb + nbk) + (int64_t)(kb + nbk) * h;
+      ldc = h;
+    } else {
+      local -= d.upd_panel_tiles;
+      M = N = static_cast<int>(h) - w;
+      A     = Pp + w + (int64_t)kb * h;
+      C     = uarena + d.uofs;
+      ldc   = M;
+    }
+    lda = ldb = h;
+    B         = A;
+    const int ntr = (M + kBM - 1) / kBM;
+    int       j   = 0;
+    while (local >= ntr - j) {
+      local -= ntr - j;
+      j++;
+    }
+    m0 = (j + local) * kBM;
+    n0 = j * kBN;
+    for (int k = threadIdx.x; k < nbk; k += blockDim.x)
+      sd[k] = Pp[(kb + k) + (int64_t)(kb + k) * h];
+  }
+  const int tid = threadIdx.x;
+  const int tr = tid / 16, tc = tid % 16;
+  float     acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+#pragma unroll
+    for (int j = 0; j < 8; j++) acc[i][j] = 0.0f;
+  __syncthreads();
+  for (int k0 = 0; k0 < K; k0 += kBK) {
+#pragma unroll
+    for (int q = 0; q < (kBM * kBK) / kGemmThreads; q++) {
+      const int idx = tid + q * kGemmThreads;
+      const int i = idx % kBM, kk = idx / kBM;
+      const int r = m0 + i, k = k0 + kk;
+      float     v = 0.0f;
+      if (r < M && k < K) {
+        v = A[r + (int64_t)k * lda];
+        if (!TRSM) v *= sd[k];
+      }
+      As[kk][i] = v;
+      const int c  = n0 + i;
+      float     bv = 0.0f;
+      if (c < N && k < K) bv = B[c + (int64_t)k * ldb];
+      Bs[kk][i] = bv;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < kBK; kk++) {
+      float a[8], b[8];
+#pragma unroll
+      for (int i = 0; i < 8; i++) a[i] = As[kk][tr * 8 + i];
+#pragma unroll
+      for (int j = 0; j < 8; j++) b[j] = Bs[kk][tc * 8 + j];
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    const int c = n0 + tc * 8 + j;
+    if (c >= N) continue;
+    const float dv = TRSM ? Dinv[(int64_t)d.col0 + kb + c] : 0.0f;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const int r = m0 + tr * 8 + i;
+      if (r >= M) continue;
+      if (TRSM) {
+        C[r + (int64_t)c * ldc] = acc[i][j] * dv;
+      } else if (r >= c) {
+        C[r + (int64_t)c * ldc] -= acc[i][j];
+      }
+    }
+  }
+}
+
+// Inverses of the unit-lower diagonal blocks of a factor that was supplied
+// rather than computed here (the QDLDL_solve entry point).
+__global__ void __launch_bounds__(kDiagThreads)
+    k_invert_blocks(const StepDesc *descs, const float *panel, float *linv) {
+  extern __shared__ float sm[];
+  constexpr int           LD = kNB + 1;
+  float                  *F  = sm;
+  float                  *X  = sm + kNB * LD;
+  const StepDesc          d  = descs[blockIdx.x];
+  const int               n  = d.nbk;
+  const int64_t           h  = d.h;
+  const int               tid = threadIdx.x, bd = blockDim.x;
+  const float            *P   = panel + d.panel + d.kb + (int64_t)d.kb * h;
+  for (int idx = tid; idx < n * n; idx += bd) {
+    const int i = idx % n, j = idx / n;
+    F[i * LD + j] = i > j ? P[i + (int64_t)j * h] : 0.0f;
+    X[i * LD + j] = i == j ? 1.0f : 0.0f;
+  }
+  __syncthreads();
+  for (int k = 0; k < n; k++) {
+    const int m = n - k - 1;
+    for (int idx = tid; idx < m * (k + 1); idx += bd) {
+      const int i = k + 1 + idx % m, j = idx / m;
+      X[i * LD + j] -= F[i * LD + k] * X[k * LD + j];
+    }
+    __syncthreads();
+  }
+  float *Lv = linv + d.linv;
+  for (int idx = tid; idx < kNB * kNB; idx += bd) {
+    const int i = idx % kNB, j = idx / kNB;
+    Lv[i + j * kNB] = (i < n && j < n) ? X[i * LD + j] : 0.0f;
+  }
+}
+
+void invert_diag_blocks(const Plan &P, Numeric &F, cudaStream_t s) {
+  if (P.ndesc == 0) return;
+  const int smem = 2 * kNB * (kNB + 1) * sizeof(float);
+  MPIR_CUDA(cudaFuncSetAttribute(k_invert_blocks,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  launch(k_invert_blocks, static_cast<unsigned>(P.ndesc), kDiagThreads, smem, s, 
+      P.steps.as<StepDesc>(), F.panel.as<float>(), F.linv.as<float>());
+  MPIR_CHECK_LAUNCH();
+}
+
+// ---------------------------------------------------------------------------
+// Plan construction.
+
+void Plan::build(Symbolic &&sym, cudaStream_t s) {
+  S              = std::move(sym);
+  const int64_t ns = S.ns;
+  nnz_full         = static_cast<int64_t>(S.Kj.size());
+  // Persistent Linv storage for the large fronts.
+  linv_ofs.assign(ns, -1);
+  linv_elems   = 0;
+  bpart_elems  = 0;
+  update_flops = 0;
+  trsm_flops   = 0;
+  for (int64_t J = 0; J < ns; J++)
+    if (is_large(J)) {
+      linv_ofs[J] = linv_elems;
+      linv_elems += ((S.w(J) + kNB - 1) / kNB) * (int64_t)kNB * kNB;
+    }
+  // Per-level launch lists.
+  levels.assign(S.nlevels, LevelPlan{});
+  h_small.clear();
+  h_large.clear();
+  std::vector<StepDesc> descs;
+  std::vector<EaTask>   tasks;
+  std::vector<Segment>  segs;
+  for (int32_t t = 0; t < S.nlevels; t++) {
+    LevelPlan &L = levels[t];
+    L.small_begin = static_cast<int32_t>(h_small.size());
+    L.large_begin = static_cast<int32_t>(h_large.size());
+    for (int64_t q = S.level_ptr[t]; q < S.level_ptr[t + 1]; q++) {
+      const int32_t J = S.level_sup[q];
+      (is_large(J) ? h_large : h_small).push_back(J);
+    }
+    L.small_count = static_cast<int32_t>(h_small.size()) - L.small_begin;
+    L.large_count = static_cast<int32_t>(h_large.size()) - L.large_begin;
+    // Zero-fill of the large fronts' update matrices.
+    L.zero_begin  = static_cast<int32_t>(segs.size());
+    int64_t chunk = 0;
+    for (int32_t q = L.large_begin; q < L.large_begin + L.large_count; q++) {
+      const int64_t J = h_large[q], r = S.h(J) - S.w(J);
+      if (r <= 0) continue;
+      segs.push_back(Segment{S.uofs[J], r * r, chunk});
+      chunk += (r * r + kZeroChunk - 1) / kZeroChunk;
+    }
+    L.zero_count  = static_cast<int32_t>(segs.size()) - L.zero_begin;
+    L.zero_chunks = chunk;
+    // Extend-add rounds for the large fronts (round q = q-th child).
+    int64_t maxkids = 0;
+    for (int32_t q = L.large_begin; q < L.large_begin + L.large_count; q++) {
+      const int64_t J = h_large[q];
+      maxkids = std::max(maxkids, S.child_ptr[J + 1] - S.child_ptr[J]);
+    }
+    for (int64_t round = 0; round < maxkids; round++) {
+      LevelPlan::Round R{static_cast<int32_t>(tasks.size()), 0, 0};
+      int32_t          ch = 0;
+      for (int32_t q = L.large_begin; q < L.large_begin + L.large_count; q++) {
+        const int64_t P = h_large[q];
+        if (S.child_ptr[P] + round >= S.child_ptr[P + 1]) continue;
+        const int64_t C  = S.child_list[S.child_ptr[P] + round];
+        const int64_t rc = S.h(C) - S.w(C);
+        EaTask        tk;
+        tk.child_u      = S.uofs[C];
+        tk.parent_panel = S.slofs[P];
+        tk.parent_u     = S.uofs[P];
+        tk.rel          = S.srowptr[C] + S.w(C);
+        tk.rc           = static_cast<int32_t>(rc);
+        tk.hp           = static_cast<int32_t>(S.h(P));
+        tk.wp           = static_cast<int32_t>(S.w(P));
+        tk.chunk0       = ch;
+        ch += static_cast<int32_t>((rc + kEaChunk - 1) / kEaChunk);
+        tasks.push_back(tk);
+      }
+      R.count  = static_cast<int32_t>(tasks.size()) - R.begin;
+      R.chunks = ch;
+      if (R.count > 0) L.ea_rounds.push_back(R);
+    }
+    // Blocked steps.
+    int64_t maxw = 0;
+    for (int32_t q = L.large_begin; q < L.large_begin + L.large_count; q++)
+      maxw = std::max(maxw, S.w(h_large[q]));
+    for (int64_t kb = 0; kb < maxw; kb += kNB) {
+      LevelPlan::Step st{static_cast<int32_t>(descs.size()), 0, 0, 0, 0, 0};
+      int64_t         bpart = 0;
+      for (int32_t q = L.large_begin; q < L.large_begin + L.large_count; q++) {
+        const int64_t J = h_large[q], w = S.w(J), h = S.h(J);
+        if (w <= kb) continue;
+        StepDesc d;
+        d.panel  = S.slofs[J];
+        d.uofs   = S.uofs[J];
+        d.linv   = linv_ofs[J] + (kb / kNB) * (int64_t)kNB * kNB;
+        d.h      = static_cast<int32_t>(h);
+        d.w      = static_cast<int32_t>(w);
+        d.kb     = static_cast<int32_t>(kb);
+        d.nbk    = static_cast<int32_t>(std::min<int64_t>(kNB, w - kb));
+        d.col0   = static_cast<int32_t>(S.sfirst[J]);
+        const int64_t M = h - kb - d.nbk;
+        d.trsm_tile0    = st.trsm_tiles;
+        st.trsm_tiles += static_cast<int32_t>((M + kBM - 1) / kBM);
+        d.upd_tile0 = st.upd_tiles;
+        const int64_t N = w - kb - d.nbk;
+        int64_t       pt = 0;
+        if (N > 0 && M > 0) {
+          const int64_t ntr = (M + kBM - 1) / kBM, ntc = (N + kBN - 1) / kBN;
+          pt = ntc * ntr - ntc * (ntc - 1) / 2;
+        }
+        d.upd_panel_tiles = static_cast<int32_t>(pt);
+        const int64_t r   = h - w;
+        int64_t       ut  = 0;
+        if (r > 0) {
+          const int64_t nt = (r + kBM - 1) / kBM;
+          ut               = nt * (nt + 1) / 2;
+        }
+        st.upd_tiles += static_cast<int32_t>(pt + ut);
+        // Work the launches do: 2 * nbk flops per updated lower entry; the
+        // panel solve is a full M x nbk x nbk product.
+        {
+          const double nb = static_cast<double>(d.nbk), Mr = static_cast<double>(M);
+          const double Nc = static_cast<double>(std::max<int64_t>(N, 0));
+          const double rr = static_cast<double>(std::max<int64_t>(r, 0));
+          const double lower_panel = Nc > 0 ? Nc * Mr - Nc * (Nc - 1) / 2 : 0.0;
+          update_flops += 2.0 * nb * (lower_panel + rr * (rr + 1) / 2);
+          trsm_flops += 2.0 * nb * nb * Mr;
+        }
+        d.zofs         = S.zofs[J];
+        d.fsolve_tile0 = st.fsolve_tiles;
+        st.fsolve_tiles += static_cast<int32_t>(
+            std::max<int64_t>(1, (M + kSolveRows - 1) / kSolveRows));
+        d.bsolve_chunks  = static_cast<int32_t>(
+            std::max<int64_t>(1, (M + kSolveChunk - 1) / kSolveChunk));
+        d.bsolve_chunk0  = st.bsolve_chunks;
+        st.bsolve_chunks += d.bsolve_chunks;
+        d.bpart = bpart;
+        bpart += d.bsolve_chunks * (int64_t)kNB;
+        d.id    = static_cast<int32_t>(descs.size());
+        descs.push_back(d);
+        st.count++;
+      }
+      L.steps.push_back(st);
+      bpart_elems = std::max(bpart_elems, bpart);
+    }
+  }
+  ndesc = static_cast<int64_t>(descs.size());
+  panel_read_bytes = 0;
+  for (int64_t J = 0; J < ns; J++) {
+    const double w = static_cast<double>(S.w(J)), h = static_cast<double>(S.h(J));
+    panel_read_bytes += 4.0 * (w * h - w * (w - 1) / 2);
+  }
+  // Upload.
+  amap       = upload(S.amap, s);
+  arow       = upload(S.arow, s);
+  acol       = upload(S.acol, s);
+  diag_pos   = upload(S.diag_pos, s);
+  Kp         = upload(S.Kp, s);
+  Kj         = upload(S.Kj, s);
+  Ksrc       = upload(S.Ksrc, s);
+  sfirst     = upload(S.sfirst, s);
+  srowptr    = upload(S.srowptr, s);
+  srows      = upload(S.srows, s);
+  srel       = upload(S.srel, s);
+  slofs      = upload(S.slofs, s);
+  uofs       = upload(S.uofs, s);
+  zofs       = upload(S.zofs, s);
+  child_ptr  = upload(S.child_ptr, s);
+  child_list = upload(S.child_list, s);
+  perm       = upload(S.perm, s);
+  small_list = upload(h_small, s);
+  large_list = upload(h_large, s);
+  steps      = upload(descs, s);
+  ea_tasks   = upload(tasks, s);
+  zero_segs  = upload(segs, s);
+  MPIR_CUDA(cudaStreamSynchronize(s));
+}
+
+void Numeric::allocate(const Plan &P) {
+  const Symbolic &S = P.S;
+  panel.resize(std::max<int64_t>(S.panel_elems, 1) * sizeof(float));
+  uarena.resize(std::max<int64_t>(S.uarena_elems, 1) * sizeof(float));
+  linv.resize(std::max<int64_t>(P.linv_elems, 1) * sizeof(float));
+  D.resize(std::max<int64_t>(S.n, 1) * sizeof(float));
+  Dinv.resize(std::max<int64_t>(S.n, 1) * sizeof(float));
+  status.resize(sizeof(FactorStatus));
+  AD.resize(std::max<int64_t>(S.n, 1) * sizeof(double));
+  Axs.resize(std::max<int64_t>(S.nnz, 1) * sizeof(double));
+  Kval.resize(std::max<int64_t>(P.nnz_full, 1) * sizeof(double));
+  Korig.resize(std::max<int64_t>(P.nnz_full, 1) * sizeof(double));
+  Ax.resize(std::max<int64_t>(S.nnz, 1) * sizeof(double));
+  valid = false;
+}
+
+static unsigned grid_for(int64_t n, int threads) {
+  return static_cast<unsigned>((n + threads - 1) / threads);
+}
+
+void Numeric::run(const Plan &P, const double *d_Ax, double eps, cudaStream_t s) {
+  const Symbolic &S  = P.S;
+  KernelTimer    &kt = kernel_timer();
+  eps_uf             = eps;
+  valid              = false;
+  FactorStatus init{INT_MAX, 0, 0, 0};
+  MPIR_CUDA(cudaMemcpyAsync(status.as<void>(), &init, sizeof init,
+                            cudaMemcpyHostToDevice, s));
+  MPIR_CUDA(cudaMemsetAsync(panel.as<void>(), 0, S.panel_elems * sizeof(float), s));
+  if (S.n == 0) return;
+  kt.begin(kKcScatter, s);
+  launch(k_scaling, grid_for(S.n, 256), 256, 0, s, S.n, P.diag_pos.as<int64_t>(), d_Ax,
+                                               eps, AD.as<double>());
+  launch(k_scatter, grid_for(S.nnz, 256), 256, 0, s, 
+      S.nnz, d_Ax, AD.as<double>(), P.arow.as<int32_t>(), P.acol.as<int32_t>(),
+      P.amap.as<int64_t>(), Axs.as<double>(), panel.as<float>());
+  launch(k_csr_values, grid_for(P.nnz_full, 256), 256, 0, s, 
+      P.nnz_full, P.Ksrc.as<int64_t>(), Axs.as<double>(), d_Ax, Kval.as<double>(),
+      Korig.as<double>());
+  kt.end(s);
+  MPIR_CHECK_LAUNCH();
+  static bool attr = false;
+  const int   diag_smem = (2 * kNB * (kNB + 1) + kNB) * sizeof(float);
+  if (!attr) {
+    MPIR_CUDA(cudaFuncSetAttribute(k_diag_block,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   diag_smem));
+    attr = true;
+  }
+  float        *pan = panel.as<float>(), *ua = uarena.as<float>();
+  FactorStatus *st  = status.as<FactorStatus>();
+  for (const LevelPlan &L : P.levels) {
+    if (L.zero_count > 0) {
+      kt.begin(kKcZero, s);
+      launch(k_zero_segments, static_cast<unsigned>(L.zero_chunks), 256, 0, s, 
+          P.zero_segs.as<Segment>() + L.zero_begin, L.zero_count, ua);
+      kt.end(s);
+    }
+    for (const auto &R : L.ea_rounds) {
+      kt.begin(kKcExtendAdd, s);
+      launch(k_extend_add, R.chunks, 256, 0, s, P.ea_tasks.as<EaTask>() + R.begin,
+                                            R.count, P.srel.as<int32_t>(), pan, ua);
+      kt.end(s);
+    }
+    if (L.small_count > 0) {
+      kt.begin(kKcSmallFront, s);
+      launch(k_small_fronts<kSmallFront>, L.small_count, kSmallThreads, 0, s, 
+          P.small_list.as<int32_t>() + L.small_begin, P.sfirst.as<int64_t>(),
+          P.srowptr.as<int64_t>(), P.slofs.as<int64_t>(), P.uofs.as<int64_t>(),
+          P.child_ptr.as<int64_t>(), P.child_list.as<int32_t>(),
+          P.srel.as<int32_t>(), pan, ua, D.as<float>(), Dinv.as<float>(), st);
+      kt.end(s);
+    }
+    for (const auto &stp : L.steps) {
+      const StepDesc *dd = P.steps.as<StepDesc>() + stp.begin;
+      kt.begin(kKcDiag, s);
+      launch(k_diag_block, stp.count, kDiagThreads, diag_smem, s, 
+          dd, pan, linv.as<float>(), D.as<float>(), Dinv.as<float>(), st);
+      kt.end(s);
+      if (stp.trsm_tiles > 0) {
+        kt.begin(kKcTrsm, s);
+        launch(k_step_gemm<true>, stp.trsm_tiles, kGemmThreads, 0, s, 
+            dd, stp.count, pan, ua, linv.as<float>(), Dinv.as<float>());
+        kt.end(s);
+      }
+      if (stp.upd_tiles > 0) {
+        kt.begin(kKcUpdate, s);
+        launch(k_step_gemm<false>, stp.upd_tiles, kGemmThreads, 0, s, 
+            dd, stp.count, pan, ua, linv.as<float>(), Dinv.as<float>());
+        kt.end(s);
+      }
+    }
+    MPIR_CHECK_LAUNCH();
+  }
+  valid = true;
+}
+
+int64_t Numeric::result(cudaStream_t s, int32_t *zero_col, bool *nonfinite) const {
+  FactorStatus h;
+  MPIR_CUDA(cudaMemcpyAsync(&h, status.as<void>(), sizeof h, cudaMemcpyDeviceToHost, s));
+  MPIR_CUDA(cudaStreamSynchronize(s));
+  if (zero_col) *zero_col = h.zero_pivot;
+  if (nonfinite) *nonfinite = h.nonfinite != 0;
+  if (h.zero_pivot != INT_MAX) return -1;
+  return h.npos;
+}
+
+// ---------------------------------------------------------------------------
+int64_t &launch_counter() {
+  static int64_t c = 0;
+  return c;
+}
+
+KernelTimer &kernel_timer() {
+  static KernelTimer t;
+  return t;
+}
+
+void KernelTimer::begin(int c, cudaStream_t s) {
+  if (!enabled) return;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  cudaEventRecord(a, s);
+  ev.push_back(a);
+  ev.push_back(b);
+  cls.push_back(c);
+}
+
+void KernelTimer::end(cudaStream_t s) {
+  if (!enabled) return;
+  cudaEventRecord(ev.back(), s);
+}
+
+void KernelTimer::reset() {
+  for (auto e : ev) cudaEventDestroy(e);
+  ev.clear();
+  cls.clear();
+}
+
+void KernelTimer::collect(double *ms, int64_t *count, int nclass) {
+  for (int c = 0; c < nclass; c++) {
+    ms[c]    = 0;
+    count[c] = 0;
+  }
+  for (size_t i = 0; i < cls.size(); i++) {
+    float t = 0;
+    cudaEventElapsedTime(&t, ev[2 * i], ev[2 * i + 1]);
+    if (cls[i] < nclass) {
+      ms[cls[i]] += t;
+      count[cls[i]] += 1;
+    }
+  }
+}
+
+}  // namespace mpir

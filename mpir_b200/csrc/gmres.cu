@@ -1,0 +1,320 @@
+// GMRES-IR on the device: GmresLDLIR::Solve (gmres_ir.hpp:536-634) and
+// PrecondGmres (gmres_ir.hpp:636-741) with the supernodal LDL^T factor as the
+// left preconditioner.  Vectors and the Arnoldi basis are float64 in the
+// permuted order; the host keeps the small Hessenberg least-squares problem
+// and its Givens rotations, reading back one column of H per inner step.
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "solver.hpp"
+
+namespace mpir {
+
+double eps_of(int prec) {
+  switch (prec) {
+    case kF64: return DBL_EPSILON;
+    case kF32: return FLT_EPSILON;
+    case kBF16: return 0.0078125;          // 2^-7
+    case kF16: return 0.0009765625;        // 2^-10
+    case kDD: return 4.93038065763132e-32;  // 2^-104
+  }
+  return DBL_EPSILON;
+}
+
+Solver::Solver(int uf_, int uw_, int ur_, int dev)
+    : device(dev), uf(uf_), uw(uw_), ur(ur_) {
+  MPIR_CUDA(cudaSetDevice(device));
+  MPIR_CUDA(cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking));
+  stream_ = own_stream_;
+  MPIR_CUDA(cudaEventCreate(&ev0_));
+  MPIR_CUDA(cudaEventCreate(&ev1_));
+}
+
+Solver::~Solver() {
+  cudaSetDevice(device);
+  if (own_stream_) cudaStreamSynchronize(own_stream_);
+  if (ev0_) cudaEventDestroy(ev0_);
+  if (ev1_) cudaEventDestroy(ev1_);
+  plan_.reset();
+  if (own_stream_) cudaStreamDestroy(own_stream_);
+}
+
+int Solver::analyze(int64_t n, const int64_t *Ap, const int64_t *Ai,
+                    const double *Ax, int ordering) {
+  MPIR_CUDA(cudaSetDevice(device));
+  std::vector<int8_t> sign;
+  if (Ax) {
+    sign.assign(n, 0);
+    for (int64_t j = 0; j < n; j++)
+      for (int64_t p = Ap[j]; p < Ap[j + 1]; p++)
+        if (Ai[p] == j && Ax[p] > 0) sign[j] = 1;
+  }
+  Symbolic    S;
+  std::string err;
+  const int   rc = mpir::analyze(n, Ap, Ai, Ax ? sign.data() : nullptr,
+                                 static_cast<Ordering>(ordering), S, err);
+  if (rc != kOk) throw std::invalid_argument(err.empty() ? "analysis failed" : err);
+  auto P = std::make_unique<Plan>();
+  P->build(std::move(S), stream_);
+  plan_ = std::move(P);
+  num_.allocate(*plan_);
+  ws_.allocate(*plan_);
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  vec_.allocate(n, sms);
+  vec_m_ = -1;
+  return kOk;
+}
+
+void Solver::ensure_vectors() {
+  const int64_t n = plan_->S.n, m = std::max<int64_t>(std::min(gmres_iter, n), 1);
+  if (vec_m_ == m) return;
+  const size_t vb = std::max<int64_t>(n, 1) * sizeof(double);
+  V_.resize(vb * (m + 1));
+  bs_.resize(vb);
+  bp_.resize(vb);
+  ADp_.resize(vb);
+  x_.resize(vb);
+  r_.resize(vb);
+  t_.resize(vb);
+  d_.resize(vb);
+  hb_.resize(vb);
+  hx_.resize(vb);
+  hd_.resize(sizeof(double) * 2 * (m + 4));
+  y_.resize(sizeof(double) * (m + 1));
+  vec_m_ = m;
+}
+
+int Solver::factor_device(const double *d_Ax) {
+  if (!plan_) throw std::logic_error("factor before analyze");
+  MPIR_CUDA(cudaSetDevice(device));
+  MPIR_CUDA(cudaEventRecord(ev0_, stream_));
+  num_.run(*plan_, d_Ax, eps_of(uf), stream_);
+  MPIR_CUDA(cudaEventRecord(ev1_, stream_));
+  int32_t zc  = 0;
+  bool    bad = false;
+  last_npos   = num_.result(stream_, &zc, &bad);
+  float ms    = 0;
+  MPIR_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
+  last_factor_ms = ms;
+  if (last_npos < 0) {
+    num_.valid = false;
+    return kBadInput;
+  }
+  return kOk;
+}
+
+int Solver::factor(const double *Ax) {
+  if (!plan_) throw std::logic_error("factor before analyze");
+  MPIR_CUDA(cudaSetDevice(device));
+  MPIR_CUDA(cudaMemcpyAsync(num_.Ax.as<void>(), Ax, plan_->S.nnz * sizeof(double),
+                            cudaMemcpyHostToDevice, stream_));
+  return factor_device(num_.Ax.as<double>());
+}
+
+// PrecondGmres, gmres_ir.hpp:636-741.
+void Solver::precond_gmres(const double *b, double *res, Report &st) {
+  const Plan   &P  = *plan_;
+  const int64_t n  = P.S.n;
+  cudaStream_t  s  = stream_;
+  gmres_iter       = std::min<int64_t>(gmres_iter, n);  // gmres_ir.hpp:643
+  const int64_t m  = gmres_iter;
+  double       *V  = V_.as<double>();
+  double       *hd = hd_.as<double>();
+  const int64_t *Kp = P.Kp.as<int64_t>();
+  const int32_t *Kj = P.Kj.as<int32_t>();
+  const double  *Kv = num_.Kval.as<double>();
+  MPIR_CUDA(cudaMemsetAsync(res, 0, n * sizeof(double), s));
+  auto read = [&](double *h, int first, int cnt) {
+    MPIR_CUDA(cudaMemcpyAsync(h, hd + first, cnt * sizeof(double), cudaMemcpyDeviceToHost, s));
+    MPIR_CUDA(cudaStreamSynchronize(s));
+  };
+  double rho;
+  vec_.mgs_pass(const_cast<double *>(b), nullptr, nullptr, nullptr, 1, hd, s);
+  read(&rho, 0, 1);
+  if (rho < tol) return;
+  MPIR_CUDA(cudaMemcpyAsync(V, b, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  ldlt_solve(P, num_, V, ws_, s);
+  st.precond_applies++;
+  vec_.mgs_pass(V, nullptr, nullptr, nullptr, 1, hd, s);
+  read(&rho, 0, 1);
+  vec_.scale(V, 1 / rho, V, s);
+
+  std::vector<double> H((m + 1) * std::max<int64_t>(m, 1), 0.0), g(m + 1, 0.0),
+      c(std::max<int64_t>(m, 1), 0.0), sn(std::max<int64_t>(m, 1), 0.0),
+      col(m + 2, 0.0);
+  auto h = [&](int64_t i, int64_t j) -> double & { return H[i * std::max<int64_t>(m, 1) + j]; };
+  g[0] = rho;
+  int64_t k;
+  for (k = 0; k < m && rho > tol; k++) {
+    double *vk = V + k * n, *w = V + (k + 1) * n;
+    vec_.spmv(Kp, Kj, Kv, vk, w, s);
+    st.spmv_count++;
+    ldlt_solve(P, num_, w, ws_, s);
+    st.precond_applies++;
+    double *hn = hd + (m + 2);  // normav
+    vec_.mgs_pass(w, nullptr, nullptr, nullptr, 1, hn, s);
+    vec_.mgs_pass(w, nullptr, nullptr, V, 0, hd, s);
+    for (int64_t j = 0; j <= k; j++)
+      vec_.mgs_pass(w, V + j * n, hd + j, j < k ? V + (j + 1) * n : nullptr, j < k ? 0 : 1,
+                    hd + j + 1, s);
+    read(col.data(), 0, static_cast<int>(k + 2));
+    double normav;
+    read(&normav, static_cast<int>(m + 2), 1);
+    for (int64_t j = 0; j <= k + 1; j++) h(j, k) = col[j];
+    const double normav2 = h(k + 1, k);
+    if (normav + 0.001 * normav2 == normav) {  // Brown/Hindmarsh, gmres_ir.hpp:683
+      st.reorth_count++;
+      double *h2 = hd + (m + 4);  // second bank is hd[m+4 .. 2m+8)
+      vec_.mgs_pass(w, nullptr, nullptr, V, 0, h2, s);
+      for (int64_t j = 0; j <= k; j++)
+        vec_.mgs_pass(w, V + j * n, h2 + j, j < k ? V + (j + 1) * n : nullptr, j < k ? 0 : 1,
+                      h2 + j + 1, s);
+      read(col.data(), static_cast<int>(m + 4), static_cast<int>(k + 2));
+      for (int64_t j = 0; j <= k; j++) h(j, k) += col[j];
+      h(k + 1, k) = col[k + 1];
+    }
+    if (h(k + 1, k) != 0) vec_.scale(w, 1 / h(k + 1, k), w, s);
+    for (int64_t j = 0; j < k; j++) {  // apply previous rotations
+      const double w1 = c[j] * h(j, k) - sn[j] * h(j + 1, k);
+      const double w2 = sn[j] * h(j, k) + c[j] * h(j + 1, k);
+      h(j, k)         = w1;
+      h(j + 1, k)     = w2;
+    }
+    // Dnrm2 of {h_kk, h_k+1,k}, walked last to first as ops.hpp:243 does.
+    double nu;
+    {
+      double scale = 0.0, ssq = 1.0;
+      const double pr[2] = {h(k, k), h(k + 1, k)};
+      for (int q = 1; q >= 0; q--)
+        if (pr[q] != 0.0) {
+          const double a = std::fabs(pr[q]);
+          if (scale < a) {
+            ssq   = 1.0 + ssq * ((scale / a) * (scale / a));
+            scale = a;
+          } else {
+            ssq = ssq + ((a / scale) * (a / scale));
+          }
+        }
+      nu = scale * std::sqrt(ssq);
+    }
+    if (nu != 0) {
+      c[k]            = h(k, k) / nu;
+      sn[k]           = -h(k + 1, k) / nu;
+      h(k, k)         = c[k] * h(k, k) - sn[k] * h(k + 1, k);
+      h(k + 1, k)     = 0.0;
+      const double w1 = c[k] * g[k] - sn[k] * g[k + 1];
+      const double w2 = sn[k] * g[k] + c[k] * g[k + 1];
+      g[k]            = w1;
+      g[k + 1]        = w2;
+    }
+    rho = std::fabs(g[k + 1]);
+  }
+  st.gmres_iterations += static_cast<int32_t>(k);
+  std::vector<double> y(std::max<int64_t>(k, 1), 0.0);
+  for (int64_t i = k; i-- > 0;) {
+    y[i] = g[i];
+    for (int64_t j = i + 1; j < k; j++) y[i] -= h(i, j) * y[j];
+    y[i] /= h(i, i);
+  }
+  if (k > 0) {
+    MPIR_CUDA(cudaMemcpyAsync(y_.as<double>(), y.data(), k * sizeof(double),
+                              cudaMemcpyHostToDevice, s));
+    vec_.combine(V, n, static_cast<int>(k), y_.as<double>(), res, s);
+    MPIR_CUDA(cudaStreamSynchronize(s));  // y lives on the host stack
+  }
+}
+
+// GmresLDLIR::Solve, gmres_ir.hpp:536-634.
+int Solver::solve_device(const double *d_b, double *d_x, Report *rep) {
+  if (!plan_) throw std::logic_error("solve before analyze");
+  if (!num_.valid) throw std::logic_error("solve before a successful factor");
+  MPIR_CUDA(cudaSetDevice(device));
+  ensure_vectors();
+  Report        st;
+  const Plan   &P = *plan_;
+  const int64_t n = P.S.n;
+  cudaStream_t  s = stream_;
+  MPIR_CUDA(cudaEventRecord(ev0_, s));
+  const int64_t *Kp = P.Kp.as<int64_t>();
+  const int32_t *Kj = P.Kj.as<int32_t>();
+  const double  *Kv = num_.Kval.as<double>();
+  double *bs = bs_.as<double>(), *x = x_.as<double>(), *r = r_.as<double>(),
+         *t = t_.as<double>(), *d = d_.as<double>();
+  const bool dd = ur == kDD;
+  if (n == 0) {
+    if (rep) *rep = st;
+    return kOk;
+  }
+  vec_.rhs_in(P.perm.as<int64_t>(), num_.AD.as<double>(), d_b, bs, ADp_.as<double>(),
+              bp_.as<double>(), s);
+  double bs_inf;
+  vec_.read_inf(&bs_inf, 3, 1, s);
+  precond_gmres(bs, x, st);
+  vec_.residual(Kp, Kj, Kv, x, bs, r, dd, 0, s);
+  st.spmv_count++;
+  double r_inf;
+  vec_.read_inf(&r_inf, 0, 1, s);
+  double r_prev = DBL_MAX, r_norm = r_inf / bs_inf;
+  const double eps_w = eps_of(uw);
+  for (int64_t iter = 1; iter <= ir_iter; iter++) {
+    const double scale = r_inf;
+    if (scale == 0.0) {  // exact: nothing left to refine
+      st.stop_reason = 3;
+      break;
+    }
+    vec_.scale(r, 1.0 / scale, t, s);
+    precond_gmres(t, d, st);
+    vec_.ir_update(d, scale, x, s);
+    double nrm[2];
+    vec_.read_inf(nrm, 1, 2, s);
+    vec_.residual(Kp, Kj, Kv, x, bs, r, dd, 0, s);
+    st.spmv_count++;
+    vec_.read_inf(&r_inf, 0, 1, s);
+    r_norm           = r_inf / bs_inf;
+    st.ir_iterations = static_cast<int32_t>(iter);
+    if (nrm[0] <= nrm[1] * (10 * eps_w)) {
+      st.stop_reason = 1;
+      break;
+    }
+    if (std::fabs(r_norm - r_prev) < tol) {
+      st.stop_reason = 2;
+      break;
+    }
+    r_prev = r_norm;
+  }
+  st.residual_norm = r_norm;
+  vec_.sol_out(P.perm.as<int64_t>(), ADp_.as<double>(), x, d_x, s);
+  vec_.backward_terms(Kp, Kj, num_.Korig.as<double>(), x, ADp_.as<double>(),
+                      bp_.as<double>(), s);
+  double be[4];
+  vec_.read_inf(be, 4, 4, s);
+  const double den  = be[1] * be[2] + be[3];
+  st.backward_error = den > 0 ? be[0] / den : be[0];
+  MPIR_CUDA(cudaEventRecord(ev1_, s));
+  MPIR_CUDA(cudaEventSynchronize(ev1_));
+  float ms = 0;
+  MPIR_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
+  st.solve_ms  = ms;
+  st.factor_ms = last_factor_ms;
+  if (rep) *rep = st;
+  return kOk;
+}
+
+int Solver::solve(const double *b, double *x, Report *rep) {
+  if (!plan_) throw std::logic_error("solve before analyze");
+  MPIR_CUDA(cudaSetDevice(device));
+  ensure_vectors();
+  const int64_t n = plan_->S.n;
+  MPIR_CUDA(cudaMemcpyAsync(hb_.as<void>(), b, n * sizeof(double), cudaMemcpyHostToDevice,
+                            stream_));
+  const int rc = solve_device(hb_.as<double>(), hx_.as<double>(), rep);
+  MPIR_CUDA(cudaMemcpyAsync(x, hx_.as<void>(), n * sizeof(double), cudaMemcpyDeviceToHost,
+                            stream_));
+  MPIR_CUDA(cudaStreamSynchronize(stream_));
+  return rc;
+}
+
+}  // namespace mpir

@@ -1,0 +1,313 @@
+// Triangular solves with the supernodal LDL^T factor on the GPU.
+//
+// Computes x <- L^{-T} D^{-1} L^{-1} x, the preconditioner application that
+// QDLDL_solve performs column by column (qdldl.hpp:362-432), level by level
+// over the supernodal elimination tree:
+//   forward   each front takes its own right-hand side entries plus its
+//             children's update vectors, solves with its unit-lower diagonal
+//             block and leaves L_{R,J} x_J (negated, accumulated) as its own
+//             update vector for its parent;
+//   diagonal  x <- Dinv .* x;
+//   backward  each front gathers the finished x of its row set R_J and solves
+//             with L_J^T, last column block first.
+// Small fronts use one warp each; large fronts run column-block steps batched
+// over the level, reusing the inverses of the diagonal blocks kept by the
+// factorization so the diagonal solves become small dense products.  Vectors
+// are float64, the factor float32 (widened on load), as QDLDL_solve with
+// FACTPREC = float and XPREC = double.  Reductions have a fixed order, so
+// results do not depend on scheduling.
+#include "common.cuh"
+#include "engine.hpp"
+#include "solve.hpp"
+
+namespace mpir {
+
+constexpr int kWarpsPerCta = 4;
+constexpr int kSmallH      = kSmallFront;
+
+// ---------------------------------------------------------------------------
+// Forward
+__global__ void __launch_bounds__(32 * kWarpsPerCta)
+    k_fwd_small(const int32_t *list, int count, const int64_t *sfirst,
+                const int64_t *srowptr, const int64_t *slofs,
+                const int64_t *child_ptr, const int32_t *child_list,
+                const int32_t *srel, const int64_t *zofs, const float *panel,
+                double *x, double *zbuf) {
+  __shared__ double zs[kWarpsPerCta][kSmallH];
+  const int         warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int         idx  = blockIdx.x * kWarpsPerCta + warp;
+  if (idx >= count) return;
+  const int      J = list[idx];
+  const int64_t  f = sfirst[J];
+  const int      w = static_cast<int>(sfirst[J + 1] - f);
+  const int      h = static_cast<int>(srowptr[J + 1] - srowptr[J]);
+  double        *z = zs[warp];
+  for (int i = lane; i < h; i += 32) z[i] = i < w ? x[f + i] : 0.0;
+  __syncwarp();
+  for (int64_t c = child_ptr[J]; c < child_ptr[J + 1]; c++) {
+    const int      C  = child_list[c];
+    const int      wc = static_cast<int>(sfirst[C + 1] - sfirst[C]);
+    const int      rc = static_cast<int>(srowptr[C + 1] - srowptr[C]) - wc;
+    const int32_t *rl = srel + srowptr[C] + wc;
+    const double  *zc = zbuf + zofs[C] + wc;
+    for (int a = lane; a < rc; a += 32) z[rl[a]] += zc[a];
+    __syncwarp();
+  }
+  const float *P = panel + slofs[J];
+  for (int k = 0; k < w; k++) {
+    const double zk = z[k];
+    for (int i = k + 1 + lane; i < h; i += 32)
+      z[i] -= static_cast<double>(P[i + (int64_t)k * h]) * zk;
+    __syncwarp();
+  }
+  double *zo = zbuf + zofs[J];
+  for (int i = lane; i < h; i += 32) {
+    if (i < w) x[f + i] = z[i];
+    zo[i] = z[i];
+  }
+}
+
+// Large fronts: right-hand side plus children's update vectors.
+__global__ void k_fwd_gather(const int32_t *list, const int64_t *sfirst,
+                             const int64_t *srowptr, const int64_t *child_ptr,
+                             const int32_t *child_list, const int32_t *srel,
+                             const int64_t *zofs, const double *x,
+                             double *zbuf) {
+  const int     J = list[blockIdx.x];
+  const int64_t f = sfirst[J];
+  const int64_t w = sfirst[J + 1] - f;
+  const int64_t h = srowptr[J + 1] - srowptr[J];
+  double       *z = zbuf + zofs[J];
+  for (int64_t i = threadIdx.x; i < h; i += blockDim.x) z[i] = i < w ? x[f + i] : 0.0;
+  __syncthreads();
+  for (int64_t c = child_ptr[J]; c < child_ptr[J + 1]; c++) {
+    const int      C  = child_list[c];
+    const int64_t  wc = sfirst[C + 1] - sfirst[C];
+    const int64_t  rc = srowptr[C + 1] - srowptr[C] - wc;
+    const int32_t *rl = srel + srowptr[C] + wc;
+    const double  *zc = zbuf + zofs[C] + wc;
+    for (int64_t a = threadIdx.x; a < rc; a += blockDim.x) z[rl[a]] += zc[a];
+    __syncthreads();
+  }
+}
+
+// One column block of the large fronts: y = Linv z_b (every CTA of the desc
+// recomputes it), the desc's first CTA stores y into x, and each CTA updates
+// its rows below the block: z_r -= L_{r,b} y.
+__global__ void __launch_bounds__(kSolveRows)
+    k_fwd_step(const StepDesc *descs, int ndesc, const float *panel,
+               const float *linv, double *x, double *zbuf) {
+  __shared__ double zb[kNB], y[kNB];
+  const int         t  = blockIdx.x;
+  int               lo = 0, hi = ndesc - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    if (descs[mid].fsolve_tile0 <= t) lo = mid; else hi = mid - 1;
+  }
+  const StepDesc d     = descs[lo];
+  const int      local = t - d.fsolve_tile0;
+  const int      tid   = threadIdx.x;
+  const int64_t  h     = d.h;
+  double        *z     = zbuf + d.zofs;
+  const float   *Lv    = linv + d.linv;
+  if (tid < d.nbk) zb[tid] = z[d.kb + tid];
+  __syncthreads();
+  if (tid < d.nbk) {
+    double acc = 0.0;
+    for (int j = 0; j <= tid; j++)
+      acc += static_cast<double>(Lv[tid + j * kNB]) * zb[j];
+    y[tid] = acc;
+  }
+  __syncthreads();
+  if (local == 0 && tid < d.nbk) x[(int64_t)d.col0 + d.kb + tid] = y[tid];
+  const int64_t r = (int64_t)d.kb + d.nbk + (int64_t)local * kSolveRows + tid;
+  if (r < h) {
+    const float *P   = panel + d.panel + r + (int64_t)d.kb * h;
+    double       acc = z[r];
+    for (int k = 0; k < d.nbk; k++)
+      acc -= static_cast<double>(P[(int64_t)k * h]) * y[k];
+    z[r] = acc;
+  }
+}
+
+__global__ void k_dscale(int64_t n, const float *Dinv, double *x) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) x[i] *= static_cast<double>(Dinv[i]);
+}
+
+// ---------------------------------------------------------------------------
+// Backward
+__global__ void __launch_bounds__(32 * kWarpsPerCta)
+    k_bwd_small(const int32_t *list, int count, const int64_t *sfirst,
+                const int64_t *srowptr, const int32_t *srows,
+                const int64_t *slofs, const float *panel, double *x) {
+  __shared__ double zs[kWarpsPerCta][kSmallH];
+  const int         warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int         idx  = blockIdx.x * kWarpsPerCta + warp;
+  if (idx >= count) return;
+  const int      J  = list[idx];
+  const int64_t  f  = sfirst[J];
+  const int      w  = static_cast<int>(sfirst[J + 1] - f);
+  const int      h  = static_cast<int>(srowptr[J + 1] - srowptr[J]);
+  const int32_t *rw = srows + srowptr[J];
+  double        *z  = zs[warp];
+  for (int i = lane; i < h; i += 32) z[i] = i < w ? x[f + i] : x[rw[i]];
+  __syncwarp();
+  const float *P = panel + slofs[J];
+  for (int k = w - 1; k >= 0; k--) {
+    double s = 0.0;
+    for (int i = k + 1 + lane; i < h; i += 32)
+      s += static_cast<double>(P[i + (int64_t)k * h]) * z[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) z[k] -= s;
+    __syncwarp();
+  }
+  for (int i = lane; i < w; i += 32) x[f + i] = z[i];
+}
+
+__global__ void k_bwd_gather(const int32_t *list, const int64_t *sfirst,
+                             const int64_t *srowptr, const int32_t *srows,
+                             const int64_t *zofs, const double *x,
+                             double *zbuf) {
+  const int      J  = list[blockIdx.x];
+  const int64_t  f  = sfirst[J];
+  const int64_t  w  = sfirst[J + 1] - f;
+  const int64_t  h  = srowptr[J + 1] - srowptr[J];
+  const int32_t *rw = srows + srowptr[J];
+  double        *z  = zbuf + zofs[J];
+  for (int64_t i = threadIdx.x; i < h; i += blockDim.x)
+    z[i] = i < w ? x[f + i] : x[rw[i]];
+}
+
+// One column block, backward: partial sums t_k = sum_r L_{r,kb+k} z_r over a
+// chunk of rows below the block; the last chunk to finish adds the partials
+// in chunk order and solves x_b = Linv^T (z_b - t).
+__global__ void __launch_bounds__(kSolveChunk)
+    k_bwd_step(const StepDesc *descs, int ndesc, const float *panel,
+               const float *linv, double *x, double *zbuf, double *part,
+               int32_t *counter) {
+  __shared__ double zr[kSolveChunk];
+  __shared__ double v[kNB];
+  __shared__ int    last;
+  const int         t  = blockIdx.x;
+  int               lo = 0, hi = ndesc - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    if (descs[mid].bsolve_chunk0 <= t) lo = mid; else hi = mid - 1;
+  }
+  const StepDesc d     = descs[lo];
+  const int      chunk = t - d.bsolve_chunk0;
+  const int      tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+  const int64_t  h   = d.h;
+  double        *z   = zbuf + d.zofs;
+  const int64_t  r0  = (int64_t)d.kb + d.nbk + (int64_t)chunk * kSolveChunk;
+  const int64_t  r1  = min(r0 + kSolveChunk, h);
+  zr[tid]            = r0 + tid < r1 ? z[r0 + tid] : 0.0;
+  __syncthreads();
+  const float *P  = panel + d.panel;
+  double      *pp = part + d.bpart + (int64_t)chunk * kNB;
+  for (int k = warp; k < d.nbk; k += kSolveChunk / 32) {
+    const float *col = P + (int64_t)(d.kb + k) * h;
+    double       s   = 0.0;
+    for (int64_t r = r0 + lane; r < r1; r += 32)
+      s += static_cast<double>(col[r]) * zr[r - r0];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) pp[k] = s;
+  }
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) last = atomicAdd(counter + d.id, 1) == d.bsolve_chunks - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (tid < d.nbk) {
+    double s = 0.0;
+    for (int c = 0; c < d.bsolve_chunks; c++)
+      s += __ldcg(part + d.bpart + (int64_t)c * kNB + tid);
+    v[tid] = z[d.kb + tid] - s;
+  }
+  __syncthreads();
+  if (tid < d.nbk) {
+    const float *Lv  = linv + d.linv;
+    double       acc = 0.0;
+    for (int i = tid; i < d.nbk; i++)
+      acc += static_cast<double>(Lv[i + tid * kNB]) * v[i];
+    z[d.kb + tid]                    = acc;
+    x[(int64_t)d.col0 + d.kb + tid] = acc;
+  }
+}
+
+// ---------------------------------------------------------------------------
+void SolveWorkspace::allocate(const Plan &P) {
+  zbuf.resize(std::max<int64_t>(P.S.z_elems, 1) * sizeof(double));
+  part.resize(std::max<int64_t>(P.bpart_elems, 1) * sizeof(double));
+  counters.resize(std::max<int64_t>(P.ndesc, 1) * sizeof(int32_t));
+}
+
+void ldlt_solve(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
+                cudaStream_t s, int phases) {
+  const Symbolic &S  = P.S;
+  KernelTimer    &kt = kernel_timer();
+  if (S.n == 0) return;
+  const float *pan  = F.panel.as<float>();
+  const float *lv   = F.linv.as<float>();
+  double      *zbuf = ws.zbuf.as<double>();
+  const int    nl   = static_cast<int>(P.levels.size());
+  kt.begin(kKcSolveFwd, s);
+  for (int t = 0; t < nl && (phases & kForward); t++) {
+    const LevelPlan &L = P.levels[t];
+    if (L.small_count > 0)
+      launch(k_fwd_small, (L.small_count + kWarpsPerCta - 1) / kWarpsPerCta,
+                    32 * kWarpsPerCta, 0, s, 
+          P.small_list.as<int32_t>() + L.small_begin, L.small_count,
+          P.sfirst.as<int64_t>(), P.srowptr.as<int64_t>(), P.slofs.as<int64_t>(),
+          P.child_ptr.as<int64_t>(), P.child_list.as<int32_t>(),
+          P.srel.as<int32_t>(), P.zofs.as<int64_t>(), pan, x, zbuf);
+    if (L.large_count > 0) {
+      launch(k_fwd_gather, L.large_count, 256, 0, s, 
+          P.large_list.as<int32_t>() + L.large_begin, P.sfirst.as<int64_t>(),
+          P.srowptr.as<int64_t>(), P.child_ptr.as<int64_t>(),
+          P.child_list.as<int32_t>(), P.srel.as<int32_t>(), P.zofs.as<int64_t>(),
+          x, zbuf);
+      for (const auto &st : L.steps)
+        launch(k_fwd_step, st.fsolve_tiles, kSolveRows, 0, s, 
+            P.steps.as<StepDesc>() + st.begin, st.count, pan, lv, x, zbuf);
+    }
+  }
+  if (phases & kDiagonal)
+    launch(k_dscale, static_cast<unsigned>((S.n + 255) / 256), 256, 0, s, 
+        S.n, F.Dinv.as<float>(), x);
+  kt.end(s);
+  if (!(phases & kBackward)) return;
+  MPIR_CHECK_LAUNCH();
+  kt.begin(kKcSolveBwd, s);
+  MPIR_CUDA(cudaMemsetAsync(ws.counters.as<void>(), 0,
+                            std::max<int64_t>(P.ndesc, 1) * sizeof(int32_t), s));
+  for (int t = nl - 1; t >= 0; t--) {
+    const LevelPlan &L = P.levels[t];
+    if (L.small_count > 0)
+      launch(k_bwd_small, (L.small_count + kWarpsPerCta - 1) / kWarpsPerCta,
+                    32 * kWarpsPerCta, 0, s, 
+          P.small_list.as<int32_t>() + L.small_begin, L.small_count,
+          P.sfirst.as<int64_t>(), P.srowptr.as<int64_t>(), P.srows.as<int32_t>(),
+          P.slofs.as<int64_t>(), pan, x);
+    if (L.large_count > 0) {
+      launch(k_bwd_gather, L.large_count, 256, 0, s, 
+          P.large_list.as<int32_t>() + L.large_begin, P.sfirst.as<int64_t>(),
+          P.srowptr.as<int64_t>(), P.srows.as<int32_t>(), P.zofs.as<int64_t>(), x,
+          zbuf);
+      for (size_t q = L.steps.size(); q-- > 0;) {
+        const auto &st = L.steps[q];
+        launch(k_bwd_step, st.bsolve_chunks, kSolveChunk, 0, s, 
+            P.steps.as<StepDesc>() + st.begin, st.count, pan, lv, x, zbuf,
+            ws.part.as<double>(), ws.counters.as<int32_t>());
+      }
+    }
+  }
+  kt.end(s);
+  MPIR_CHECK_LAUNCH();
+}
+
+}  // namespace mpir

@@ -1,0 +1,79 @@
+// GMRES-IR solver object behind the C ABI: one analysed pattern, one numeric
+// factor, the GMRES basis and the refinement vectors, all on one device.
+#pragma once
+#include <memory>
+#include <stdexcept>
+
+#include "engine.hpp"
+#include "solve.hpp"
+#include "vec.hpp"
+
+namespace mpir {
+
+enum Prec : int { kF64 = 0, kF32 = 1, kBF16 = 2, kF16 = 3, kDD = 4 };
+
+struct Report {
+  int32_t status           = 0;
+  int32_t ir_iterations    = 0;
+  int32_t gmres_iterations = 0;
+  int32_t precond_applies  = 0;
+  int32_t spmv_count       = 0;
+  int32_t reorth_count     = 0;
+  int32_t stop_reason      = 0;  // 0 max iterations, 1 small update,
+                                 // 2 stagnation, 3 exact residual
+  int32_t pad              = 0;
+  double  residual_norm    = 0;
+  double  backward_error   = 0;
+  double  factor_ms        = 0;
+  double  solve_ms         = 0;
+};
+
+class Solver {
+ public:
+  Solver(int uf, int uw, int ur, int device);
+  ~Solver();
+
+  int  device;
+  int  uf, uw, ur;
+  int64_t ir_iter    = 10;    // gmres_ir.hpp:113-114
+  int64_t gmres_iter = 10;    // gmres_ir.hpp:115-116 (clamped to n on use)
+  double  tol        = 1e-10; // gmres_ir.hpp:117
+
+  // Host entry points (caller arrays on the host, caller order).
+  int analyze(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *Ax,
+              int ordering);
+  int factor(const double *Ax);
+  int solve(const double *b, double *x, Report *rep);
+  // Device entry points (caller arrays already on this device).
+  int factor_device(const double *d_Ax);
+  int solve_device(const double *d_b, double *d_x, Report *rep);
+
+  void set_stream(cudaStream_t s) { stream_ = s ? s : own_stream_; }
+  cudaStream_t stream() const { return stream_; }
+
+  bool analyzed() const { return plan_ != nullptr; }
+  const Plan &plan() const {
+    if (!plan_) throw std::logic_error("no analysed pattern");
+    return *plan_;
+  }
+  const Numeric &numeric() const { return num_; }
+  double last_factor_ms = 0;
+  int64_t last_npos     = 0;
+
+ private:
+  void precond_gmres(const double *b, double *res, Report &st);
+  void ensure_vectors();
+
+  cudaStream_t          own_stream_ = nullptr, stream_ = nullptr;
+  std::unique_ptr<Plan> plan_;
+  Numeric               num_;
+  SolveWorkspace        ws_;
+  VecOps                vec_;
+  DeviceBuffer          V_, bs_, bp_, ADp_, x_, r_, t_, d_, hd_, y_, hb_, hx_;
+  int64_t               vec_m_ = -1;
+  cudaEvent_t           ev0_ = nullptr, ev1_ = nullptr;
+};
+
+double eps_of(int prec);
+
+}  // namespace mpir

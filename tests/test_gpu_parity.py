@@ -1,0 +1,181 @@
+"""GPU parity: the CUDA path through the C ABI against the oracle and the
+reference compiled from its headers, on the same seeded inputs.
+
+Tolerances: symbolic results bit-exact; the float32 L and D within 1e-5
+normwise relative of the reference's float32 QDLDL factor of the same matrix
+(the GPU factor adds in a different order); solves within 1e-10 normwise
+relative of the reference's solve with the same factor; the GMRES-IR
+solution at normwise backward error <= 1e-14."""
+import numpy as np
+import pytest
+
+import mpir_b200 as mp
+from mpir_b200 import kkt
+from helpers import permuted_upper, rel_norm_diff
+
+pytestmark = pytest.mark.gpu
+
+FLT_EPS = float(np.finfo(np.float32).eps)
+
+
+def small_systems():
+    yield "small2d", kkt.small2d()
+    yield "grid3d_10", kkt.grid3d(grid=10, seed=1)
+    yield "illcond3d_10", kkt.illcond3d(grid=10, seed=2)
+    yield "batch2d_32", kkt.batch2d(instances=1, grid=32, nrhs=1, seed=3)[0]
+
+
+# ---------------------------------------------------------------- QDLDL drop-in
+@pytest.mark.parametrize("name,s", list(small_systems())[:2])
+def test_qdldl_factor_matches_reference(ref_lib, name, s):
+    tot, Lnz, et = mp.QDLDL_etree(s.n, s.Ap, s.Ai)
+    st, Lp, Li, Lx, D, Dinv = mp.QDLDL_factor(s.n, s.Ap, s.Ai, s.Ax, Lnz, et)
+    rs, rLp, rLi, rLx, rD, rDinv = ref_lib.factor(s.n, s.Ap, s.Ai, s.Ax, np.float32)
+    assert st == rs
+    np.testing.assert_array_equal(Lp, rLp)
+    np.testing.assert_array_equal(Li, rLi)
+    assert rel_norm_diff(Lx, rLx) <= 1e-5
+    assert rel_norm_diff(D, rD) <= 1e-5
+    assert rel_norm_diff(Dinv, rDinv) <= 1e-5
+
+
+def test_qdldl_factor_permuted_and_16bit(ref_lib):
+    s = kkt.grid3d(grid=8, seed=7)
+    out = mp.analyze_host(s.Ap, s.Ai, s.Ax)
+    Cp, Ci, Cx = permuted_upper(s.n, s.Ap, s.Ai, s.Ax, out["perm"])
+    tot, Lnz, et = mp.QDLDL_etree(s.n, Cp, Ci)
+    st, Lp, Li, Lx, D, Dinv = mp.QDLDL_factor(s.n, Cp, Ci, Cx, Lnz, et)
+    rs, rLp, rLi, rLx, rD, rDinv = ref_lib.factor(s.n, Cp, Ci, Cx, np.float32)
+    assert st == rs
+    np.testing.assert_array_equal(Li, rLi)
+    assert rel_norm_diff(Lx, rLx) <= 1e-5
+    assert rel_norm_diff(D, rD) <= 1e-5
+    # 16-bit storage is the float32 factor rounded to nearest
+    import torch
+    for prec, tdt in (("bf16", torch.bfloat16), ("f16", torch.float16)):
+        st2, _, _, Lx2, D2, _ = mp.QDLDL_factor(s.n, Cp, Ci, Cx, Lnz, et, fact_prec=prec)
+        assert st2 == st
+        want = torch.from_numpy(Lx).to(tdt).view(torch.int16).numpy().view(np.uint16)
+        np.testing.assert_array_equal(Lx2, want)
+
+
+def test_qdldl_zero_pivot_and_errors():
+    Ap, Ai, Ax = np.array([0, 1, 3]), np.array([0, 0, 1]), np.array([1.0, 1.0, 1.0])
+    tot, Lnz, et = mp.QDLDL_etree(2, Ap, Ai)
+    assert mp.QDLDL_factor(2, Ap, Ai, Ax, Lnz, et)[0] == -1
+    with pytest.raises(mp.MpirError):
+        mp.QDLDL_factor(2, Ap, Ai, Ax, Lnz, et, fact_prec="f64")
+
+
+@pytest.mark.parametrize("name,s", list(small_systems())[:2])
+def test_qdldl_solve_matches_reference(ref_lib, name, s):
+    rs, Lp, Li, Lx, D, Dinv = ref_lib.factor(s.n, s.Ap, s.Ai, s.Ax, np.float32)
+    xr = ref_lib.solve(s.n, Lp, Li, Lx, Dinv, s.b)
+    x = s.b.copy()
+    mp.QDLDL_solve(s.n, Lp, Li, Lx, Dinv, x)
+    assert rel_norm_diff(x, xr) <= 1e-10
+    # float32 vectors
+    x32 = s.b.astype(np.float32)
+    mp.QDLDL_solve(s.n, Lp, Li, Lx, Dinv, x32)
+    xr32 = ref_lib.solve(s.n, Lp, Li, Lx, Dinv, s.b.astype(np.float32), xdtype=np.float32)
+    assert rel_norm_diff(x32, xr32) <= 1e-4
+
+
+# ---------------------------------------------------------------- GMRES-IR
+@pytest.mark.parametrize("name,s", list(small_systems()))
+def test_gmres_ir_matches_reference(ref_lib, name, s):
+    solver = mp.GmresLDLIR()
+    solver.Compute(s.Ap, s.Ai, s.Ax, 0)
+    x = solver.Solve(s.b)
+    rep = solver.last_report
+    be = kkt.backward_error(s.n, s.Ap, s.Ai, s.Ax, x, s.b)
+    assert be <= 1e-14, (be, rep)
+    assert rep["backward_error"] <= 1e-14
+    assert abs(rep["backward_error"] - be) <= 1e-15 + 0.5 * be
+    # the reference's GMRES-IR on the same ordering (its QDLDL on P K P^T)
+    sym = solver.symbolic()
+    perm = sym["perm"]
+    Cp, Ci, Cx = permuted_upper(s.n, s.Ap, s.Ai, s.Ax, perm)
+    bp = s.b[perm]
+    xr_p, AD, info = ref_lib.gmres_ir(s.n, Cp, Ci, Cx, bp)
+    xr = np.empty_like(xr_p)
+    xr[perm] = xr_p
+    fe_gpu = kkt.forward_error(x, s.x_true)
+    fe_ref = kkt.forward_error(xr, s.x_true)
+    assert fe_gpu <= max(10 * fe_ref, 1e-12), (fe_gpu, fe_ref)
+    assert np.max(np.abs(x - xr)) / np.max(np.abs(xr)) <= max(20 * fe_ref, 1e-12)
+
+
+def test_factor_matches_reference_on_scaled_permuted_matrix(oracle_lib, ref_lib):
+    s = kkt.grid3d(grid=10, seed=5)
+    solver = mp.GmresLDLIR()
+    solver.Compute(s.Ap, s.Ai, s.Ax)
+    sym = solver.symbolic()
+    AD, Axs = oracle_lib.scale(s.n, s.Ap, s.Ai, s.Ax, FLT_EPS)
+    Cp, Ci, Cx = permuted_upper(s.n, s.Ap, s.Ai, Axs, sym["perm"])
+    np.testing.assert_array_equal(sym["Cp"], Cp)
+    np.testing.assert_array_equal(sym["Ci"], Ci)
+    tot, Lnz, et = ref_lib.etree(s.n, Cp, Ci)
+    np.testing.assert_array_equal(sym["Lnz"], Lnz)
+    np.testing.assert_array_equal(sym["etree"], et)
+    Lp, Li, Lx, D, Dinv = solver.export_factor()
+    rs, rLp, rLi, rLx, rD, rDinv = ref_lib.factor(s.n, Cp, Ci, Cx, np.float32)
+    np.testing.assert_array_equal(Lp, rLp)
+    np.testing.assert_array_equal(Li, rLi)
+    assert rel_norm_diff(Lx, rLx) <= 1e-5
+    assert rel_norm_diff(D, rD) <= 1e-5
+
+
+def test_gmres_ir_settings_and_edges():
+    s = kkt.small2d()
+    solver = mp.GmresLDLIR()
+    solver.SetMaxIRIterations(0)
+    solver.SetMaxGmresIterations(30)
+    solver.SetTolerance(1e-14)
+    solver.Compute(s.Ap, s.Ai, s.Ax)
+    x0 = solver.Solve(s.b)  # GMRES only, no refinement step
+    assert solver.last_report["ir_iterations"] == 0
+    assert kkt.backward_error(s.n, s.Ap, s.Ai, s.Ax, x0, s.b) < 1e-10
+    assert solver.Solve(s.b[:-1]).size == 0  # size mismatch -> empty
+    # zero right-hand side
+    z = solver.Solve(np.zeros(s.n))
+    assert np.all(z == 0)
+    # new values on the same pattern
+    solver.SetMaxIRIterations(10)
+    Ax2 = s.Ax * 2.0
+    assert solver.factor(Ax2) == 0
+    x2 = solver.Solve(s.b)
+    np.testing.assert_allclose(x2, s.x_true / 2.0, rtol=0, atol=1e-10)
+
+
+def test_gmres_ir_double_double_residual():
+    s = kkt.illcond3d(grid=8, seed=11)
+    a = mp.GmresLDLIR(ur="f64")
+    a.Compute(s.Ap, s.Ai, s.Ax)
+    xa = a.Solve(s.b)
+    b = mp.GmresLDLIR(ur="dd")
+    b.Compute(s.Ap, s.Ai, s.Ax)
+    xb = b.Solve(s.b)
+    for x in (xa, xb):
+        assert kkt.backward_error(s.n, s.Ap, s.Ai, s.Ax, x, s.b) <= 1e-14
+
+
+def test_zero_pivot_reported():
+    # K = [[1, 1], [1, 1]] is singular: the factor hits D = 0.
+    Ap, Ai, Ax = np.array([0, 1, 3]), np.array([0, 0, 1]), np.array([1.0, 1.0, 1.0])
+    solver = mp.GmresLDLIR()
+    with pytest.raises(mp.MpirError) as e:
+        solver.Compute(Ap, Ai, Ax)
+    assert e.value.code == -1
+
+
+def test_tiny_systems():
+    for n in (1, 2, 3):
+        Ap = np.arange(n + 1)
+        Ai = np.arange(n)
+        Ax = np.arange(1.0, n + 1)
+        solver = mp.GmresLDLIR()
+        solver.Compute(Ap, Ai, Ax)
+        b = np.ones(n)
+        x = solver.Solve(b)
+        np.testing.assert_allclose(x, 1.0 / Ax, rtol=1e-15)
