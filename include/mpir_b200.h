@@ -131,8 +131,11 @@ int mpir_qdldl_ltsolve(int64_t n, const int64_t *Lp, const int64_t *Li,
 
 /* ---- GMRES-IR solver (replaces GmresLDLIR, gmres_ir.hpp:90-315) --------- */
 
-/* uf/uw/ur as MPIR_F* above.  Provided: uf = MPIR_F32, uw = MPIR_F64,
- * ur = MPIR_F64 or MPIR_DD. */
+/* uf/uw/ur as MPIR_F* above.  Provided: uf = MPIR_F32 (float32 factor),
+ * MPIR_BF16 or MPIR_F16 (factor whose trailing updates run on the tensor
+ * cores with 16-bit operands and float32 accumulation; panels, diagonal
+ * blocks and panel solves stay float32); uw = MPIR_F64; ur = MPIR_F64 or
+ * MPIR_DD. */
 int mpir_solver_create(mpir_solver *out, int uf, int uw, int ur, int device);
 int mpir_solver_destroy(mpir_solver s);
 

@@ -338,9 +338,9 @@ int mpir_solver_create(mpir_solver *out, int uf, int uw, int ur, int device) {
   return guard([&]() -> int {
     if (!out) return MPIR_ERR_ARGUMENT;
     *out = nullptr;
-    if (uf != kF32 || uw != kF64 || (ur != kF64 && ur != kDD))
+    if ((uf != kF32 && uf != kBF16 && uf != kF16) || uw != kF64 || (ur != kF64 && ur != kDD))
       throw StatusError(MPIR_ERR_UNSUPPORTED,
-                        "provided precisions: UF=F32, UW=F64, UR=F64 or DD");
+                        "provided precisions: UF=F32/BF16/F16, UW=F64, UR=F64 or DD");
     auto *h = new mpir_solver_s{nullptr};
     try {
       h->impl = new Solver(uf, uw, ur, device);
@@ -411,6 +411,7 @@ int mpir_solver_factor(mpir_solver s, const double *Ax) {
   return guard([&]() -> int {
     const int rc = s->impl->factor(Ax);
     if (rc == kBadInput) g_err = "zero pivot";
+    if (rc == MPIR_ERR_TIMEOUT) g_err = "a bounded device wait ran out";
     return rc;
   });
 }
@@ -420,6 +421,7 @@ int mpir_solver_factor_device(mpir_solver s, const double *d_Ax) {
   return guard([&]() -> int {
     const int rc = s->impl->factor_device(d_Ax);
     if (rc == kBadInput) g_err = "zero pivot";
+    if (rc == MPIR_ERR_TIMEOUT) g_err = "a bounded device wait ran out";
     return rc;
   });
 }

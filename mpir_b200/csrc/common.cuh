@@ -87,7 +87,7 @@ struct FactorStatus {
   int32_t zero_pivot;  // smallest column (permuted) with D == 0, or INT_MAX
   int32_t npos;        // number of positive D entries
   int32_t nonfinite;   // 1 if a non-finite D was produced
-  int32_t pad;
+  int32_t timeout;     // 1 if a bounded device wait ran out
 };
 
 constexpr int kSmallThreads = 256;

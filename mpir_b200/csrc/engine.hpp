@@ -95,7 +95,7 @@ class Plan {
   DeviceBuffer amap, arow, acol, diag_pos, Kp, Kj, Ksrc;
   DeviceBuffer sfirst, srowptr, srows, srel, slofs, uofs, zofs, child_ptr,
       child_list, perm;
-  DeviceBuffer small_list, large_list, steps, ea_tasks, zero_segs;
+  DeviceBuffer small_list, large_list, steps, ea_tasks, zero_segs, linv_ofs_d;
   std::vector<int32_t> h_small, h_large;
   std::vector<int64_t> linv_ofs;  // per supernode, -1 for small fronts
 
@@ -106,18 +106,27 @@ class Plan {
 // Numeric factor of one value set on a plan.
 class Numeric {
  public:
-  DeviceBuffer panel, uarena, linv, D, Dinv, status;
+  // linv: float32 inverses of the diagonal blocks (the factor's panel solve);
+  // linv64: the same inverses in float64 (the triangular solves).
+  DeviceBuffer panel, uarena, linv, linv64, D, Dinv, status;
   DeviceBuffer AD, Axs, Kval, Korig, Ax;
   double       eps_uf = 0;
   bool         valid  = false;
+  // Trailing-update engine: -1 float32 SIMT, 0 bfloat16 tensor cores,
+  // 1 3xTF32 tensor cores, 2 float16 tensor cores.
+  int          update_mode = -1;
 
   void allocate(const Plan &P);
   // Scale the caller's values (device, caller order), assemble and factor.
   void run(const Plan &P, const double *d_Ax, double eps_uf, cudaStream_t s);
-  // Reads the status; returns #positive D or -1 on a zero pivot.
+  // Reads the status; returns #positive D, -1 on a zero pivot or -5 when a
+  // bounded device wait ran out.
   int64_t result(cudaStream_t s, int32_t *zero_col = nullptr,
                  bool *nonfinite = nullptr) const;
 };
+
+void launch_update_tc(int mode, const StepDesc *descs, int ndesc, int tiles, float *panel,
+                      float *uarena, FactorStatus *st, cudaStream_t s);
 
 // Kernel-class timer used by the benchmark's roofline figures.
 struct KernelTimer {

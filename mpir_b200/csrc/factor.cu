@@ -196,24 +196,24 @@ __global__ void k_extend_add(const EaTask *tasks, int ntasks,
 // together with the inverse of its unit-lower factor (right-looking forward
 // substitution on the identity, done in the same sweep).
 __global__ void __launch_bounds__(kDiagThreads)
-    k_diag_block(const StepDesc *descs, float *panel, float *linv, float *D,
-                 float *Dinv, FactorStatus *st) {
-  extern __shared__ float sm[];
-  constexpr int           LD = kNB + 1;
-  float                  *F  = sm;
-  float                  *X  = sm + kNB * LD;
-  float                  *wv = X + kNB * LD;
-  __shared__ int          s_npos;
-  const StepDesc          d   = descs[blockIdx.x];
-  const int               n   = d.nbk;
-  const int64_t           h   = d.h;
-  const int               tid = threadIdx.x, bd = blockDim.x;
-  float                  *P   = panel + d.panel + d.kb + (int64_t)d.kb * h;
+    k_diag_block(const StepDesc *descs, float *panel, float *linv, double *linv64,
+                 float *D, float *Dinv, FactorStatus *st) {
+  extern __shared__ double smd[];
+  constexpr int            LD = kNB + 1;
+  double                  *X  = smd;                                      // float64
+  float                   *F  = reinterpret_cast<float *>(smd + kNB * LD);  // float32
+  float                   *wv = F + kNB * LD;
+  __shared__ int           s_npos;
+  const StepDesc           d   = descs[blockIdx.x];
+  const int                n   = d.nbk;
+  const int64_t            h   = d.h;
+  const int                tid = threadIdx.x, bd = blockDim.x;
+  float                   *P   = panel + d.panel + d.kb + (int64_t)d.kb * h;
   if (tid == 0) s_npos = 0;
   for (int idx = tid; idx < n * n; idx += bd) {
     const int i = idx % n, j = idx / n;
     F[i * LD + j] = i >= j ? P[i + (int64_t)j * h] : 0.0f;
-    X[i * LD + j] = i == j ? 1.0f : 0.0f;
+    X[i * LD + j] = i == j ? 1.0 : 0.0;
   }
   __syncthreads();
   int npos = 0;
@@ -230,9 +230,10 @@ __global__ void __launch_bounds__(kDiagThreads)
         F[i * LD + j] -= (wv[i] * dinv) * wv[j];
       }
     }
+    // Inverse of the stored (float32) unit-lower factor, in float64.
     for (int idx = tid; idx < m * (k + 1); idx += bd) {
       const int i = k + 1 + idx % m, j = idx / m;
-      X[i * LD + j] -= (wv[i] * dinv) * X[k * LD + j];
+      X[i * LD + j] -= static_cast<double>(wv[i] * dinv) * X[k * LD + j];
     }
     for (int i = k + 1 + tid; i < n; i += bd) F[i * LD + k] = wv[i] * dinv;
     if (tid == 0) {
@@ -244,14 +245,17 @@ __global__ void __launch_bounds__(kDiagThreads)
     __syncthreads();
   }
   if (tid == 0) atomicAdd(&st->npos, npos);
-  float *Lv = linv + d.linv;
+  float  *Lv = linv + d.linv;
+  double *Ld = linv64 + d.linv;
   for (int idx = tid; idx < kNB * kNB; idx += bd) {
     const int i = idx % kNB, j = idx / kNB;
     if (i < n && j < n) {
       if (i >= j) P[i + (int64_t)j * h] = F[i * LD + j];
-      Lv[i + j * kNB] = X[i * LD + j];
+      Lv[i + j * kNB] = static_cast<float>(X[i * LD + j]);
+      Ld[i + j * kNB] = X[i * LD + j];
     } else {
       Lv[i + j * kNB] = 0.0f;
+      Ld[i + j * kNB] = 0.0;
     }
   }
 }
@@ -385,46 +389,46 @@ __global__ void __launch_bounds__(kGemmThreads)
 }
 
 // Inverses of the unit-lower diagonal blocks of a factor that was supplied
-// rather than computed here (the QDLDL_solve entry point).
+// rather than computed here (the QDLDL_solve entry point), in float64.
 __global__ void __launch_bounds__(kDiagThreads)
-    k_invert_blocks(const StepDesc *descs, const float *panel, float *linv) {
-  extern __shared__ float sm[];
-  constexpr int           LD = kNB + 1;
-  float                  *F  = sm;
-  float                  *X  = sm + kNB * LD;
-  const StepDesc          d  = descs[blockIdx.x];
-  const int               n  = d.nbk;
-  const int64_t           h  = d.h;
-  const int               tid = threadIdx.x, bd = blockDim.x;
-  const float            *P   = panel + d.panel + d.kb + (int64_t)d.kb * h;
+    k_invert_blocks(const StepDesc *descs, const float *panel, double *linv64) {
+  extern __shared__ double smd[];
+  constexpr int            LD = kNB + 1;
+  double                  *X  = smd;
+  float                   *F  = reinterpret_cast<float *>(smd + kNB * LD);
+  const StepDesc           d  = descs[blockIdx.x];
+  const int                n  = d.nbk;
+  const int64_t            h  = d.h;
+  const int                tid = threadIdx.x, bd = blockDim.x;
+  const float             *P   = panel + d.panel + d.kb + (int64_t)d.kb * h;
   for (int idx = tid; idx < n * n; idx += bd) {
     const int i = idx % n, j = idx / n;
     F[i * LD + j] = i > j ? P[i + (int64_t)j * h] : 0.0f;
-    X[i * LD + j] = i == j ? 1.0f : 0.0f;
+    X[i * LD + j] = i == j ? 1.0 : 0.0;
   }
   __syncthreads();
   for (int k = 0; k < n; k++) {
     const int m = n - k - 1;
     for (int idx = tid; idx < m * (k + 1); idx += bd) {
       const int i = k + 1 + idx % m, j = idx / m;
-      X[i * LD + j] -= F[i * LD + k] * X[k * LD + j];
+      X[i * LD + j] -= static_cast<double>(F[i * LD + k]) * X[k * LD + j];
     }
     __syncthreads();
   }
-  float *Lv = linv + d.linv;
+  double *Ld = linv64 + d.linv;
   for (int idx = tid; idx < kNB * kNB; idx += bd) {
     const int i = idx % kNB, j = idx / kNB;
-    Lv[i + j * kNB] = (i < n && j < n) ? X[i * LD + j] : 0.0f;
+    Ld[i + j * kNB] = (i < n && j < n) ? X[i * LD + j] : 0.0;
   }
 }
 
 void invert_diag_blocks(const Plan &P, Numeric &F, cudaStream_t s) {
   if (P.ndesc == 0) return;
-  const int smem = 2 * kNB * (kNB + 1) * sizeof(float);
+  const int smem = kNB * (kNB + 1) * (sizeof(double) + sizeof(float));
   MPIR_CUDA(cudaFuncSetAttribute(k_invert_blocks,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  launch(k_invert_blocks, static_cast<unsigned>(P.ndesc), kDiagThreads, smem, s, 
-      P.steps.as<StepDesc>(), F.panel.as<float>(), F.linv.as<float>());
+  launch(k_invert_blocks, static_cast<unsigned>(P.ndesc), kDiagThreads, smem, s,
+         P.steps.as<StepDesc>(), F.panel.as<float>(), F.linv64.as<double>());
   MPIR_CHECK_LAUNCH();
 }
 
@@ -598,6 +602,7 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
   steps      = upload(descs, s);
   ea_tasks   = upload(tasks, s);
   zero_segs  = upload(segs, s);
+  linv_ofs_d = upload(linv_ofs, s);
   MPIR_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -606,6 +611,7 @@ void Numeric::allocate(const Plan &P) {
   panel.resize(std::max<int64_t>(S.panel_elems, 1) * sizeof(float));
   uarena.resize(std::max<int64_t>(S.uarena_elems, 1) * sizeof(float));
   linv.resize(std::max<int64_t>(P.linv_elems, 1) * sizeof(float));
+  linv64.resize(std::max<int64_t>(P.linv_elems, 1) * sizeof(double));
   D.resize(std::max<int64_t>(S.n, 1) * sizeof(float));
   Dinv.resize(std::max<int64_t>(S.n, 1) * sizeof(float));
   status.resize(sizeof(FactorStatus));
@@ -643,7 +649,7 @@ void Numeric::run(const Plan &P, const double *d_Ax, double eps, cudaStream_t s)
   kt.end(s);
   MPIR_CHECK_LAUNCH();
   static bool attr = false;
-  const int   diag_smem = (2 * kNB * (kNB + 1) + kNB) * sizeof(float);
+  const int   diag_smem = kNB * (kNB + 1) * (sizeof(double) + sizeof(float)) + kNB * sizeof(float);
   if (!attr) {
     MPIR_CUDA(cudaFuncSetAttribute(k_diag_block,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -678,7 +684,7 @@ void Numeric::run(const Plan &P, const double *d_Ax, double eps, cudaStream_t s)
       const StepDesc *dd = P.steps.as<StepDesc>() + stp.begin;
       kt.begin(kKcDiag, s);
       launch(k_diag_block, stp.count, kDiagThreads, diag_smem, s, 
-          dd, pan, linv.as<float>(), D.as<float>(), Dinv.as<float>(), st);
+          dd, pan, linv.as<float>(), linv64.as<double>(), D.as<float>(), Dinv.as<float>(), st);
       kt.end(s);
       if (stp.trsm_tiles > 0) {
         kt.begin(kKcTrsm, s);
@@ -688,8 +694,11 @@ void Numeric::run(const Plan &P, const double *d_Ax, double eps, cudaStream_t s)
       }
       if (stp.upd_tiles > 0) {
         kt.begin(kKcUpdate, s);
-        launch(k_step_gemm<false>, stp.upd_tiles, kGemmThreads, 0, s, 
-            dd, stp.count, pan, ua, linv.as<float>(), Dinv.as<float>());
+        if (update_mode < 0)
+          launch(k_step_gemm<false>, stp.upd_tiles, kGemmThreads, 0, s, dd, stp.count, pan, ua,
+                 linv.as<float>(), Dinv.as<float>());
+        else
+          launch_update_tc(update_mode, dd, stp.count, stp.upd_tiles, pan, ua, st, s);
         kt.end(s);
       }
     }
@@ -704,6 +713,7 @@ int64_t Numeric::result(cudaStream_t s, int32_t *zero_col, bool *nonfinite) cons
   MPIR_CUDA(cudaStreamSynchronize(s));
   if (zero_col) *zero_col = h.zero_pivot;
   if (nonfinite) *nonfinite = h.nonfinite != 0;
+  if (h.timeout) return -5;
   if (h.zero_pivot != INT_MAX) return -1;
   return h.npos;
 }

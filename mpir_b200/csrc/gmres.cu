@@ -5,7 +5,9 @@
 // and its Givens rotations, reading back one column of H per inner step.
 #include <cfloat>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "solver.hpp"
@@ -21,6 +23,21 @@ double eps_of(int prec) {
     case kDD: return 4.93038065763132e-32;  // 2^-104
   }
   return DBL_EPSILON;
+}
+
+// Trailing-update engine for a factor type: float32 runs float32 SIMT
+// products, bfloat16 / float16 factors single-pass tensor-core products in
+// that type; MPIR_UPDATE ("simt", "tf32x3", "bf16", "f16") overrides.
+static int update_mode_for(int uf) {
+  int mode = uf == kBF16 ? 0 : uf == kF16 ? 2 : -1;
+  if (const char *e = std::getenv("MPIR_UPDATE")) {
+    const std::string v(e);
+    if (v == "simt") mode = -1;
+    else if (v == "bf16") mode = 0;
+    else if (v == "tf32x3") mode = 1;
+    else if (v == "f16") mode = 2;
+  }
+  return mode;
 }
 
 Solver::Solver(int uf_, int uw_, int ur_, int dev)
@@ -60,6 +77,7 @@ int Solver::analyze(int64_t n, const int64_t *Ap, const int64_t *Ai,
   P->build(std::move(S), stream_);
   plan_ = std::move(P);
   num_.allocate(*plan_);
+  num_.update_mode = update_mode_for(uf);
   ws_.allocate(*plan_);
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -101,7 +119,7 @@ int Solver::factor_device(const double *d_Ax) {
   last_factor_ms = ms;
   if (last_npos < 0) {
     num_.valid = false;
-    return kBadInput;
+    return last_npos == -5 ? -5 : kBadInput;
   }
   return kOk;
 }
@@ -136,7 +154,7 @@ void Solver::precond_gmres(const double *b, double *res, Report &st) {
   read(&rho, 0, 1);
   if (rho < tol) return;
   MPIR_CUDA(cudaMemcpyAsync(V, b, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-  ldlt_solve(P, num_, V, ws_, s);
+  ldlt_solve_graph(P, num_, V, ws_, s, own_stream_);
   st.precond_applies++;
   vec_.mgs_pass(V, nullptr, nullptr, nullptr, 1, hd, s);
   read(&rho, 0, 1);
@@ -152,7 +170,7 @@ void Solver::precond_gmres(const double *b, double *res, Report &st) {
     double *vk = V + k * n, *w = V + (k + 1) * n;
     vec_.spmv(Kp, Kj, Kv, vk, w, s);
     st.spmv_count++;
-    ldlt_solve(P, num_, w, ws_, s);
+    ldlt_solve_graph(P, num_, w, ws_, s, own_stream_);
     st.precond_applies++;
     double *hn = hd + (m + 2);  // normav
     vec_.mgs_pass(w, nullptr, nullptr, nullptr, 1, hn, s);

@@ -67,12 +67,13 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta)
   }
 }
 
-// Large fronts: right-hand side plus children's update vectors.
+// Large fronts: right-hand side plus children's update vectors, then the
+// solution of the first column block, y_0 = Linv_0 z_0, stored into x.
 __global__ void k_fwd_gather(const int32_t *list, const int64_t *sfirst,
                              const int64_t *srowptr, const int64_t *child_ptr,
                              const int32_t *child_list, const int32_t *srel,
-                             const int64_t *zofs, const double *x,
-                             double *zbuf) {
+                             const int64_t *zofs, const int64_t *linv_ofs,
+                             const double *linv64, double *x, double *zbuf) {
   const int     J = list[blockIdx.x];
   const int64_t f = sfirst[J];
   const int64_t w = sfirst[J + 1] - f;
@@ -89,15 +90,24 @@ __global__ void k_fwd_gather(const int32_t *list, const int64_t *sfirst,
     for (int64_t a = threadIdx.x; a < rc; a += blockDim.x) z[rl[a]] += zc[a];
     __syncthreads();
   }
+  const int     nb = static_cast<int>(w < kNB ? w : kNB);
+  const double *Lv = linv64 + linv_ofs[J];
+  if (threadIdx.x < nb) {
+    const int i   = threadIdx.x;
+    double    acc = 0.0;
+    for (int j = 0; j <= i; j++) acc += Lv[i + j * kNB] * z[j];
+    x[f + i] = acc;
+  }
 }
 
-// One column block of the large fronts: y = Linv z_b (every CTA of the desc
-// recomputes it), the desc's first CTA stores y into x, and each CTA updates
-// its rows below the block: z_r -= L_{r,b} y.
+// One column block of the large fronts.  The block's solution y is already
+// in x; each CTA updates its rows below the block, z_r -= L_{r,b} y.  The
+// first CTA's rows include the next block, so once they are updated it
+// solves that block, y' = Linv_{b+1} z_{b+1}, into x for the next step.
 __global__ void __launch_bounds__(kSolveRows)
     k_fwd_step(const StepDesc *descs, int ndesc, const float *panel,
-               const float *linv, double *x, double *zbuf) {
-  __shared__ double zb[kNB], y[kNB];
+               const double *linv64, double *x, double *zbuf) {
+  __shared__ double y[kNB];
   const int         t  = blockIdx.x;
   int               lo = 0, hi = ndesc - 1;
   while (lo < hi) {
@@ -109,17 +119,8 @@ __global__ void __launch_bounds__(kSolveRows)
   const int      tid   = threadIdx.x;
   const int64_t  h     = d.h;
   double        *z     = zbuf + d.zofs;
-  const float   *Lv    = linv + d.linv;
-  if (tid < d.nbk) zb[tid] = z[d.kb + tid];
+  if (tid < d.nbk) y[tid] = x[(int64_t)d.col0 + d.kb + tid];
   __syncthreads();
-  if (tid < d.nbk) {
-    double acc = 0.0;
-    for (int j = 0; j <= tid; j++)
-      acc += static_cast<double>(Lv[tid + j * kNB]) * zb[j];
-    y[tid] = acc;
-  }
-  __syncthreads();
-  if (local == 0 && tid < d.nbk) x[(int64_t)d.col0 + d.kb + tid] = y[tid];
   const int64_t r = (int64_t)d.kb + d.nbk + (int64_t)local * kSolveRows + tid;
   if (r < h) {
     const float *P   = panel + d.panel + r + (int64_t)d.kb * h;
@@ -127,6 +128,17 @@ __global__ void __launch_bounds__(kSolveRows)
     for (int k = 0; k < d.nbk; k++)
       acc -= static_cast<double>(P[(int64_t)k * h]) * y[k];
     z[r] = acc;
+  }
+  const int kn = d.kb + d.nbk;
+  if (local == 0 && kn < d.w) {
+    __syncthreads();
+    const int nb = d.w - kn < kNB ? d.w - kn : kNB;
+    if (tid < nb) {
+      const double *Lv  = linv64 + d.linv + (int64_t)kNB * kNB;
+      double        acc = 0.0;
+      for (int j = 0; j <= tid; j++) acc += Lv[tid + j * kNB] * z[kn + j];
+      x[(int64_t)d.col0 + kn + tid] = acc;
+    }
   }
 }
 
@@ -185,7 +197,7 @@ __global__ void k_bwd_gather(const int32_t *list, const int64_t *sfirst,
 // in chunk order and solves x_b = Linv^T (z_b - t).
 __global__ void __launch_bounds__(kSolveChunk)
     k_bwd_step(const StepDesc *descs, int ndesc, const float *panel,
-               const float *linv, double *x, double *zbuf, double *part,
+               const double *linv64, double *x, double *zbuf, double *part,
                int32_t *counter) {
   __shared__ double zr[kSolveChunk];
   __shared__ double v[kNB];
@@ -230,10 +242,9 @@ __global__ void __launch_bounds__(kSolveChunk)
   }
   __syncthreads();
   if (tid < d.nbk) {
-    const float *Lv  = linv + d.linv;
-    double       acc = 0.0;
-    for (int i = tid; i < d.nbk; i++)
-      acc += static_cast<double>(Lv[i + tid * kNB]) * v[i];
+    const double *Lv  = linv64 + d.linv;
+    double        acc = 0.0;
+    for (int i = tid; i < d.nbk; i++) acc += Lv[i + tid * kNB] * v[i];
     z[d.kb + tid]                    = acc;
     x[(int64_t)d.col0 + d.kb + tid] = acc;
   }
@@ -241,9 +252,42 @@ __global__ void __launch_bounds__(kSolveChunk)
 
 // ---------------------------------------------------------------------------
 void SolveWorkspace::allocate(const Plan &P) {
+  release_graph();
   zbuf.resize(std::max<int64_t>(P.S.z_elems, 1) * sizeof(double));
   part.resize(std::max<int64_t>(P.bpart_elems, 1) * sizeof(double));
   counters.resize(std::max<int64_t>(P.ndesc, 1) * sizeof(int32_t));
+  xbuf.resize(std::max<int64_t>(P.S.n, 1) * sizeof(double));
+}
+
+void SolveWorkspace::release_graph() {
+  if (graph) cudaGraphExecDestroy(graph);
+  graph = nullptr;
+}
+
+void ldlt_solve_graph(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
+                      cudaStream_t s, cudaStream_t capture_stream) {
+  const int64_t n = P.S.n;
+  if (n == 0) return;
+  if (kernel_timer().enabled) {  // per-class timing needs the plain launches
+    ldlt_solve(P, F, x, ws, s);
+    return;
+  }
+  if (!ws.graph) {
+    cudaGraph_t g = nullptr;
+    MPIR_CUDA(cudaStreamSynchronize(capture_stream));
+    MPIR_CUDA(cudaStreamBeginCapture(capture_stream, cudaStreamCaptureModeThreadLocal));
+    const int64_t before = launch_counter();
+    ldlt_solve(P, F, ws.xbuf.as<double>(), ws, capture_stream);
+    MPIR_CUDA(cudaStreamEndCapture(capture_stream, &g));
+    ws.graph_launches = launch_counter() - before;
+    launch_counter() = before;
+    MPIR_CUDA(cudaGraphInstantiate(&ws.graph, g, 0));
+    cudaGraphDestroy(g);
+  }
+  MPIR_CUDA(cudaMemcpyAsync(ws.xbuf.as<void>(), x, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  MPIR_CUDA(cudaGraphLaunch(ws.graph, s));
+  launch_counter() += ws.graph_launches;
+  MPIR_CUDA(cudaMemcpyAsync(x, ws.xbuf.as<void>(), n * sizeof(double), cudaMemcpyDeviceToDevice, s));
 }
 
 void ldlt_solve(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
@@ -252,7 +296,7 @@ void ldlt_solve(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
   KernelTimer    &kt = kernel_timer();
   if (S.n == 0) return;
   const float *pan  = F.panel.as<float>();
-  const float *lv   = F.linv.as<float>();
+  const double *lv  = F.linv64.as<double>();
   double      *zbuf = ws.zbuf.as<double>();
   const int    nl   = static_cast<int>(P.levels.size());
   kt.begin(kKcSolveFwd, s);
@@ -266,11 +310,11 @@ void ldlt_solve(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
           P.child_ptr.as<int64_t>(), P.child_list.as<int32_t>(),
           P.srel.as<int32_t>(), P.zofs.as<int64_t>(), pan, x, zbuf);
     if (L.large_count > 0) {
-      launch(k_fwd_gather, L.large_count, 256, 0, s, 
-          P.large_list.as<int32_t>() + L.large_begin, P.sfirst.as<int64_t>(),
-          P.srowptr.as<int64_t>(), P.child_ptr.as<int64_t>(),
-          P.child_list.as<int32_t>(), P.srel.as<int32_t>(), P.zofs.as<int64_t>(),
-          x, zbuf);
+      launch(k_fwd_gather, L.large_count, 256, 0, s,
+             P.large_list.as<int32_t>() + L.large_begin, P.sfirst.as<int64_t>(),
+             P.srowptr.as<int64_t>(), P.child_ptr.as<int64_t>(),
+             P.child_list.as<int32_t>(), P.srel.as<int32_t>(), P.zofs.as<int64_t>(),
+             P.linv_ofs_d.as<int64_t>(), lv, x, zbuf);
       for (const auto &st : L.steps)
         launch(k_fwd_step, st.fsolve_tiles, kSolveRows, 0, s, 
             P.steps.as<StepDesc>() + st.begin, st.count, pan, lv, x, zbuf);

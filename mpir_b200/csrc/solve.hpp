@@ -8,7 +8,12 @@ struct SolveWorkspace {
   DeviceBuffer zbuf;      // front vectors, zofs layout (doubles)
   DeviceBuffer part;      // backward partial sums (doubles)
   DeviceBuffer counters;  // backward completion counters, one per step desc
+  DeviceBuffer xbuf;      // fixed vector the captured solve works on
+  cudaGraphExec_t graph = nullptr;  // captured L D L^T solve (all phases)
+  int64_t graph_launches = 0;       // kernels one replay runs
   void allocate(const Plan &P);
+  void release_graph();
+  ~SolveWorkspace() { release_graph(); }
 };
 
 // Phases of the solve, combinable as bits.
@@ -18,5 +23,11 @@ enum SolvePhase : int { kForward = 1, kDiagonal = 2, kBackward = 4, kAllPhases =
 // selected: (L+I)^{-1} x, Dinv .* x, (L+I)^{-T} x (qdldl.hpp:362-432).
 void ldlt_solve(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
                 cudaStream_t s, int phases = kAllPhases);
+
+// The same full solve replayed from a CUDA graph captured on first use on
+// `capture_stream` (a non-default stream) and launched on `s`; x is copied
+// into and out of the workspace vector the graph was captured on.
+void ldlt_solve_graph(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
+                      cudaStream_t s, cudaStream_t capture_stream);
 
 }  // namespace mpir
