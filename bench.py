@@ -52,6 +52,10 @@ def parse():
     ap.add_argument("--cpu-budget", type=float, default=12.0,
                     help="seconds of reference factor sampling for the CPU baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--uf", default="f32", choices=["f32", "bf16", "f16"],
+                    help="factor precision (bf16/f16: 16-bit tensor-core updates)")
+    ap.add_argument("--gmres-iter", type=int, default=None)
+    ap.add_argument("--ir-iter", type=int, default=None)
     return ap.parse_args()
 
 
@@ -269,7 +273,10 @@ def run_gpu(args):
         return float(t.item())
 
     s = kkt.grid3d(seed=args.seed + rank, grid=args.grid)
-    solver = mp.GmresLDLIR(device=local)
+    solver = mp.GmresLDLIR(uf=args.uf, device=local)
+    low = args.uf != "f32"
+    solver.SetMaxGmresIterations(args.gmres_iter or (50 if low else 10))
+    solver.SetMaxIRIterations(args.ir_iter or (30 if low else 10))
     stream = torch.cuda.current_stream(dev)
     solver.set_stream(stream.cuda_stream)
     solver.analyze(s.Ap, s.Ai, s.Ax)
@@ -372,7 +379,7 @@ def run_gpu(args):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32 factor / f64 solve",
+        "scaling": "weak", "vs_baseline": None, "dtype": f"{args.uf} factor / f64 solve",
         "data": "synthetic (seeded KKT generator, one system per rank)",
         "config": {"workload": workload_name(args.grid), "global_batch": world,
                    "seq_len": None, "parallelism": f"replicas{world}",

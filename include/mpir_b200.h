@@ -59,7 +59,7 @@ typedef struct mpir_report {
   int32_t spmv_count;       /* products with K */
   int32_t reorth_count;     /* Brown/Hindmarsh re-orthogonalisations */
   int32_t stop_reason;      /* 0 iteration cap, 1 small update, 2 stagnation,
-                               3 zero residual */
+                               3 zero residual, 4 non-finite residual */
   int32_t pad;
   double residual_norm;  /* ||r||_inf / ||b_scaled||_inf at exit (gmres_ir.hpp:580) */
   double backward_error; /* ||b - Kx||_inf / (||K||_inf ||x||_inf + ||b||_inf) */

@@ -283,6 +283,10 @@ int Solver::solve_device(const double *d_b, double *d_x, Report *rep) {
       st.stop_reason = 3;
       break;
     }
+    if (!std::isfinite(scale)) {  // a non-finite factor or input
+      st.stop_reason = 4;
+      break;
+    }
     vec_.scale(r, 1.0 / scale, t, s);
     precond_gmres(t, d, st);
     vec_.ir_update(d, scale, x, s);

@@ -354,4 +354,5 @@ void ldlt_solve(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
   MPIR_CHECK_LAUNCH();
 }
 
+
 }  // namespace mpir

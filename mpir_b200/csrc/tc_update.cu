@@ -138,7 +138,7 @@ __global__ void __launch_bounds__(tc::kThreads)
   // Buffer layout: [buf][A parts][B parts], each kOperandBytes.
   __shared__ __align__(8) uint64_t mbar[2];
   __shared__ uint32_t tmem_slot;
-  __shared__ float    sd[kNB];
+  __shared__ float    sa[kNB], sb[kNB];
 
   const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
   // ---- locate the tile (same enumeration as the SIMT update kernel)
@@ -179,7 +179,20 @@ __global__ void __launch_bounds__(tc::kThreads)
   }
   const int m0 = (j + local) * kTileM;
   const int n0 = j * kTileN;
-  for (int k = tid; k < nbk; k += blockDim.x) sd[k] = Pp[(kb + k) + (int64_t)(kb + k) * h];
+  // Column scales of the two operands: (L D) L^T for 3xTF32; for 16-bit
+  // operands the balanced (L sqrt|D| sign D)(L sqrt|D|)^T, which keeps both
+  // within the 16-bit range when pivots are tiny and multipliers large.
+  for (int k = tid; k < nbk; k += blockDim.x) {
+    const float dk = Pp[(kb + k) + (int64_t)(kb + k) * h];
+    if (HALF) {
+      const float r = sqrtf(fabsf(dk));
+      sa[k]         = dk < 0.0f ? -r : r;
+      sb[k]         = r;
+    } else {
+      sa[k] = dk;
+      sb[k] = 1.0f;
+    }
+  }
 
   // ---- tensor memory and barriers
   if (warp == 0) {
@@ -214,8 +227,8 @@ __global__ void __launch_bounds__(tc::kThreads)
 #pragma unroll
     for (int k = 0; k < KC; k++) {
       const bool kin = k0 + k < nbk;
-      av[k] = (va && kin) ? A[ra + (int64_t)(k0 + k) * lda] * sd[k0 + k] : 0.0f;
-      bv[k] = (vb && kin) ? A[rb + (int64_t)(k0 + k) * lda] : 0.0f;
+      av[k] = (va && kin) ? A[ra + (int64_t)(k0 + k) * lda] * sa[k0 + k] : 0.0f;
+      bv[k] = (vb && kin) ? A[rb + (int64_t)(k0 + k) * lda] * sb[k0 + k] : 0.0f;
     }
     if (HALF) {
 #pragma unroll

@@ -179,3 +179,44 @@ def test_tiny_systems():
         b = np.ones(n)
         x = solver.Solve(b)
         np.testing.assert_allclose(x, 1.0 / Ax, rtol=1e-15)
+
+
+# ---------------------------------------------------------------- tensor cores
+@pytest.fixture
+def update_engine(monkeypatch):
+    def set_engine(name):
+        monkeypatch.setenv("MPIR_UPDATE", name)
+    return set_engine
+
+
+def test_tf32x3_update_matches_reference(oracle_lib, ref_lib, update_engine):
+    """3xTF32 tensor-core trailing updates keep the float32 factor within the
+    same 1e-5 of the reference's float32 QDLDL factor."""
+    update_engine("tf32x3")
+    s = kkt.grid3d(grid=12, seed=9)
+    solver = mp.GmresLDLIR()
+    solver.Compute(s.Ap, s.Ai, s.Ax)
+    sym = solver.symbolic()
+    AD, Axs = oracle_lib.scale(s.n, s.Ap, s.Ai, s.Ax, FLT_EPS)
+    Cp, Ci, Cx = permuted_upper(s.n, s.Ap, s.Ai, Axs, sym["perm"])
+    Lp, Li, Lx, D, Dinv = solver.export_factor()
+    rs, rLp, rLi, rLx, rD, rDinv = ref_lib.factor(s.n, Cp, Ci, Cx, np.float32)
+    np.testing.assert_array_equal(Li, rLi)
+    assert rel_norm_diff(Lx, rLx) <= 1e-5
+    assert rel_norm_diff(D, rD) <= 1e-5
+    x = solver.Solve(s.b)
+    assert kkt.backward_error(s.n, s.Ap, s.Ai, s.Ax, x, s.b) <= 1e-14
+
+
+@pytest.mark.parametrize("uf", ["bf16", "f16"])
+def test_low_precision_factor_tier_converges(uf):
+    """16-bit tensor-core trailing updates: a rougher preconditioner, same
+    float64 backward error after refinement."""
+    for s in (kkt.grid3d(grid=12, seed=4), kkt.illcond3d(grid=10, seed=5)):
+        solver = mp.GmresLDLIR(uf=uf)
+        solver.SetMaxGmresIterations(50)
+        solver.SetMaxIRIterations(30)
+        solver.Compute(s.Ap, s.Ai, s.Ax)
+        x = solver.Solve(s.b)
+        be = kkt.backward_error(s.n, s.Ap, s.Ai, s.Ax, x, s.b)
+        assert be <= 1e-14, (uf, be, solver.last_report)
