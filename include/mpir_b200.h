@@ -129,6 +129,25 @@ int mpir_qdldl_ltsolve(int64_t n, const int64_t *Lp, const int64_t *Li,
                        const void *Lx, int fact_prec, void *x, int x_prec,
                        int device);
 
+/* QDLDL_solve without device allocation (no counterpart in the reference).
+ * For callers that cannot call cudaMalloc: code that runs while a CUDA stream
+ * capture is open, where allocation is not allowed, and processes whose device
+ * memory is handed out entirely by their own pooling allocator.  Same
+ * arithmetic as mpir_qdldl_solve (float32 L and Dinv, float64 x, host
+ * arrays), but every device buffer it needs is carved out of one fixed 32 MiB
+ * array that each GPU holds for as long as the library is loaded.  Limits:
+ * every supernodal front of L has at most 64 rows, and the packed layout of
+ * L, Dinv, x and the fronts' update vectors fits 32 MiB; otherwise it
+ * returns MPIR_ERR_UNSUPPORTED or MPIR_ERR_ARGUMENT with a message and
+ * touches no device memory.  The first call on a device looks up the array's
+ * device address, so make it before any stream capture.  All calls share the
+ * array: calls that overlap on the GPU (other host threads, other streams)
+ * race and must be serialised by the caller.  Runs on the calling thread's
+ * per-thread default stream and returns when x is back on the host. */
+int mpir_qdldl_solve_noalloc(int64_t n, const int64_t *Lp, const int64_t *Li,
+                             const float *Lx, const float *Dinv, double *x,
+                             int device);
+
 /* ---- GMRES-IR solver (replaces GmresLDLIR, gmres_ir.hpp:90-315) --------- */
 
 /* uf/uw/ur as MPIR_F* above.  Provided: uf = MPIR_F32 (float32 factor),

@@ -86,6 +86,7 @@ def lib():
         "mpir_qdldl_etree": (i64, [i64, vp, vp, vp, vp, vp]),
         "mpir_qdldl_factor": (i64, [i64, vp, vp, vp, vp, vp, vp, vp, vp, i32, vp, vp, i32]),
         "mpir_qdldl_solve": (i32, [i64, vp, vp, vp, vp, i32, vp, i32, i32]),
+        "mpir_qdldl_solve_noalloc": (i32, [i64, vp, vp, vp, vp, vp, i32]),
         "mpir_solver_create": (i32, [vp, i32, i32, i32, i32]),
         "mpir_solver_destroy": (i32, [vp]),
         "mpir_solver_set_max_ir_iterations": (i32, [vp, i64]),
@@ -192,6 +193,21 @@ def QDLDL_solve(n, Lp, Li, Lx, Dinv, x, fact_prec="f32", device=0):
     Dinv = np.ascontiguousarray(Dinv)
     _check(lib().mpir_qdldl_solve(n, _p(_i64(Lp)), _p(_i64(Li)), _p(Lx), _p(Dinv), prec,
                                   _p(x), xp, device))
+    return x
+
+
+def QDLDL_solve_noalloc(n, Lp, Li, Lx, Dinv, x, device=0):
+    """QDLDL_solve for callers that cannot allocate device memory (inside an
+    open stream capture, or under a process-wide pooling allocator): float32
+    factor, float64 x in place; all device data lives in the library's fixed
+    32 MiB array.  Fronts of at most 64 rows; raises MpirError beyond the
+    limits.  Calls overlapping on the GPU share that array and race."""
+    if x.dtype != np.float64 or not x.flags["C_CONTIGUOUS"]:
+        raise ValueError("x must be contiguous float64")
+    Lx = np.ascontiguousarray(Lx, dtype=np.float32)
+    Dinv = np.ascontiguousarray(Dinv, dtype=np.float32)
+    _check(lib().mpir_qdldl_solve_noalloc(n, _p(_i64(Lp)), _p(_i64(Li)), _p(Lx), _p(Dinv),
+                                          _p(x), device))
     return x
 
 

@@ -334,6 +334,17 @@ int mpir_qdldl_ltsolve(int64_t n, const int64_t *Lp, const int64_t *Li, const vo
   return qdldl_solve_phases(n, Lp, Li, Lx, nullptr, fact_prec, x, x_prec, device, kBackward);
 }
 
+int mpir_qdldl_solve_noalloc(int64_t n, const int64_t *Lp, const int64_t *Li, const float *Lx,
+                             const float *Dinv, double *x, int device) {
+  return guard([&]() -> int {
+    if (n > 0 && (!Lp || !Li || !Lx || !Dinv || !x)) return MPIR_ERR_ARGUMENT;
+    std::string err;
+    const int   rc = qdldl_solve_noalloc(n, Lp, Li, Lx, Dinv, x, device, err);
+    if (rc != MPIR_OK) throw StatusError(rc, err);
+    return MPIR_OK;
+  });
+}
+
 int mpir_solver_create(mpir_solver *out, int uf, int uw, int ur, int device) {
   return guard([&]() -> int {
     if (!out) return MPIR_ERR_ARGUMENT;

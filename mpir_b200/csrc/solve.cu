@@ -16,6 +16,9 @@
 // are float64, the factor float32 (widened on load), as QDLDL_solve with
 // FACTPREC = float and XPREC = double.  Reductions have a fixed order, so
 // results do not depend on scheduling.
+#include <string>
+#include <vector>
+
 #include "common.cuh"
 #include "engine.hpp"
 #include "solve.hpp"
@@ -354,5 +357,142 @@ void ldlt_solve(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
   MPIR_CHECK_LAUNCH();
 }
 
+
+// ---------------------------------------------------------------------------
+// QDLDL_solve without device allocation.
+//
+// For callers that cannot call cudaMalloc: code running while a CUDA stream
+// capture is open (allocation is not allowed there), and processes whose
+// device memory is handed out entirely by their own pooling allocator.  All
+// device data of this entry point (the supernodal layout of L, the factor
+// values, Dinv, the fronts' update vectors and x) is packed into the one
+// file-scope array below, of fixed size, that every GPU holds once this
+// library is loaded.  Only factors whose supernodal fronts have at most
+// kSmallFront rows are taken (the warp-per-front kernels; no diagonal-block
+// inverses), and the packed data must fit the array.
+namespace {
+constexpr size_t kNoAllocScratchBytes = size_t{32} << 20;  // 32 MiB
+constexpr int    kNoAllocMaxDevices   = 64;
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_solve_scratch[kNoAllocScratchBytes];
+
+namespace {
+// Device address of g_solve_scratch on each device, looked up on the first
+// call that uses that device.
+void *g_solve_scratch_addr[kNoAllocMaxDevices] = {};
+}  // namespace
+
+int qdldl_solve_noalloc(int64_t n, const int64_t *Lp, const int64_t *Li, const float *Lx,
+                        const float *Dinv, double *x, int device, std::string &err) {
+  if (n < 0 || device < 0 || device >= kNoAllocMaxDevices) {
+    err = "invalid dimension or device";
+    return kBadArgument;
+  }
+  if (n == 0) return kOk;
+  Symbolic  S;
+  const int rc = analyze_from_L(n, Lp, Li, S, err);
+  if (rc != kOk) return rc;
+  for (int64_t J = 0; J < S.ns; J++)
+    if (S.h(J) > kSmallFront) {
+      err = "a supernodal front has " + std::to_string(S.h(J)) + " rows; this entry point takes at most " +
+            std::to_string(kSmallFront);
+      return -7;
+    }
+  // Factor values in the panel layout (explicit zeros for padding).
+  std::vector<float> pan(S.panel_elems, 0.0f);
+  for (int64_t J = 0; J < S.ns; J++) {
+    const int64_t f = S.sfirst[J], l = S.sfirst[J + 1], w = l - f, h = S.h(J);
+    for (int64_t j = f; j < l; j++) {
+      int64_t q = S.srowptr[J] + w;  // rows below the supernode's own columns
+      for (int64_t p = Lp[j]; p < Lp[j + 1]; p++) {
+        const int64_t r = Li[p];
+        int64_t       lr;
+        if (r < l) {
+          lr = r - f;
+        } else {
+          while (S.srows[q] < r) q++;
+          lr = w + (q - S.srowptr[J] - w);
+        }
+        pan[S.slofs[J] + (j - f) * h + lr] = Lx[p];
+      }
+    }
+  }
+  // Pack every region into the scratch array, 256-byte aligned.
+  struct Region {
+    const void *src;
+    size_t      bytes;
+    size_t      ofs;
+  };
+  std::vector<Region> reg;
+  size_t              top = 0;
+  auto add = [&](const void *src, size_t bytes) {
+    top = (top + 255) / 256 * 256;
+    reg.push_back({src, bytes, top});
+    top += bytes;
+    return reg.size() - 1;
+  };
+  const size_t r_sfirst = add(S.sfirst.data(), S.sfirst.size() * sizeof(int64_t));
+  const size_t r_srowptr = add(S.srowptr.data(), S.srowptr.size() * sizeof(int64_t));
+  const size_t r_srows = add(S.srows.data(), S.srows.size() * sizeof(int32_t));
+  const size_t r_srel = add(S.srel.data(), S.srel.size() * sizeof(int32_t));
+  const size_t r_slofs = add(S.slofs.data(), S.slofs.size() * sizeof(int64_t));
+  const size_t r_cptr = add(S.child_ptr.data(), S.child_ptr.size() * sizeof(int64_t));
+  const size_t r_clist = add(S.child_list.data(), S.child_list.size() * sizeof(int32_t));
+  const size_t r_zofs = add(S.zofs.data(), S.zofs.size() * sizeof(int64_t));
+  const size_t r_level = add(S.level_sup.data(), S.level_sup.size() * sizeof(int32_t));
+  const size_t r_panel = add(pan.data(), pan.size() * sizeof(float));
+  const size_t r_dinv = add(Dinv, n * sizeof(float));
+  const size_t r_x = add(x, n * sizeof(double));
+  const size_t r_zbuf = add(nullptr, S.z_elems * sizeof(double));  // written on the device
+  if (top > kNoAllocScratchBytes) {
+    err = "needs " + std::to_string(top) + " bytes of device scratch; this entry point has " +
+          std::to_string(kNoAllocScratchBytes);
+    return kBadArgument;
+  }
+  MPIR_CUDA(cudaSetDevice(device));
+  if (!g_solve_scratch_addr[device]) {
+    void             *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_solve_scratch);
+    if (e != cudaSuccess) throw CudaError(e, "cudaGetSymbolAddress(g_solve_scratch)");
+    g_solve_scratch_addr[device] = p;
+  }
+  unsigned char     *base = static_cast<unsigned char *>(g_solve_scratch_addr[device]);
+  const cudaStream_t s    = cudaStreamPerThread;
+  for (const Region &r : reg)
+    if (r.src && r.bytes)
+      MPIR_CUDA(cudaMemcpyAsync(base + r.ofs, r.src, r.bytes, cudaMemcpyHostToDevice, s));
+  auto at = [&](size_t i) { return static_cast<void *>(base + reg[i].ofs); };
+  const int64_t *sfirst  = static_cast<const int64_t *>(at(r_sfirst));
+  const int64_t *srowptr = static_cast<const int64_t *>(at(r_srowptr));
+  const int32_t *srows   = static_cast<const int32_t *>(at(r_srows));
+  const int32_t *srel    = static_cast<const int32_t *>(at(r_srel));
+  const int64_t *slofs   = static_cast<const int64_t *>(at(r_slofs));
+  const int64_t *cptr    = static_cast<const int64_t *>(at(r_cptr));
+  const int32_t *clist   = static_cast<const int32_t *>(at(r_clist));
+  const int64_t *zofs    = static_cast<const int64_t *>(at(r_zofs));
+  const int32_t *level   = static_cast<const int32_t *>(at(r_level));
+  const float   *panel   = static_cast<const float *>(at(r_panel));
+  const float   *dinv    = static_cast<const float *>(at(r_dinv));
+  double        *xd      = static_cast<double *>(at(r_x));
+  double        *zbuf    = static_cast<double *>(at(r_zbuf));
+  const int      nl      = S.nlevels;
+  for (int t = 0; t < nl; t++) {
+    const int32_t cnt = static_cast<int32_t>(S.level_ptr[t + 1] - S.level_ptr[t]);
+    launch(k_fwd_small, (cnt + kWarpsPerCta - 1) / kWarpsPerCta, 32 * kWarpsPerCta, 0, s,
+           level + S.level_ptr[t], cnt, sfirst, srowptr, slofs, cptr, clist, srel, zofs, panel,
+           xd, zbuf);
+  }
+  launch(k_dscale, static_cast<unsigned>((n + 255) / 256), 256, 0, s, n, dinv, xd);
+  for (int t = nl - 1; t >= 0; t--) {
+    const int32_t cnt = static_cast<int32_t>(S.level_ptr[t + 1] - S.level_ptr[t]);
+    launch(k_bwd_small, (cnt + kWarpsPerCta - 1) / kWarpsPerCta, 32 * kWarpsPerCta, 0, s,
+           level + S.level_ptr[t], cnt, sfirst, srowptr, srows, slofs, panel, xd);
+  }
+  MPIR_CHECK_LAUNCH();
+  MPIR_CUDA(cudaMemcpyAsync(x, xd, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  MPIR_CUDA(cudaStreamSynchronize(s));
+  return kOk;
+}
 
 }  // namespace mpir

@@ -1,5 +1,7 @@
 // Triangular-solve workspace and entry point (solve.cu).
 #pragma once
+#include <string>
+
 #include "engine.hpp"
 
 namespace mpir {
@@ -29,5 +31,12 @@ void ldlt_solve(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
 // into and out of the workspace vector the graph was captured on.
 void ldlt_solve_graph(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
                       cudaStream_t s, cudaStream_t capture_stream);
+
+// QDLDL_solve (float32 factor, float64 x, host arrays) whose device data
+// lives in a fixed file-scope array instead of allocated memory; see
+// mpir_qdldl_solve_noalloc in include/mpir_b200.h.  Returns a status and a
+// message in err.
+int qdldl_solve_noalloc(int64_t n, const int64_t *Lp, const int64_t *Li, const float *Lx,
+                        const float *Dinv, double *x, int device, std::string &err);
 
 }  // namespace mpir
