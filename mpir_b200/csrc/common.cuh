@@ -64,6 +64,29 @@ struct StepDesc {
   int32_t id;
 };
 
+// One GEMM-shaped update of a front, C -= (A D) A^T restricted to N columns:
+//   C[r, c] -= sum_{k < K} A[r, k] D[k] A[c, k]   (r < M, c < N, c <= r if lower)
+// A is M x K inside a panel (leading dimension lda), D the K pivots at
+// D[d_ofs ...], C at c_ofs in the panels or in the update arena.  Used for
+// the left-looking block updates of a front's own columns (K = columns
+// eliminated so far) and for its update matrix (K = all its columns).  The
+// K range may be split across CTAs whose partial tiles go to a workspace and
+// are added in split order by a reduction launch.
+struct GemmProb {
+  int64_t a_ofs;   // panel offset of A(0, 0)
+  int64_t c_ofs;   // offset of C(0, 0)
+  int64_t d_ofs;   // index of D for column 0 of A
+  int64_t ws_ofs;  // float offset of the split partials, -1 when unsplit
+  int32_t lda, ldc;
+  int32_t M, N, K;
+  int32_t c_in_u;  // C lives in the update arena (else in the panels)
+  int32_t lower;
+  int32_t splits;
+  int32_t ntm, ntiles;  // row tiles; tiles of the (lower) tile pattern
+  int32_t tile0;   // first CTA of this problem in its GEMM launch
+  int32_t rtile0;  // first CTA of this problem in its reduction launch
+};
+
 // Extend-add task: add the lower triangle of child C's update matrix into
 // its parent's front, CTA-chunked by columns of U_C.
 struct EaTask {
@@ -95,7 +118,8 @@ constexpr int kDiagThreads  = 512;
 constexpr int kGemmThreads  = 256;
 constexpr int kEaChunk      = 8;     // U_C columns per extend-add CTA
 constexpr int64_t kZeroChunk = 16384;  // floats per zero-fill CTA
-constexpr int kSolveRows = 256;        // rows per forward-solve CTA
-constexpr int kSolveChunk = 256;       // rows per backward-solve CTA
+constexpr int kSolveRows = 128;        // rows per forward-solve CTA
+constexpr int kSolveChunk = 128;       // rows per backward-solve CTA
+constexpr int kSolveThreads = 512;     // 4 column quarters x 128 rows
 
 }  // namespace mpir

@@ -75,8 +75,12 @@ struct LevelPlan {
   std::vector<Round> ea_rounds;
   struct Step {
     int32_t begin, count, trsm_tiles, upd_tiles, fsolve_tiles, bsolve_chunks;
+    // left-looking update of this block column before its diagonal block
+    int32_t ll_begin, ll_count, ll_tiles, ll_rtiles;
   };
   std::vector<Step> steps;
+  // update matrices of the level's large fronts, after their last step
+  int32_t u_begin = 0, u_count = 0, u_tiles = 0, u_rtiles = 0;
   // Solve: large fronts' gather list = large list; small fronts handled by
   // one thread block each.
 };
@@ -95,7 +99,8 @@ class Plan {
   DeviceBuffer amap, arow, acol, diag_pos, Kp, Kj, Ksrc;
   DeviceBuffer sfirst, srowptr, srows, srel, slofs, uofs, zofs, child_ptr,
       child_list, perm;
-  DeviceBuffer small_list, large_list, steps, ea_tasks, zero_segs, linv_ofs_d;
+  DeviceBuffer small_list, large_list, steps, ea_tasks, zero_segs, linv_ofs_d, gemm_probs;
+  int64_t      ws_elems = 0;  // split-K partial tiles (floats)
   std::vector<int32_t> h_small, h_large;
   std::vector<int64_t> linv_ofs;  // per supernode, -1 for small fronts
 
@@ -107,8 +112,9 @@ class Plan {
 class Numeric {
  public:
   // linv: float32 inverses of the diagonal blocks (the factor's panel solve);
-  // linv64: the same inverses in float64 (the triangular solves).
-  DeviceBuffer panel, uarena, linv, linv64, D, Dinv, status;
+  // linv64: the same inverses in float64 (the triangular solves), column-major;
+  // linv64t: row-major copy of linv64 (the backward solve).
+  DeviceBuffer panel, uarena, linv, linv64, linv64t, D, Dinv, status, ws;
   DeviceBuffer AD, Axs, Kval, Korig, Ax;
   double       eps_uf = 0;
   bool         valid  = false;
@@ -125,8 +131,8 @@ class Numeric {
                  bool *nonfinite = nullptr) const;
 };
 
-void launch_update_tc(int mode, const StepDesc *descs, int ndesc, int tiles, float *panel,
-                      float *uarena, FactorStatus *st, cudaStream_t s);
+void launch_gemm_tc(int mode, const GemmProb *probs, int nprob, int tiles, float *panel,
+                    float *uarena, const float *D, float *ws, FactorStatus *st, cudaStream_t s);
 
 // Kernel-class timer used by the benchmark's roofline figures.
 struct KernelTimer {

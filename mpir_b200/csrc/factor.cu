@@ -196,46 +196,48 @@ __global__ void k_extend_add(const EaTask *tasks, int ntasks,
 // together with the inverse of its unit-lower factor (right-looking forward
 // substitution on the identity, done in the same sweep).
 __global__ void __launch_bounds__(kDiagThreads)
-    k_diag_block(const StepDesc *descs, float *panel, float *linv, double *linv64,
-                 float *D, float *Dinv, FactorStatus *st) {
-  extern __shared__ double smd[];
-  constexpr int            LD = kNB + 1;
-  double                  *X  = smd;                                      // float64
-  float                   *F  = reinterpret_cast<float *>(smd + kNB * LD);  // float32
-  float                   *wv = F + kNB * LD;
-  __shared__ int           s_npos;
-  const StepDesc           d   = descs[blockIdx.x];
-  const int                n   = d.nbk;
-  const int64_t            h   = d.h;
-  const int                tid = threadIdx.x, bd = blockDim.x;
-  float                   *P   = panel + d.panel + d.kb + (int64_t)d.kb * h;
+    k_diag_block(const StepDesc *descs, float *panel, float *linv, float *D, float *Dinv,
+                 FactorStatus *st) {
+  extern __shared__ float sm[];
+  constexpr int           LD = kNB + 1;
+  float                  *F  = sm;
+  float                  *X  = sm + kNB * LD;
+  float                  *wv = X + kNB * LD;
+  __shared__ int          s_npos;
+  const StepDesc          d   = descs[blockIdx.x];
+  const int               n   = d.nbk;
+  const int64_t           h   = d.h;
+  const int               tid = threadIdx.x, bd = blockDim.x;
+  float                  *P   = panel + d.panel + d.kb + (int64_t)d.kb * h;
   if (tid == 0) s_npos = 0;
   for (int idx = tid; idx < n * n; idx += bd) {
     const int i = idx % n, j = idx / n;
     F[i * LD + j] = i >= j ? P[i + (int64_t)j * h] : 0.0f;
-    X[i * LD + j] = i == j ? 1.0 : 0.0;
+    X[i * LD + j] = i == j ? 1.0f : 0.0f;
   }
   __syncthreads();
-  int npos = 0;
+  // Thread t owns row i = t % kNB and the columns j = t / kNB (mod 4): no
+  // index arithmetic per element and an even split of each rank-1 update.
+  static_assert(kDiagThreads == 4 * kNB, "diag kernel thread mapping");
+  const int ri = tid % kNB, cj = tid / kNB;
+  int       npos = 0;
   for (int k = 0; k < n; k++) {
     const float dk = F[k * LD + k];
-    for (int i = k + 1 + tid; i < n; i += bd) wv[i] = F[i * LD + k];
+    if (tid > k && tid < n) wv[tid] = F[tid * LD + k];
     __syncthreads();
     const float dinv = 1.0f / dk;
-    const int   m    = n - k - 1;
-    for (int idx = tid; idx < m * m; idx += bd) {
-      const int ii = idx % m, jj = idx / m;
-      if (ii >= jj) {
-        const int i = k + 1 + ii, j = k + 1 + jj;
-        F[i * LD + j] -= (wv[i] * dinv) * wv[j];
-      }
+    if (ri > k && ri < n) {
+      const float li = wv[ri] * dinv;
+      // trailing update, columns k < j <= i
+      int j0 = k + 1 + ((cj - (k + 1)) % 4 + 4) % 4;
+      for (int j = j0; j <= ri; j += 4) F[ri * LD + j] -= li * wv[j];
+      // inverse of the unit-lower factor (float32, for the panel solve;
+      // the float64 inverses the triangular solves use are formed after
+      // the whole factorization by k_invert_blocks): columns j <= k
+      for (int j = cj; j <= k; j += 4) X[ri * LD + j] -= li * X[k * LD + j];
     }
-    // Inverse of the stored (float32) unit-lower factor, in float64.
-    for (int idx = tid; idx < m * (k + 1); idx += bd) {
-      const int i = k + 1 + idx % m, j = idx / m;
-      X[i * LD + j] -= static_cast<double>(wv[i] * dinv) * X[k * LD + j];
-    }
-    for (int i = k + 1 + tid; i < n; i += bd) F[i * LD + k] = wv[i] * dinv;
+    __syncthreads();
+    if (ri > k && ri < n && cj == 0) F[ri * LD + k] = wv[ri] * dinv;
     if (tid == 0) {
       const int64_t col = (int64_t)d.col0 + d.kb + k;
       D[col]            = dk;
@@ -245,17 +247,14 @@ __global__ void __launch_bounds__(kDiagThreads)
     __syncthreads();
   }
   if (tid == 0) atomicAdd(&st->npos, npos);
-  float  *Lv = linv + d.linv;
-  double *Ld = linv64 + d.linv;
+  float *Lv = linv + d.linv;
   for (int idx = tid; idx < kNB * kNB; idx += bd) {
     const int i = idx % kNB, j = idx / kNB;
     if (i < n && j < n) {
       if (i >= j) P[i + (int64_t)j * h] = F[i * LD + j];
-      Lv[i + j * kNB] = static_cast<float>(X[i * LD + j]);
-      Ld[i + j * kNB] = X[i * LD + j];
+      Lv[i + j * kNB] = X[i * LD + j];
     } else {
       Lv[i + j * kNB] = 0.0f;
-      Ld[i + j * kNB] = 0.0;
     }
   }
 }
@@ -388,10 +387,132 @@ __global__ void __launch_bounds__(kGemmThreads)
   }
 }
 
-// Inverses of the unit-lower diagonal blocks of a factor that was supplied
-// rather than computed here (the QDLDL_solve entry point), in float64.
+// ---------------------------------------------------------------------------
+// GemmProb updates on the SIMT units (float32), the same tile and split
+// mapping as the tensor-core kernel.
+__device__ __forceinline__ void locate_tile(const GemmProb &pb, int local, int &sp, int &tile,
+                                            int &m0, int &n0) {
+  sp     = local % pb.splits;
+  int tl = local / pb.splits;
+  tile   = tl;
+  int j  = 0;
+  if (pb.lower) {
+    while (tl >= pb.ntm - j) {
+      tl -= pb.ntm - j;
+      j++;
+    }
+    m0 = (j + tl) * kBM;
+  } else {
+    j  = tl / pb.ntm;
+    m0 = (tl % pb.ntm) * kBM;
+  }
+  n0 = j * kBN;
+}
+
+__global__ void __launch_bounds__(kGemmThreads)
+    k_gemm_simt(const GemmProb *probs, int nprob, float *panel, float *uarena, const float *D,
+                float *ws) {
+  __shared__ float As[kBK][kBM];
+  __shared__ float Bs[kBK][kBN];
+  const int        t  = blockIdx.x;
+  int              lo = 0, hi = nprob - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    if (probs[mid].tile0 <= t) lo = mid; else hi = mid - 1;
+  }
+  const GemmProb pb = probs[lo];
+  int            sp, tile, m0, n0;
+  locate_tile(pb, t - pb.tile0, sp, tile, m0, n0);
+  const int     M = pb.M, N = pb.N, K = pb.K;
+  const int     ks   = ((K + pb.splits - 1) / pb.splits + 31) / 32 * 32;
+  const int     k_lo = sp * ks, k_hi = min(K, k_lo + ks);
+  const float  *A    = panel + pb.a_ofs;
+  const int64_t lda  = pb.lda;
+  const float  *Dk   = D + pb.d_ofs;
+  const int     tid  = threadIdx.x;
+  const int     tr = tid / 16, tc = tid % 16;
+  float         acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+#pragma unroll
+    for (int j = 0; j < 8; j++) acc[i][j] = 0.0f;
+  for (int k0 = k_lo; k0 < k_hi; k0 += kBK) {
+#pragma unroll
+    for (int q = 0; q < (kBM * kBK) / kGemmThreads; q++) {
+      const int idx = tid + q * kGemmThreads;
+      const int i = idx % kBM, kk = idx / kBM;
+      const int k = k0 + kk;
+      const bool kin = k < k_hi;
+      const int r = m0 + i, c = n0 + i;
+      As[kk][i] = (r < M && kin) ? A[r + (int64_t)k * lda] * Dk[k] : 0.0f;
+      Bs[kk][i] = (c < N && kin) ? A[c + (int64_t)k * lda] : 0.0f;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < kBK; kk++) {
+      float a[8], b[8];
+#pragma unroll
+      for (int i = 0; i < 8; i++) a[i] = As[kk][tr * 8 + i];
+#pragma unroll
+      for (int j = 0; j < 8; j++) b[j] = Bs[kk][tc * 8 + j];
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+  if (pb.splits > 1) {
+    float *W = ws + pb.ws_ofs + (static_cast<int64_t>(tile) * pb.splits + sp) * (kBM * kBN);
+#pragma unroll
+    for (int j = 0; j < 8; j++)
+#pragma unroll
+      for (int i = 0; i < 8; i++) W[(tr * 8 + i) + (tc * 8 + j) * kBM] = acc[i][j];
+    return;
+  }
+  float *C = (pb.c_in_u ? uarena : panel) + pb.c_ofs;
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    const int c = n0 + tc * 8 + j;
+    if (c >= N) continue;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const int r = m0 + tr * 8 + i;
+      if (r < M && (!pb.lower || r >= c)) C[r + (int64_t)c * pb.ldc] -= acc[i][j];
+    }
+  }
+}
+
+// C -= sum of the split partials of one tile, added in split order.
+__global__ void k_split_reduce(const GemmProb *probs, int nprob, float *panel, float *uarena,
+                               const float *ws) {
+  const int t  = blockIdx.x;
+  int       lo = 0, hi = nprob - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    if (probs[mid].rtile0 <= t) lo = mid; else hi = mid - 1;
+  }
+  const GemmProb pb = probs[lo];
+  int            sp, tile, m0, n0;
+  locate_tile(pb, (t - pb.rtile0) * pb.splits, sp, tile, m0, n0);
+  float       *C = (pb.c_in_u ? uarena : panel) + pb.c_ofs;
+  const float *W = ws + pb.ws_ofs + static_cast<int64_t>(tile) * pb.splits * (kBM * kBN);
+  for (int e = threadIdx.x; e < kBM * kBN; e += blockDim.x) {
+    const int r = m0 + e % kBM, c = n0 + e / kBM;
+    if (r >= pb.M || c >= pb.N || (pb.lower && r < c)) continue;
+    float acc = 0.0f;
+    for (int q = 0; q < pb.splits; q++) acc += W[static_cast<int64_t>(q) * (kBM * kBN) + e];
+    C[r + (int64_t)c * pb.ldc] -= acc;
+  }
+}
+
+// Inverses, in float64, of the unit-lower diagonal blocks of the large
+// fronts, for the triangular solves: run once after a factorization (off its
+// critical path), and for a factor supplied by the caller (the QDLDL_solve
+// entry point).
 __global__ void __launch_bounds__(kDiagThreads)
-    k_invert_blocks(const StepDesc *descs, const float *panel, double *linv64) {
+    k_invert_blocks(const StepDesc *descs, const float *panel, double *linv64,
+                    double *linv64t) {
   extern __shared__ double smd[];
   constexpr int            LD = kNB + 1;
   double                  *X  = smd;
@@ -415,10 +536,12 @@ __global__ void __launch_bounds__(kDiagThreads)
     }
     __syncthreads();
   }
-  double *Ld = linv64 + d.linv;
+  double *Ld = linv64 + d.linv, *Lt = linv64t + d.linv;
   for (int idx = tid; idx < kNB * kNB; idx += bd) {
-    const int i = idx % kNB, j = idx / kNB;
-    Ld[i + j * kNB] = (i < n && j < n) ? X[i * LD + j] : 0.0;
+    const int    i = idx % kNB, j = idx / kNB;
+    const double v = (i < n && j < n) ? X[i * LD + j] : 0.0;
+    Ld[i + j * kNB] = v;
+    Lt[i * kNB + j] = v;
   }
 }
 
@@ -428,7 +551,8 @@ void invert_diag_blocks(const Plan &P, Numeric &F, cudaStream_t s) {
   MPIR_CUDA(cudaFuncSetAttribute(k_invert_blocks,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   launch(k_invert_blocks, static_cast<unsigned>(P.ndesc), kDiagThreads, smem, s,
-         P.steps.as<StepDesc>(), F.panel.as<float>(), F.linv64.as<double>());
+         P.steps.as<StepDesc>(), F.panel.as<float>(), F.linv64.as<double>(),
+         F.linv64t.as<double>());
   MPIR_CHECK_LAUNCH();
 }
 
@@ -457,6 +581,49 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
   std::vector<StepDesc> descs;
   std::vector<EaTask>   tasks;
   std::vector<Segment>  segs;
+  std::vector<GemmProb> probs;
+  ws_elems = 0;
+  // Tiles, K splits, launch offsets and workspace of the problems
+  // [begin, begin + count) of one launch.  With fewer tiles than about two
+  // per SM, K is split (at least 256 per split) and the partials reduced.
+  auto finish_launch = [&](int32_t begin, int32_t count, int32_t &tiles, int32_t &rtiles) {
+    int64_t total = 0;
+    for (int32_t q = begin; q < begin + count; q++) {
+      GemmProb &g  = probs[q];
+      g.ntm        = (g.M + kBM - 1) / kBM;
+      const int nn = (g.N + kBN - 1) / kBN;
+      g.ntiles     = g.lower ? nn * g.ntm - nn * (nn - 1) / 2 : nn * g.ntm;
+      total += g.ntiles;
+      const double Mr = g.M, Nc = g.N;
+      update_flops += 2.0 * g.K * (g.lower ? Nc * Mr - Nc * (Nc - 1) / 2 : Nc * Mr);
+    }
+    constexpr int64_t kTarget = 296;
+    int64_t t0 = 0, r0 = 0, w0 = 0;
+    for (int32_t q = begin; q < begin + count; q++) {
+      GemmProb &g = probs[q];
+      g.splits    = 1;
+      if (total < kTarget) {
+        const int64_t want = std::max<int64_t>(
+            1, std::min<int64_t>((kTarget + total - 1) / total, g.K / 256));
+        // Split length as the kernels compute it (a multiple of 32); then as
+        // many splits as that length needs, so no split is empty.
+        const int64_t ks = ((g.K + want - 1) / want + 31) / 32 * 32;
+        g.splits         = static_cast<int32_t>((g.K + ks - 1) / ks);
+      }
+      g.tile0  = static_cast<int32_t>(t0);
+      t0 += static_cast<int64_t>(g.ntiles) * g.splits;
+      g.rtile0 = static_cast<int32_t>(r0);
+      g.ws_ofs = -1;
+      if (g.splits > 1) {
+        r0 += g.ntiles;
+        g.ws_ofs = w0;
+        w0 += static_cast<int64_t>(g.ntiles) * g.splits * kBM * kBN;
+      }
+    }
+    tiles    = static_cast<int32_t>(t0);
+    rtiles   = static_cast<int32_t>(r0);
+    ws_elems = std::max(ws_elems, w0);
+  };
   for (int32_t t = 0; t < S.nlevels; t++) {
     LevelPlan &L = levels[t];
     L.small_begin = static_cast<int32_t>(h_small.size());
@@ -508,12 +675,15 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
       R.chunks = ch;
       if (R.count > 0) L.ea_rounds.push_back(R);
     }
-    // Blocked steps.
+    // Blocked steps.  Step kb: the left-looking update of block column kb
+    // by the columns before it, then its diagonal block and panel solve;
+    // after the last step the update matrix, in one product.
     int64_t maxw = 0;
     for (int32_t q = L.large_begin; q < L.large_begin + L.large_count; q++)
       maxw = std::max(maxw, S.w(h_large[q]));
     for (int64_t kb = 0; kb < maxw; kb += kNB) {
-      LevelPlan::Step st{static_cast<int32_t>(descs.size()), 0, 0, 0, 0, 0};
+      LevelPlan::Step st{static_cast<int32_t>(descs.size()), 0, 0, 0, 0, 0,
+                         static_cast<int32_t>(probs.size()), 0, 0, 0};
       int64_t         bpart = 0;
       for (int32_t q = L.large_begin; q < L.large_begin + L.large_count; q++) {
         const int64_t J = h_large[q], w = S.w(J), h = S.h(J);
@@ -530,30 +700,22 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
         const int64_t M = h - kb - d.nbk;
         d.trsm_tile0    = st.trsm_tiles;
         st.trsm_tiles += static_cast<int32_t>((M + kBM - 1) / kBM);
-        d.upd_tile0 = st.upd_tiles;
-        const int64_t N = w - kb - d.nbk;
-        int64_t       pt = 0;
-        if (N > 0 && M > 0) {
-          const int64_t ntr = (M + kBM - 1) / kBM, ntc = (N + kBN - 1) / kBN;
-          pt = ntc * ntr - ntc * (ntc - 1) / 2;
-        }
-        d.upd_panel_tiles = static_cast<int32_t>(pt);
-        const int64_t r   = h - w;
-        int64_t       ut  = 0;
-        if (r > 0) {
-          const int64_t nt = (r + kBM - 1) / kBM;
-          ut               = nt * (nt + 1) / 2;
-        }
-        st.upd_tiles += static_cast<int32_t>(pt + ut);
-        // Work the launches do: 2 * nbk flops per updated lower entry; the
-        // panel solve is a full M x nbk x nbk product.
-        {
-          const double nb = static_cast<double>(d.nbk), Mr = static_cast<double>(M);
-          const double Nc = static_cast<double>(std::max<int64_t>(N, 0));
-          const double rr = static_cast<double>(std::max<int64_t>(r, 0));
-          const double lower_panel = Nc > 0 ? Nc * Mr - Nc * (Nc - 1) / 2 : 0.0;
-          update_flops += 2.0 * nb * (lower_panel + rr * (rr + 1) / 2);
-          trsm_flops += 2.0 * nb * nb * Mr;
+        d.upd_tile0       = 0;
+        d.upd_panel_tiles = 0;
+        trsm_flops += 2.0 * d.nbk * static_cast<double>(d.nbk) * static_cast<double>(M);
+        if (kb > 0) {
+          GemmProb g{};
+          g.a_ofs  = S.slofs[J] + kb;
+          g.lda    = static_cast<int32_t>(h);
+          g.c_ofs  = S.slofs[J] + kb + kb * h;
+          g.ldc    = static_cast<int32_t>(h);
+          g.d_ofs  = S.sfirst[J];
+          g.M      = static_cast<int32_t>(h - kb);
+          g.N      = d.nbk;
+          g.K      = static_cast<int32_t>(kb);
+          g.c_in_u = 0;
+          g.lower  = 1;
+          probs.push_back(g);
         }
         d.zofs         = S.zofs[J];
         d.fsolve_tile0 = st.fsolve_tiles;
@@ -569,9 +731,29 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
         descs.push_back(d);
         st.count++;
       }
+      st.ll_count = static_cast<int32_t>(probs.size()) - st.ll_begin;
+      finish_launch(st.ll_begin, st.ll_count, st.ll_tiles, st.ll_rtiles);
       L.steps.push_back(st);
       bpart_elems = std::max(bpart_elems, bpart);
     }
+    L.u_begin = static_cast<int32_t>(probs.size());
+    for (int32_t q = L.large_begin; q < L.large_begin + L.large_count; q++) {
+      const int64_t J = h_large[q], w = S.w(J), h = S.h(J), r = h - w;
+      if (r <= 0) continue;
+      GemmProb g{};
+      g.a_ofs  = S.slofs[J] + w;
+      g.lda    = static_cast<int32_t>(h);
+      g.c_ofs  = S.uofs[J];
+      g.ldc    = static_cast<int32_t>(r);
+      g.d_ofs  = S.sfirst[J];
+      g.M = g.N = static_cast<int32_t>(r);
+      g.K      = static_cast<int32_t>(w);
+      g.c_in_u = 1;
+      g.lower  = 1;
+      probs.push_back(g);
+    }
+    L.u_count = static_cast<int32_t>(probs.size()) - L.u_begin;
+    finish_launch(L.u_begin, L.u_count, L.u_tiles, L.u_rtiles);
   }
   ndesc = static_cast<int64_t>(descs.size());
   panel_read_bytes = 0;
@@ -602,6 +784,7 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
   steps      = upload(descs, s);
   ea_tasks   = upload(tasks, s);
   zero_segs  = upload(segs, s);
+  gemm_probs = upload(probs, s);
   linv_ofs_d = upload(linv_ofs, s);
   MPIR_CUDA(cudaStreamSynchronize(s));
 }
@@ -612,6 +795,8 @@ void Numeric::allocate(const Plan &P) {
   uarena.resize(std::max<int64_t>(S.uarena_elems, 1) * sizeof(float));
   linv.resize(std::max<int64_t>(P.linv_elems, 1) * sizeof(float));
   linv64.resize(std::max<int64_t>(P.linv_elems, 1) * sizeof(double));
+  linv64t.resize(std::max<int64_t>(P.linv_elems, 1) * sizeof(double));
+  ws.resize(std::max<int64_t>(P.ws_elems, 1) * sizeof(float));
   D.resize(std::max<int64_t>(S.n, 1) * sizeof(float));
   Dinv.resize(std::max<int64_t>(S.n, 1) * sizeof(float));
   status.resize(sizeof(FactorStatus));
@@ -649,7 +834,7 @@ void Numeric::run(const Plan &P, const double *d_Ax, double eps, cudaStream_t s)
   kt.end(s);
   MPIR_CHECK_LAUNCH();
   static bool attr = false;
-  const int   diag_smem = kNB * (kNB + 1) * (sizeof(double) + sizeof(float)) + kNB * sizeof(float);
+  const int   diag_smem = (2 * kNB * (kNB + 1) + kNB) * sizeof(float);
   if (!attr) {
     MPIR_CUDA(cudaFuncSetAttribute(k_diag_block,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -680,11 +865,27 @@ void Numeric::run(const Plan &P, const double *d_Ax, double eps, cudaStream_t s)
           P.srel.as<int32_t>(), pan, ua, D.as<float>(), Dinv.as<float>(), st);
       kt.end(s);
     }
+    const GemmProb *gp = P.gemm_probs.as<GemmProb>();
+    auto gemm = [&](int32_t begin, int32_t count, int32_t tiles, int32_t rtiles) {
+      if (count <= 0 || tiles <= 0) return;
+      kt.begin(kKcUpdate, s);
+      if (update_mode < 0)
+        launch(k_gemm_simt, tiles, kGemmThreads, 0, s, gp + begin, count, pan, ua,
+               static_cast<const float *>(D.as<float>()), ws.as<float>());
+      else
+        launch_gemm_tc(update_mode, gp + begin, count, tiles, pan, ua, D.as<float>(),
+                       ws.as<float>(), st, s);
+      if (rtiles > 0)
+        launch(k_split_reduce, rtiles, 256, 0, s, gp + begin, count, pan, ua,
+               static_cast<const float *>(ws.as<float>()));
+      kt.end(s);
+    };
     for (const auto &stp : L.steps) {
       const StepDesc *dd = P.steps.as<StepDesc>() + stp.begin;
+      gemm(stp.ll_begin, stp.ll_count, stp.ll_tiles, stp.ll_rtiles);
       kt.begin(kKcDiag, s);
-      launch(k_diag_block, stp.count, kDiagThreads, diag_smem, s, 
-          dd, pan, linv.as<float>(), linv64.as<double>(), D.as<float>(), Dinv.as<float>(), st);
+      launch(k_diag_block, stp.count, kDiagThreads, diag_smem, s, dd, pan, linv.as<float>(),
+             D.as<float>(), Dinv.as<float>(), st);
       kt.end(s);
       if (stp.trsm_tiles > 0) {
         kt.begin(kKcTrsm, s);
@@ -692,18 +893,14 @@ void Numeric::run(const Plan &P, const double *d_Ax, double eps, cudaStream_t s)
             dd, stp.count, pan, ua, linv.as<float>(), Dinv.as<float>());
         kt.end(s);
       }
-      if (stp.upd_tiles > 0) {
-        kt.begin(kKcUpdate, s);
-        if (update_mode < 0)
-          launch(k_step_gemm<false>, stp.upd_tiles, kGemmThreads, 0, s, dd, stp.count, pan, ua,
-                 linv.as<float>(), Dinv.as<float>());
-        else
-          launch_update_tc(update_mode, dd, stp.count, stp.upd_tiles, pan, ua, st, s);
-        kt.end(s);
-      }
     }
+    gemm(L.u_begin, L.u_count, L.u_tiles, L.u_rtiles);
     MPIR_CHECK_LAUNCH();
   }
+  // Float64 inverses of the diagonal blocks for the triangular solves.
+  kt.begin(kKcDiag, s);
+  invert_diag_blocks(P, *this, s);
+  kt.end(s);
   valid = true;
 }
 

@@ -29,6 +29,39 @@ constexpr int kWarpsPerCta = 4;
 constexpr int kSmallH      = kSmallFront;
 
 // ---------------------------------------------------------------------------
+// y = Linv z for one 128-column block with 512 threads: thread (q, i) adds
+// the 32 products of row i in column slice q (unrolled, independent loads);
+// slices are summed in order.  Linv is lower triangular, column-major.
+__device__ __forceinline__ double block_lower_apply(const double *Lv, const double *zb, int nb,
+                                                    double (*part)[kNB]) {
+  const int tid = threadIdx.x, i = tid % kNB, q = tid / kNB;
+  double    acc = 0.0;
+#pragma unroll
+  for (int jj = 0; jj < kNB / 4; jj++) {
+    const int j = q * (kNB / 4) + jj;
+    if (j <= i && i < nb) acc += Lv[i + j * kNB] * zb[j];
+  }
+  part[q][i] = acc;
+  __syncthreads();
+  return (part[0][i] + part[1][i]) + (part[2][i] + part[3][i]);
+}
+
+// x = Linv^T v with the row-major copy Lt (Lt[i * kNB + j] = Linv[i][j]):
+// thread (q, j) adds rows i >= j of slice q.
+__device__ __forceinline__ double block_upper_apply(const double *Lt, const double *v, int nb,
+                                                    double (*part)[kNB]) {
+  const int tid = threadIdx.x, j = tid % kNB, q = tid / kNB;
+  double    acc = 0.0;
+#pragma unroll
+  for (int ii = 0; ii < kNB / 4; ii++) {
+    const int i = q * (kNB / 4) + ii;
+    if (i >= j && i < nb) acc += Lt[i * kNB + j] * v[i];
+  }
+  part[q][j] = acc;
+  __syncthreads();
+  return (part[0][j] + part[1][j]) + (part[2][j] + part[3][j]);
+}
+
 // Forward
 __global__ void __launch_bounds__(32 * kWarpsPerCta)
     k_fwd_small(const int32_t *list, int count, const int64_t *sfirst,
@@ -72,11 +105,13 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta)
 
 // Large fronts: right-hand side plus children's update vectors, then the
 // solution of the first column block, y_0 = Linv_0 z_0, stored into x.
-__global__ void k_fwd_gather(const int32_t *list, const int64_t *sfirst,
-                             const int64_t *srowptr, const int64_t *child_ptr,
-                             const int32_t *child_list, const int32_t *srel,
-                             const int64_t *zofs, const int64_t *linv_ofs,
-                             const double *linv64, double *x, double *zbuf) {
+__global__ void __launch_bounds__(kSolveThreads)
+    k_fwd_gather(const int32_t *list, const int64_t *sfirst, const int64_t *srowptr,
+                 const int64_t *child_ptr, const int32_t *child_list, const int32_t *srel,
+                 const int64_t *zofs, const int64_t *linv_ofs, const double *linv64, double *x,
+                 double *zbuf) {
+  __shared__ double zb[kNB];
+  __shared__ double part[4][kNB];
   const int     J = list[blockIdx.x];
   const int64_t f = sfirst[J];
   const int64_t w = sfirst[J + 1] - f;
@@ -93,24 +128,23 @@ __global__ void k_fwd_gather(const int32_t *list, const int64_t *sfirst,
     for (int64_t a = threadIdx.x; a < rc; a += blockDim.x) z[rl[a]] += zc[a];
     __syncthreads();
   }
-  const int     nb = static_cast<int>(w < kNB ? w : kNB);
-  const double *Lv = linv64 + linv_ofs[J];
-  if (threadIdx.x < nb) {
-    const int i   = threadIdx.x;
-    double    acc = 0.0;
-    for (int j = 0; j <= i; j++) acc += Lv[i + j * kNB] * z[j];
-    x[f + i] = acc;
-  }
+  const int nb = static_cast<int>(w < kNB ? w : kNB);
+  if (threadIdx.x < nb) zb[threadIdx.x] = z[threadIdx.x];
+  __syncthreads();
+  const double y = block_lower_apply(linv64 + linv_ofs[J], zb, nb, part);
+  if (threadIdx.x < nb) x[f + threadIdx.x] = y;
 }
 
 // One column block of the large fronts.  The block's solution y is already
-// in x; each CTA updates its rows below the block, z_r -= L_{r,b} y.  The
-// first CTA's rows include the next block, so once they are updated it
+// in x; each CTA updates its 128 rows below the block, z_r -= L_{r,b} y, with
+// the block's columns split in four quarters over the CTA's 512 threads.
+// The first CTA's rows are the next block, so once they are updated it
 // solves that block, y' = Linv_{b+1} z_{b+1}, into x for the next step.
-__global__ void __launch_bounds__(kSolveRows)
+__global__ void __launch_bounds__(kSolveThreads)
     k_fwd_step(const StepDesc *descs, int ndesc, const float *panel,
                const double *linv64, double *x, double *zbuf) {
   __shared__ double y[kNB];
+  __shared__ double part[4][kNB];
   const int         t  = blockIdx.x;
   int               lo = 0, hi = ndesc - 1;
   while (lo < hi) {
@@ -124,24 +158,26 @@ __global__ void __launch_bounds__(kSolveRows)
   double        *z     = zbuf + d.zofs;
   if (tid < d.nbk) y[tid] = x[(int64_t)d.col0 + d.kb + tid];
   __syncthreads();
-  const int64_t r = (int64_t)d.kb + d.nbk + (int64_t)local * kSolveRows + tid;
+  const int     rr = tid % kSolveRows, qq = tid / kSolveRows;
+  const int64_t r  = (int64_t)d.kb + d.nbk + (int64_t)local * kSolveRows + rr;
+  double        acc = 0.0;
   if (r < h) {
-    const float *P   = panel + d.panel + r + (int64_t)d.kb * h;
-    double       acc = z[r];
-    for (int k = 0; k < d.nbk; k++)
-      acc -= static_cast<double>(P[(int64_t)k * h]) * y[k];
-    z[r] = acc;
+    const float *P  = panel + d.panel + r + (int64_t)d.kb * h;
+    const int    k1 = min(d.nbk, (qq + 1) * (kNB / 4));
+    for (int k = qq * (kNB / 4); k < k1; k++)
+      acc += static_cast<double>(P[(int64_t)k * h]) * y[k];
   }
+  part[qq][rr] = acc;
+  __syncthreads();
+  if (qq == 0 && r < h) z[r] -= (part[0][rr] + part[1][rr]) + (part[2][rr] + part[3][rr]);
   const int kn = d.kb + d.nbk;
   if (local == 0 && kn < d.w) {
     __syncthreads();
     const int nb = d.w - kn < kNB ? d.w - kn : kNB;
-    if (tid < nb) {
-      const double *Lv  = linv64 + d.linv + (int64_t)kNB * kNB;
-      double        acc = 0.0;
-      for (int j = 0; j <= tid; j++) acc += Lv[tid + j * kNB] * z[kn + j];
-      x[(int64_t)d.col0 + kn + tid] = acc;
-    }
+    if (tid < nb) y[tid] = z[kn + tid];  // the next block's right-hand side
+    __syncthreads();
+    const double yn = block_lower_apply(linv64 + d.linv + (int64_t)kNB * kNB, y, nb, part);
+    if (tid < nb) x[(int64_t)d.col0 + kn + tid] = yn;
   }
 }
 
@@ -196,14 +232,16 @@ __global__ void k_bwd_gather(const int32_t *list, const int64_t *sfirst,
 }
 
 // One column block, backward: partial sums t_k = sum_r L_{r,kb+k} z_r over a
-// chunk of rows below the block; the last chunk to finish adds the partials
-// in chunk order and solves x_b = Linv^T (z_b - t).
-__global__ void __launch_bounds__(kSolveChunk)
+// chunk of 128 rows below the block (each warp takes 8 of the block's
+// columns); the last chunk to finish adds the partials in chunk order and
+// solves x_b = Linv^T (z_b - t) with the row-major copy of the inverse.
+__global__ void __launch_bounds__(kSolveThreads)
     k_bwd_step(const StepDesc *descs, int ndesc, const float *panel,
-               const double *linv64, double *x, double *zbuf, double *part,
+               const double *linv64t, double *x, double *zbuf, double *part,
                int32_t *counter) {
   __shared__ double zr[kSolveChunk];
   __shared__ double v[kNB];
+  __shared__ double red[4][kNB];
   __shared__ int    last;
   const int         t  = blockIdx.x;
   int               lo = 0, hi = ndesc - 1;
@@ -218,11 +256,12 @@ __global__ void __launch_bounds__(kSolveChunk)
   double        *z   = zbuf + d.zofs;
   const int64_t  r0  = (int64_t)d.kb + d.nbk + (int64_t)chunk * kSolveChunk;
   const int64_t  r1  = min(r0 + kSolveChunk, h);
-  zr[tid]            = r0 + tid < r1 ? z[r0 + tid] : 0.0;
+  if (tid < kSolveChunk) zr[tid] = r0 + tid < r1 ? z[r0 + tid] : 0.0;
   __syncthreads();
   const float *P  = panel + d.panel;
   double      *pp = part + d.bpart + (int64_t)chunk * kNB;
-  for (int k = warp; k < d.nbk; k += kSolveChunk / 32) {
+  constexpr int kWarps = kSolveThreads / 32;
+  for (int k = warp; k < d.nbk; k += kWarps) {
     const float *col = P + (int64_t)(d.kb + k) * h;
     double       s   = 0.0;
     for (int64_t r = r0 + lane; r < r1; r += 32)
@@ -237,19 +276,25 @@ __global__ void __launch_bounds__(kSolveChunk)
   __syncthreads();
   if (!last) return;
   __threadfence();
-  if (tid < d.nbk) {
-    double s = 0.0;
-    for (int c = 0; c < d.bsolve_chunks; c++)
-      s += __ldcg(part + d.bpart + (int64_t)c * kNB + tid);
-    v[tid] = z[d.kb + tid] - s;
+  {
+    // Partials of column k: thread (q, k) adds chunks q, q + 4, ...; the
+    // four sums are then added in order.
+    const int k = tid % kNB, q = tid / kNB;
+    double    s = 0.0;
+    if (k < d.nbk)
+      for (int c = q; c < d.bsolve_chunks; c += 4)
+        s += __ldcg(part + d.bpart + (int64_t)c * kNB + k);
+    red[q][k] = s;
   }
   __syncthreads();
+  if (tid < d.nbk)
+    v[tid] = z[d.kb + tid] - ((red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]));
+  __syncthreads();
+  // Lt[i * kNB + j] = Linv[i][j]
+  const double xb = block_upper_apply(linv64t + d.linv, v, d.nbk, red);
   if (tid < d.nbk) {
-    const double *Lv  = linv64 + d.linv;
-    double        acc = 0.0;
-    for (int i = tid; i < d.nbk; i++) acc += Lv[i + tid * kNB] * v[i];
-    z[d.kb + tid]                    = acc;
-    x[(int64_t)d.col0 + d.kb + tid] = acc;
+    z[d.kb + tid]                    = xb;
+    x[(int64_t)d.col0 + d.kb + tid] = xb;
   }
 }
 
@@ -313,13 +358,13 @@ void ldlt_solve(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
           P.child_ptr.as<int64_t>(), P.child_list.as<int32_t>(),
           P.srel.as<int32_t>(), P.zofs.as<int64_t>(), pan, x, zbuf);
     if (L.large_count > 0) {
-      launch(k_fwd_gather, L.large_count, 256, 0, s,
+      launch(k_fwd_gather, L.large_count, kSolveThreads, 0, s,
              P.large_list.as<int32_t>() + L.large_begin, P.sfirst.as<int64_t>(),
              P.srowptr.as<int64_t>(), P.child_ptr.as<int64_t>(),
              P.child_list.as<int32_t>(), P.srel.as<int32_t>(), P.zofs.as<int64_t>(),
              P.linv_ofs_d.as<int64_t>(), lv, x, zbuf);
       for (const auto &st : L.steps)
-        launch(k_fwd_step, st.fsolve_tiles, kSolveRows, 0, s, 
+        launch(k_fwd_step, st.fsolve_tiles, kSolveThreads, 0, s, 
             P.steps.as<StepDesc>() + st.begin, st.count, pan, lv, x, zbuf);
     }
   }
@@ -347,9 +392,9 @@ void ldlt_solve(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
           zbuf);
       for (size_t q = L.steps.size(); q-- > 0;) {
         const auto &st = L.steps[q];
-        launch(k_bwd_step, st.bsolve_chunks, kSolveChunk, 0, s, 
-            P.steps.as<StepDesc>() + st.begin, st.count, pan, lv, x, zbuf,
-            ws.part.as<double>(), ws.counters.as<int32_t>());
+        launch(k_bwd_step, st.bsolve_chunks, kSolveThreads, 0, s,
+               P.steps.as<StepDesc>() + st.begin, st.count, pan, F.linv64t.as<double>(), x,
+               zbuf, ws.part.as<double>(), ws.counters.as<int32_t>());
       }
     }
   }
