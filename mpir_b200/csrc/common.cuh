@@ -62,6 +62,31 @@ struct StepDesc {
   int32_t bsolve_chunk0;
   int32_t bsolve_chunks;
   int32_t id;
+  // Packed copy of the front for the tensor-core updates (see PackedFront):
+  // float offset of the front's packed rows and pivots, K-groups per row
+  // tile, and the packed row of the first off-diagonal row.
+  int64_t pk;
+  int64_t pd;
+  int32_t pk_g;
+  int32_t pk_wt;
+};
+
+// Packed copy of a large front's L for the tensor-core updates.  Rows are
+// renumbered so that the off-diagonal rows start on a 128-row boundary:
+// packed row p = r for r < w, p = Wt + (r - w) for r >= w, Wt = w rounded up
+// to 128.  Row tile t (packed rows 128t .. 128t+127) holds the columns in
+// K-groups of 4; K-group g of row tile t is 2048 contiguous bytes at float
+// offset pk + (t * G + g) * 512, in the tensor cores' K-major core-matrix
+// layout without swizzle (packed row m of the tile at byte 16m, its 4 columns
+// consecutive).  G = ceil(w / 32) * 8, so every stage of 16 or 32 columns is
+// one contiguous, 16-byte aligned block.  Positions that hold no value of L
+// (rows Wt > p >= w, rows past the last, columns >= w, the diagonal blocks)
+// stay zero.  The pivots D of the front's columns are packed beside it at pd
+// (G * 4 floats, zero past w), and sign(D) sqrt|D| in a second array at the
+// same offsets.
+struct PackedFront {
+  static constexpr int kRowTile = 128;
+  static constexpr int kGroupFloats = 512;  // 128 rows x 4 columns
 };
 
 // One GEMM-shaped update of a front, C -= (A D) A^T restricted to N columns:
@@ -72,11 +97,20 @@ struct StepDesc {
 // eliminated so far) and for its update matrix (K = all its columns).  The
 // K range may be split across CTAs whose partial tiles go to a workspace and
 // are added in split order by a reduction launch.
+//
+// Rows are counted in the packed numbering of the front (PackedFront): local
+// row m of the problem is output row m for m < gap_at, nothing for
+// gap_at <= m < gap_at + gap, and output row m - gap beyond.  The columns
+// (N <= gap_at) have no gap.
 struct GemmProb {
   int64_t a_ofs;   // panel offset of A(0, 0)
   int64_t c_ofs;   // offset of C(0, 0)
   int64_t d_ofs;   // index of D for column 0 of A
   int64_t ws_ofs;  // float offset of the split partials, -1 when unsplit
+  int64_t pa, pb;  // packed offsets of the first row tile of A and of B
+  int64_t pd;      // packed offset of D for column 0
+  int64_t prow;    // floats between consecutive packed row tiles
+  int32_t gap_at, gap;
   int32_t lda, ldc;
   int32_t M, N, K;
   int32_t c_in_u;  // C lives in the update arena (else in the panels)
@@ -104,6 +138,11 @@ struct Segment {
   int64_t ofs, len;
   int64_t chunk0;  // first chunk of this segment within the launch
 };
+
+// Output row of local packed row m of a problem, -1 inside its gap.
+__host__ __device__ __forceinline__ int gemm_out_row(const GemmProb &pb, int m) {
+  return m < pb.gap_at ? m : (m < pb.gap_at + pb.gap ? -1 : m - pb.gap);
+}
 
 // Device status of one numeric factorization.
 struct FactorStatus {

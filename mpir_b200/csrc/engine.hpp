@@ -103,9 +103,19 @@ class Plan {
   int64_t      ws_elems = 0;  // split-K partial tiles (floats)
   std::vector<int32_t> h_small, h_large;
   std::vector<int64_t> linv_ofs;  // per supernode, -1 for small fronts
+  // Packed fronts (PackedFront) of the large fronts: float offsets of the
+  // packed rows and of the packed pivots per supernode (-1 for small
+  // fronts), and the totals.
+  std::vector<int64_t> pk_ofs, pd_ofs;
+  int64_t              pk_elems = 0, pd_elems = 0;
 
   void build(Symbolic &&sym, cudaStream_t s);
   bool is_large(int64_t J) const { return S.h(J) > kSmallFront; }
+  // Packed-front geometry (PackedFront): first packed row of the
+  // off-diagonal rows, K-groups per row tile, row tiles.
+  int64_t pk_wt(int64_t J) const { return (S.w(J) + 127) / 128 * 128; }
+  int64_t pk_groups(int64_t J) const { return (S.w(J) + 31) / 32 * 8; }
+  int64_t pk_tiles(int64_t J) const { return (pk_wt(J) + S.h(J) - S.w(J) + 127) / 128; }
 };
 
 // Numeric factor of one value set on a plan.
@@ -115,6 +125,9 @@ class Numeric {
   // linv64: the same inverses in float64 (the triangular solves), column-major;
   // linv64t: row-major copy of linv64 (the backward solve).
   DeviceBuffer panel, uarena, linv, linv64, linv64t, D, Dinv, status, ws;
+  // Packed fronts for the tensor-core updates: rows (pack) and pivots
+  // (packd: D, then sign(D) sqrt|D|, Plan::pd_elems floats each).
+  DeviceBuffer pack, packd;
   DeviceBuffer AD, Axs, Kval, Korig, Ax;
   double       eps_uf = 0;
   bool         valid  = false;
@@ -131,8 +144,12 @@ class Numeric {
                  bool *nonfinite = nullptr) const;
 };
 
-void launch_gemm_tc(int mode, const GemmProb *probs, int nprob, int tiles, float *panel,
-                    float *uarena, const float *D, float *ws, FactorStatus *st, cudaStream_t s);
+// Tensor-core GemmProb updates from the packed fronts (mode 0 bfloat16,
+// 1 3xTF32, 2 float16).  packs = the sign(D) sqrt|D| array.
+void launch_gemm_tc(int mode, const GemmProb *probs, int nprob, int tiles, const float *pack,
+                    const float *packd, const float *packs, float *panel, float *uarena,
+                    float *ws, FactorStatus *st, cudaStream_t s);
+int  tc_gemm_smem_bytes(int mode);
 
 // Kernel-class timer used by the benchmark's roofline figures.
 struct KernelTimer {

@@ -197,7 +197,7 @@ __global__ void k_extend_add(const EaTask *tasks, int ntasks,
 // substitution on the identity, done in the same sweep).
 __global__ void __launch_bounds__(kDiagThreads)
     k_diag_block(const StepDesc *descs, float *panel, float *linv, float *D, float *Dinv,
-                 FactorStatus *st) {
+                 float *packd, float *packs, FactorStatus *st) {
   extern __shared__ float sm[];
   constexpr int           LD = kNB + 1;
   float                  *F  = sm;
@@ -242,6 +242,10 @@ __global__ void __launch_bounds__(kDiagThreads)
       const int64_t col = (int64_t)d.col0 + d.kb + k;
       D[col]            = dk;
       Dinv[col]         = dinv;
+      if (packd != nullptr && d.pd >= 0) {
+        packd[d.pd + d.kb + k] = dk;
+        packs[d.pd + d.kb + k] = copysignf(sqrtf(fabsf(dk)), dk);
+      }
       note_pivot(st, static_cast<int32_t>(col), dk, &npos);
     }
     __syncthreads();
@@ -270,7 +274,7 @@ constexpr int kBM = 128, kBN = 128, kBK = 16;
 template <bool TRSM>
 __global__ void __launch_bounds__(kGemmThreads)
     k_step_gemm(const StepDesc *descs, int ndesc, float *panel, float *uarena,
-                const float *linv, const float *Dinv) {
+                const float *linv, const float *Dinv, float *pack) {
   __shared__ float As[kBK][kBM];
   __shared__ float Bs[kBK][kBN];
   __shared__ float sd[kNB];
@@ -385,6 +389,38 @@ __global__ void __launch_bounds__(kGemmThreads)
       }
     }
   }
+  if (TRSM && pack != nullptr && d.pk >= 0) {
+    // The finished block column again, in the packed layout (PackedFront):
+    // two 4-column K-groups of each of this thread's rows.
+    float *pk = pack + d.pk;
+    float  dvs[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      const int c = n0 + tc * 8 + j;
+      dvs[j]      = c < N ? Dinv[(int64_t)d.col0 + kb + c] : 0.0f;
+    }
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const int r = m0 + tr * 8 + i;
+      if (r >= M) continue;
+      const int rf = kb + nbk + r;  // row of the front
+      const int p  = rf < w ? rf : rf - w + d.pk_wt;
+      float    *row = pk + static_cast<int64_t>(p >> 7) * d.pk_g * PackedFront::kGroupFloats +
+                   (p & 127) * 4;
+#pragma unroll
+      for (int hh = 0; hh < 2; hh++) {
+        const int c0 = n0 + tc * 8 + hh * 4;
+        if (c0 >= N) continue;
+        float4 v;
+        v.x = acc[i][hh * 4 + 0] * dvs[hh * 4 + 0];
+        v.y = acc[i][hh * 4 + 1] * dvs[hh * 4 + 1];
+        v.z = acc[i][hh * 4 + 2] * dvs[hh * 4 + 2];
+        v.w = acc[i][hh * 4 + 3] * dvs[hh * 4 + 3];
+        *reinterpret_cast<float4 *>(row + static_cast<int64_t>((kb + c0) >> 2) *
+                                              PackedFront::kGroupFloats) = v;
+      }
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -443,8 +479,8 @@ __global__ void __launch_bounds__(kGemmThreads)
       const int i = idx % kBM, kk = idx / kBM;
       const int k = k0 + kk;
       const bool kin = k < k_hi;
-      const int r = m0 + i, c = n0 + i;
-      As[kk][i] = (r < M && kin) ? A[r + (int64_t)k * lda] * Dk[k] : 0.0f;
+      const int r = m0 + i < M ? gemm_out_row(pb, m0 + i) : -1, c = n0 + i;
+      As[kk][i] = (r >= 0 && kin) ? A[r + (int64_t)k * lda] * Dk[k] : 0.0f;
       Bs[kk][i] = (c < N && kin) ? A[c + (int64_t)k * lda] : 0.0f;
     }
     __syncthreads();
@@ -477,8 +513,8 @@ __global__ void __launch_bounds__(kGemmThreads)
     if (c >= N) continue;
 #pragma unroll
     for (int i = 0; i < 8; i++) {
-      const int r = m0 + tr * 8 + i;
-      if (r < M && (!pb.lower || r >= c)) C[r + (int64_t)c * pb.ldc] -= acc[i][j];
+      const int r = m0 + tr * 8 + i < M ? gemm_out_row(pb, m0 + tr * 8 + i) : -1;
+      if (r >= 0 && (!pb.lower || r >= c)) C[r + (int64_t)c * pb.ldc] -= acc[i][j];
     }
   }
 }
@@ -498,8 +534,9 @@ __global__ void k_split_reduce(const GemmProb *probs, int nprob, float *panel, f
   float       *C = (pb.c_in_u ? uarena : panel) + pb.c_ofs;
   const float *W = ws + pb.ws_ofs + static_cast<int64_t>(tile) * pb.splits * (kBM * kBN);
   for (int e = threadIdx.x; e < kBM * kBN; e += blockDim.x) {
-    const int r = m0 + e % kBM, c = n0 + e / kBM;
-    if (r >= pb.M || c >= pb.N || (pb.lower && r < c)) continue;
+    const int m = m0 + e % kBM, c = n0 + e / kBM;
+    const int r = m < pb.M ? gemm_out_row(pb, m) : -1;
+    if (r < 0 || c >= pb.N || (pb.lower && r < c)) continue;
     float acc = 0.0f;
     for (int q = 0; q < pb.splits; q++) acc += W[static_cast<int64_t>(q) * (kBM * kBN) + e];
     C[r + (int64_t)c * pb.ldc] -= acc;
@@ -569,10 +606,17 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
   bpart_elems  = 0;
   update_flops = 0;
   trsm_flops   = 0;
+  pk_ofs.assign(ns, -1);
+  pd_ofs.assign(ns, -1);
+  pk_elems = pd_elems = 0;
   for (int64_t J = 0; J < ns; J++)
     if (is_large(J)) {
       linv_ofs[J] = linv_elems;
       linv_elems += ((S.w(J) + kNB - 1) / kNB) * (int64_t)kNB * kNB;
+      pk_ofs[J] = pk_elems;
+      pk_elems += pk_tiles(J) * pk_groups(J) * PackedFront::kGroupFloats;
+      pd_ofs[J] = pd_elems;
+      pd_elems += pk_groups(J) * 4;
     }
   // Per-level launch lists.
   levels.assign(S.nlevels, LevelPlan{});
@@ -704,19 +748,32 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
         d.upd_panel_tiles = 0;
         trsm_flops += 2.0 * d.nbk * static_cast<double>(d.nbk) * static_cast<double>(M);
         if (kb > 0) {
+          // Rows kb .. h-1 in the packed numbering: kb .. w-1, the gap up to
+          // Wt, then the off-diagonal rows.
+          const int64_t wt = pk_wt(J);
           GemmProb g{};
           g.a_ofs  = S.slofs[J] + kb;
           g.lda    = static_cast<int32_t>(h);
           g.c_ofs  = S.slofs[J] + kb + kb * h;
           g.ldc    = static_cast<int32_t>(h);
           g.d_ofs  = S.sfirst[J];
-          g.M      = static_cast<int32_t>(h - kb);
+          g.prow   = pk_groups(J) * PackedFront::kGroupFloats;
+          g.pa     = pk_ofs[J] + (kb / PackedFront::kRowTile) * g.prow;
+          g.pb     = g.pa;
+          g.pd     = pd_ofs[J];
+          g.gap_at = static_cast<int32_t>(w - kb);
+          g.gap    = static_cast<int32_t>(h > w ? wt - w : 0);
+          g.M      = static_cast<int32_t>(h > w ? wt + (h - w) - kb : w - kb);
           g.N      = d.nbk;
           g.K      = static_cast<int32_t>(kb);
           g.c_in_u = 0;
           g.lower  = 1;
           probs.push_back(g);
         }
+        d.pk           = pk_ofs[J];
+        d.pd           = pd_ofs[J];
+        d.pk_g         = static_cast<int32_t>(pk_groups(J));
+        d.pk_wt        = static_cast<int32_t>(pk_wt(J));
         d.zofs         = S.zofs[J];
         d.fsolve_tile0 = st.fsolve_tiles;
         st.fsolve_tiles += static_cast<int32_t>(
@@ -746,6 +803,12 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
       g.c_ofs  = S.uofs[J];
       g.ldc    = static_cast<int32_t>(r);
       g.d_ofs  = S.sfirst[J];
+      g.prow   = pk_groups(J) * PackedFront::kGroupFloats;
+      g.pa     = pk_ofs[J] + (pk_wt(J) / PackedFront::kRowTile) * g.prow;
+      g.pb     = g.pa;
+      g.pd     = pd_ofs[J];
+      g.gap_at = static_cast<int32_t>(r);
+      g.gap    = 0;
       g.M = g.N = static_cast<int32_t>(r);
       g.K      = static_cast<int32_t>(w);
       g.c_in_u = 1;
@@ -797,6 +860,12 @@ void Numeric::allocate(const Plan &P) {
   linv64.resize(std::max<int64_t>(P.linv_elems, 1) * sizeof(double));
   linv64t.resize(std::max<int64_t>(P.linv_elems, 1) * sizeof(double));
   ws.resize(std::max<int64_t>(P.ws_elems, 1) * sizeof(float));
+  // Packed fronts: positions that hold no value of L are never written and
+  // stay zero from here on.
+  pack.resize(std::max<int64_t>(P.pk_elems, 1) * sizeof(float));
+  packd.resize(std::max<int64_t>(2 * P.pd_elems, 1) * sizeof(float));
+  MPIR_CUDA(cudaMemset(pack.as<void>(), 0, pack.bytes()));
+  MPIR_CUDA(cudaMemset(packd.as<void>(), 0, packd.bytes()));
   D.resize(std::max<int64_t>(S.n, 1) * sizeof(float));
   Dinv.resize(std::max<int64_t>(S.n, 1) * sizeof(float));
   status.resize(sizeof(FactorStatus));
@@ -873,7 +942,8 @@ void Numeric::run(const Plan &P, const double *d_Ax, double eps, cudaStream_t s)
         launch(k_gemm_simt, tiles, kGemmThreads, 0, s, gp + begin, count, pan, ua,
                static_cast<const float *>(D.as<float>()), ws.as<float>());
       else
-        launch_gemm_tc(update_mode, gp + begin, count, tiles, pan, ua, D.as<float>(),
+        launch_gemm_tc(update_mode, gp + begin, count, tiles, pack.as<float>(),
+                       packd.as<float>(), packd.as<float>() + P.pd_elems, pan, ua,
                        ws.as<float>(), st, s);
       if (rtiles > 0)
         launch(k_split_reduce, rtiles, 256, 0, s, gp + begin, count, pan, ua,
@@ -885,12 +955,13 @@ void Numeric::run(const Plan &P, const double *d_Ax, double eps, cudaStream_t s)
       gemm(stp.ll_begin, stp.ll_count, stp.ll_tiles, stp.ll_rtiles);
       kt.begin(kKcDiag, s);
       launch(k_diag_block, stp.count, kDiagThreads, diag_smem, s, dd, pan, linv.as<float>(),
-             D.as<float>(), Dinv.as<float>(), st);
+             D.as<float>(), Dinv.as<float>(), packd.as<float>(),
+             packd.as<float>() + P.pd_elems, st);
       kt.end(s);
       if (stp.trsm_tiles > 0) {
         kt.begin(kKcTrsm, s);
         launch(k_step_gemm<true>, stp.trsm_tiles, kGemmThreads, 0, s, 
-            dd, stp.count, pan, ua, linv.as<float>(), Dinv.as<float>());
+            dd, stp.count, pan, ua, linv.as<float>(), Dinv.as<float>(), pack.as<float>());
         kt.end(s);
       }
     }

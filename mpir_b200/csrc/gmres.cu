@@ -25,11 +25,12 @@ double eps_of(int prec) {
   return DBL_EPSILON;
 }
 
-// Trailing-update engine for a factor type: float32 runs float32 SIMT
-// products, bfloat16 / float16 factors single-pass tensor-core products in
-// that type; MPIR_UPDATE ("simt", "tf32x3", "bf16", "f16") overrides.
+// Trailing-update engine for a factor type: float32 runs 3xTF32 tensor-core
+// products (float32-level accuracy), bfloat16 / float16 factors single-pass
+// tensor-core products in that type; MPIR_UPDATE ("simt" = float32 SIMT
+// units, "tf32x3", "bf16", "f16") overrides.
 static int update_mode_for(int uf) {
-  int mode = uf == kBF16 ? 0 : uf == kF16 ? 2 : -1;
+  int mode = uf == kBF16 ? 0 : uf == kF16 ? 2 : 1;
   if (const char *e = std::getenv("MPIR_UPDATE")) {
     const std::string v(e);
     if (v == "simt") mode = -1;

@@ -2,26 +2,35 @@
 // C -= (A D) A^T for the left-looking block-column updates of a front and for
 // its update matrix (GemmProb), the work that dominates the factorization.
 //
-// One CTA of 128 threads computes a 128 x 128 tile of C over its K range
-// (one split of K).  Per K-chunk every thread loads one row of A and one of
-// B (= rows of A) from the float32 panel, scales them by the pivots,
-// converts it (bfloat16, or tf32 hi + lo parts for the 3xTF32 product) and
-// stores it into shared memory in the K-major canonical layout without
-// swizzle (8-row x 16-byte core matrices, rows 16 bytes apart, K-chunks
-// 2048 bytes apart).  One thread issues tcgen05.mma into a 128 x 128 float32
-// accumulator in tensor memory and commits to an mbarrier; shared buffers
-// alternate so loads of chunk c+1 overlap the MMAs of chunk c.  The
-// epilogue reads the accumulator with tcgen05.ld (warp w owns lanes
-// 32w..32w+31 = tile rows) and subtracts it from C with coalesced column
-// stores.
+// Operands come from the packed copy of the front (PackedFront), where every
+// stage of 16 or 32 columns of a 128-row tile is one contiguous, 16-byte
+// aligned block already in the tensor cores' K-major core-matrix layout.  One
+// CTA computes a 128 x 128 tile of C over its K range (one split of K) with
+// warp-specialised roles around a ring of kStages shared-memory stages:
 //
-//   kind::f16  with bfloat16 A/B: one MMA per 16-wide K step.
+//   warp 0 (one lane)  producer: cp.async.bulk of the A block, the B block
+//                      and the stage's pivots into a free stage; the copies
+//                      complete on the stage's `full` mbarrier (tx bytes);
+//   warps 4..7         converters: thread m takes packed row m of A and B,
+//                      scales by the pivots and rounds in place (3xTF32: the
+//                      tf32 high part in place, the low part beside it;
+//                      16-bit: bfloat16 / float16 into the first half), then
+//                      arrives on the stage's `conv` mbarrier;
+//   warp 1 (one lane)  MMA issuer: tcgen05.mma into a 128 x 128 float32
+//                      accumulator in tensor memory; tcgen05.commit frees the
+//                      stage (`empty`) once its MMAs have read it;
+//   warps 4..7         epilogue: tcgen05.ld of the accumulator (warp w reads
+//                      lanes 32(w-4) .. = tile rows) and C -= tile with
+//                      coalesced column stores, or the split partial.
+//
 //   kind::tf32 3xTF32: A_hi B_hi + A_hi B_lo + A_lo B_hi per 8-wide K step,
-//                      float32-level accuracy.
+//                      float32-level accuracy (round-to-nearest splits).
+//   kind::f16 bfloat16 / float16: balanced operands (A sqrt|D| sign D) and
+//                      (A sqrt|D|), which keep both in range.
 //
 // Every mbarrier wait is bounded; on expiry the kernel records a timeout in
-// the factor status, waits (bounded) for its own MMAs, frees its tensor
-// memory and returns.
+// the factor status, stops issuing work, waits (bounded) for its own copies
+// and MMAs, frees its tensor memory and returns.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
@@ -32,16 +41,31 @@ namespace mpir {
 
 namespace tc {
 
-constexpr int      kTileM    = 128;
-constexpr int      kTileN    = 128;
-constexpr int      kThreads  = 128;
-constexpr uint32_t kTmemCols = 128;
-constexpr uint32_t kLBO      = 2048;  // bytes between K-direction core matrices
-constexpr uint32_t kSBO      = 128;   // bytes between 8-row groups
+constexpr int      kTileM     = 128;
+constexpr int      kTileN     = 128;
+constexpr int      kThreads   = 256;
+constexpr int      kStages    = 6;
+constexpr uint32_t kTmemCols  = 128;
+constexpr uint32_t kGroup     = 2048;  // bytes of one K-group (128 rows x 16 B)
+constexpr uint32_t kLBO       = 2048;  // bytes between K-adjacent core matrices
+constexpr uint32_t kSBO       = 128;   // bytes between 8-row groups
 constexpr long     kSpinLimit = 20000000;
-// Raw float32 K-chunks in flight per CTA: 4 for 3xTF32 (16-wide chunks),
-// 3 for 16-bit operands (32-wide chunks).
-__host__ __device__ constexpr int stages_for(bool half) { return half ? 3 : 4; }
+
+// Stage layout of a mode (bytes): A block, B block, [A low, B low], pivots.
+template <int MODE>
+struct Cfg {
+  static constexpr bool     kHalf  = MODE != 1;
+  static constexpr int      kKC    = kHalf ? 32 : 16;  // float32 columns per stage
+  static constexpr int      kKG    = kKC / 4;          // packed K-groups per stage
+  static constexpr uint32_t kRaw   = kKG * kGroup;     // bytes of one operand block
+  static constexpr uint32_t kA     = 0;
+  static constexpr uint32_t kB     = kRaw;
+  static constexpr uint32_t kAlo   = 2 * kRaw;
+  static constexpr uint32_t kBlo   = 3 * kRaw;
+  static constexpr uint32_t kD     = kHalf ? 2 * kRaw : 4 * kRaw;
+  static constexpr uint32_t kStage = kD + 1024;        // keeps 1024-byte alignment
+  static constexpr uint32_t kTx    = 2 * kRaw + kKC * 4;
+};
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -66,9 +90,10 @@ __host__ __device__ constexpr uint32_t make_idesc(uint32_t fmt) {
 }
 constexpr uint32_t kFmtF16 = 0, kFmtBF16 = 1, kFmtTF32 = 2;
 
-__device__ __forceinline__ void mma(uint32_t fmt_is_tf32, uint32_t tmem, uint64_t a,
-                                    uint64_t b, uint32_t idesc, uint32_t accum) {
-  if (fmt_is_tf32) {
+template <bool TF32>
+__device__ __forceinline__ void mma(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                    uint32_t accum) {
+  if (TF32) {
     asm volatile(
         "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
@@ -104,18 +129,22 @@ __device__ __forceinline__ bool wait_bounded(uint32_t mbar, uint32_t parity) {
   return false;
 }
 
-// 4-byte asynchronous global->shared copy; src_bytes = 0 fills zeros and
-// reads nothing (the source address is then only a placeholder).
-__device__ __forceinline__ void cp_async4(uint32_t dst, const void *src, uint32_t src_bytes) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst), "l"(src),
-               "r"(src_bytes) : "memory");
+__device__ __forceinline__ void arrive(uint32_t mbar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar) : "memory");
 }
-__device__ __forceinline__ void cp_async_commit() {
-  asm volatile("cp.async.commit_group;" ::: "memory");
+
+__device__ __forceinline__ void arrive_expect_tx(uint32_t mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar),
+               "r"(bytes) : "memory");
 }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+
+// Bulk global -> shared copy (16-byte aligned addresses, size a multiple of
+// 16) completing on an mbarrier.
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes,
+                                          uint32_t mbar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+      ::"r"(dst), "l"(src), "r"(bytes), "r"(mbar) : "memory");
 }
 
 __device__ __forceinline__ uint32_t to_tf32(float x) {
@@ -139,24 +168,85 @@ __device__ __forceinline__ uint32_t pack16(float a, float b) {
   return MODE == 2 ? pack_f16(a, b) : pack_bf16(a, b);
 }
 
+// Round packed row m of one stage in place (see the file comment).
+template <int MODE>
+__device__ __forceinline__ void convert_row(uint8_t *stage, int m) {
+  using C         = Cfg<MODE>;
+  const float *dv = reinterpret_cast<const float *>(stage + C::kD);
+  if (MODE == 1) {
+#pragma unroll
+    for (int g = 0; g < C::kKG; g++) {
+      float4 *pa = reinterpret_cast<float4 *>(stage + C::kA + g * kGroup + m * 16);
+      float4 *pb = reinterpret_cast<float4 *>(stage + C::kB + g * kGroup + m * 16);
+      const float4 a = *pa, b = *pb;
+      const float4 d = *reinterpret_cast<const float4 *>(dv + 4 * g);
+      const float  av[4] = {a.x, a.y, a.z, a.w};
+      const float  bv[4] = {b.x * d.x, b.y * d.y, b.z * d.z, b.w * d.w};
+      uint4        ah, al, bh, bl;
+      uint32_t    *ahp = &ah.x, *alp = &al.x, *bhp = &bh.x, *blp = &bl.x;
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const uint32_t xh = to_tf32(av[e]);
+        ahp[e]            = xh;
+        alp[e]            = to_tf32(av[e] - __uint_as_float(xh));
+        const uint32_t yh = to_tf32(bv[e]);
+        bhp[e]            = yh;
+        blp[e]            = to_tf32(bv[e] - __uint_as_float(yh));
+      }
+      *reinterpret_cast<uint4 *>(pa)                                         = ah;
+      *reinterpret_cast<uint4 *>(pb)                                         = bh;
+      *reinterpret_cast<uint4 *>(stage + C::kAlo + g * kGroup + m * 16) = al;
+      *reinterpret_cast<uint4 *>(stage + C::kBlo + g * kGroup + m * 16) = bl;
+    }
+  } else {
+    // 32 columns of row m: read all (8 float32 K-groups), then write 4
+    // 16-bit K-groups of 8 over the first half of the block.
+    float av[32], bv[32];
+#pragma unroll
+    for (int g = 0; g < C::kKG; g++) {
+      const float4 a = *reinterpret_cast<const float4 *>(stage + C::kA + g * kGroup + m * 16);
+      const float4 b = *reinterpret_cast<const float4 *>(stage + C::kB + g * kGroup + m * 16);
+      const float4 s = *reinterpret_cast<const float4 *>(dv + 4 * g);
+      av[4 * g + 0] = a.x * s.x;
+      av[4 * g + 1] = a.y * s.y;
+      av[4 * g + 2] = a.z * s.z;
+      av[4 * g + 3] = a.w * s.w;
+      bv[4 * g + 0] = b.x * fabsf(s.x);
+      bv[4 * g + 1] = b.y * fabsf(s.y);
+      bv[4 * g + 2] = b.z * fabsf(s.z);
+      bv[4 * g + 3] = b.w * fabsf(s.w);
+    }
+#pragma unroll
+    for (int q = 0; q < C::kKG / 2; q++) {
+      uint4 pa, pbk;
+      pa.x  = pack16<MODE>(av[8 * q + 0], av[8 * q + 1]);
+      pa.y  = pack16<MODE>(av[8 * q + 2], av[8 * q + 3]);
+      pa.z  = pack16<MODE>(av[8 * q + 4], av[8 * q + 5]);
+      pa.w  = pack16<MODE>(av[8 * q + 6], av[8 * q + 7]);
+      pbk.x = pack16<MODE>(bv[8 * q + 0], bv[8 * q + 1]);
+      pbk.y = pack16<MODE>(bv[8 * q + 2], bv[8 * q + 3]);
+      pbk.z = pack16<MODE>(bv[8 * q + 4], bv[8 * q + 5]);
+      pbk.w = pack16<MODE>(bv[8 * q + 6], bv[8 * q + 7]);
+      *reinterpret_cast<uint4 *>(stage + C::kA + q * kGroup + m * 16) = pa;
+      *reinterpret_cast<uint4 *>(stage + C::kB + q * kGroup + m * 16) = pbk;
+    }
+  }
+}
+
 }  // namespace tc
 
 // MODE 0: bfloat16 single pass; MODE 1: 3xTF32; MODE 2: float16 single pass.
 template <int MODE>
-__global__ void __launch_bounds__(tc::kThreads)
-    k_gemm_tc(const GemmProb *probs, int nprob, float *panel, float *uarena, const float *D,
-              float *ws, FactorStatus *st) {
+__global__ void __launch_bounds__(tc::kThreads, 1)
+    k_gemm_tc(const GemmProb *probs, int nprob, const float *pack, const float *packd,
+              const float *packs, float *panel, float *uarena, float *ws, FactorStatus *st) {
   using namespace tc;
-  constexpr bool HALF   = MODE != 1;             // 16-bit operands
-  constexpr int  KC     = HALF ? 32 : 16;        // K elements per chunk
-  constexpr int  CHUNKS = KC * (HALF ? 2 : 4) / 16;  // 16-byte chunks per row
-  constexpr int  PARTS  = HALF ? 1 : 2;              // hi (and lo) copies
-  constexpr uint32_t kOperandBytes = kTileM * CHUNKS * 16;  // one operand part
-  constexpr int      kStages       = stages_for(HALF);
+  using C = Cfg<MODE>;
   extern __shared__ __align__(1024) uint8_t smem[];
-  // Buffer layout: [buf][A parts][B parts], each kOperandBytes.
-  __shared__ __align__(8) uint64_t mbar[2];
+  // full[kStages], conv[kStages], empty[kStages], done
+  __shared__ __align__(8) uint64_t bars[3 * kStages + 1];
   __shared__ uint32_t tmem_slot;
+  __shared__ volatile int s_fail;
 
   const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
   // ---- locate problem, tile and K split
@@ -181,218 +271,187 @@ __global__ void __launch_bounds__(tc::kThreads)
     j  = tl / pb.ntm;
     tl = tl % pb.ntm;
   }
-  const int m0 = (pb.lower ? j + tl : tl) * kTileM;
+  const int mt = pb.lower ? j + tl : tl;  // row tile of A
+  const int m0 = mt * kTileM;
   const int n0 = j * kTileN;
   const int M = pb.M, N = pb.N, K = pb.K;
-  const int ks = ((K + pb.splits - 1) / pb.splits + 31) / 32 * 32;
+  const int ks   = ((K + pb.splits - 1) / pb.splits + 31) / 32 * 32;
   const int k_lo = sp * ks, k_hi = min(K, k_lo + ks);
-  const float  *A   = panel + pb.a_ofs;
-  const int64_t lda = pb.lda;
-  const float  *Dk  = D + pb.d_ofs;
+  const int nch  = k_hi > k_lo ? (k_hi - k_lo + C::kKC - 1) / C::kKC : 0;
+  // Stage c reads packed K-groups k_lo/4 + c kKG ..: one contiguous block of
+  // A's row tile, one of B's, and kKC pivots.
+  const float *Ag = pack + pb.pa + static_cast<int64_t>(mt) * pb.prow +
+                    static_cast<int64_t>(k_lo / 4) * PackedFront::kGroupFloats;
+  const float *Bg = pack + pb.pb + static_cast<int64_t>(j) * pb.prow +
+                    static_cast<int64_t>(k_lo / 4) * PackedFront::kGroupFloats;
+  const float *Dg = (C::kHalf ? packs : packd) + pb.pd + k_lo;
 
+  const uint32_t full0 = smem_u32(&bars[0]), conv0 = smem_u32(&bars[kStages]),
+                 empty0 = smem_u32(&bars[2 * kStages]), done = smem_u32(&bars[3 * kStages]);
   // ---- tensor memory and barriers
-  if (warp == 0) {
+  if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
                  ::"r"(smem_u32(&tmem_slot)), "r"(kTmemCols) : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[0])) : "memory");
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[1])) : "memory");
+    s_fail = 0;
+    for (int s = 0; s < kStages; s++) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(full0 + 8 * s) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;" ::"r"(conv0 + 8 * s) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(empty0 + 8 * s) : "memory");
+    }
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(done) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  const uint32_t tmem  = tmem_slot;
-  const uint32_t idesc = make_idesc(MODE == 0 ? kFmtBF16 : MODE == 1 ? kFmtTF32 : kFmtF16);
-  const int      nch   = k_hi > k_lo ? (k_hi - k_lo + KC - 1) / KC : 0;
-  bool           ok    = true;
-  // Raw float32 stages (A then B, column-major 128 x KC each) follow the two
-  // operand buffers in shared memory.
-  float *raw = reinterpret_cast<float *>(smem + 2 * (2 * PARTS * kOperandBytes));
-  auto   issue_stage = [&](int c) {
-    if (c < nch) {
-      float    *sA = raw + (c % kStages) * (2 * kTileM * KC);
-      float    *sB = sA + kTileM * KC;
-      const int k0 = k_lo + c * KC;
-      const int ra = m0 + tid, rb = n0 + tid;
-#pragma unroll
-      for (int k = 0; k < KC; k++) {
-        const bool kin = k0 + k < k_hi;
-        const bool okA = kin && ra < M, okB = kin && rb < N;
-        cp_async4(smem_u32(sA + k * kTileM + tid),
-                  okA ? A + ra + (int64_t)(k0 + k) * lda : A, okA ? 4u : 0u);
-        cp_async4(smem_u32(sB + k * kTileM + tid),
-                  okB ? A + rb + (int64_t)(k0 + k) * lda : A, okB ? 4u : 0u);
-      }
-    }
-    cp_async_commit();  // one group per chunk, empty past the end
-  };
-#pragma unroll
-  for (int c = 0; c < kStages - 1; c++) issue_stage(c);
+  const uint32_t tmem = tmem_slot;
 
-  for (int c = 0; c < nch && ok; c++) {
-    const int buf = c & 1;
-    issue_stage(c + kStages - 1);
-    cp_async_wait<kStages - 1>();  // this thread's copies of chunk c landed
-    if (c >= 2) ok = wait_bounded(smem_u32(&mbar[buf]), ((c - 2) >> 1) & 1);
-    ok = __syncthreads_and(ok);      // and everyone's
-    if (!ok) break;
-    uint8_t     *base = smem + buf * (2 * PARTS * kOperandBytes);
-    const float *sA   = raw + (c % kStages) * (2 * kTileM * KC);
-    const float *sB   = sA + kTileM * KC;
-    const int    k0   = k_lo + c * KC;
-    float        av[KC], bv[KC];
-#pragma unroll
-    for (int k = 0; k < KC; k++) {
-      const float dk = k0 + k < k_hi ? Dk[k0 + k] : 0.0f;
-      // (A D) A^T for 3xTF32; for 16-bit operands the balanced
-      // (A sqrt|D| sign D)(A sqrt|D|)^T, which keeps both within the 16-bit
-      // range when pivots are tiny and multipliers large.
-      float sa = dk, sbv = 1.0f;
-      if (HALF) {
-        const float r = sqrtf(fabsf(dk));
-        sa            = dk < 0.0f ? -r : r;
-        sbv           = r;
-      }
-      av[k] = sA[k * kTileM + tid] * sa;
-      bv[k] = sB[k * kTileM + tid] * sbv;
-    }
-    if (HALF) {
-#pragma unroll
-      for (int q = 0; q < CHUNKS; q++) {
-        uint4 pa, pbk;
-        pa.x  = pack16<MODE>(av[8 * q + 0], av[8 * q + 1]);
-        pa.y  = pack16<MODE>(av[8 * q + 2], av[8 * q + 3]);
-        pa.z  = pack16<MODE>(av[8 * q + 4], av[8 * q + 5]);
-        pa.w  = pack16<MODE>(av[8 * q + 6], av[8 * q + 7]);
-        pbk.x = pack16<MODE>(bv[8 * q + 0], bv[8 * q + 1]);
-        pbk.y = pack16<MODE>(bv[8 * q + 2], bv[8 * q + 3]);
-        pbk.z = pack16<MODE>(bv[8 * q + 4], bv[8 * q + 5]);
-        pbk.w = pack16<MODE>(bv[8 * q + 6], bv[8 * q + 7]);
-        *reinterpret_cast<uint4 *>(base + tid * 16 + q * kLBO)                 = pa;
-        *reinterpret_cast<uint4 *>(base + kOperandBytes + tid * 16 + q * kLBO) = pbk;
-      }
-    } else {
-#pragma unroll
-      for (int q = 0; q < CHUNKS; q++) {
-        uint4     ah, al, bh, bl;
-        uint32_t *ahp = &ah.x, *alp = &al.x, *bhp = &bh.x, *blp = &bl.x;
-#pragma unroll
-        for (int e = 0; e < 4; e++) {
-          const float    x  = av[4 * q + e];
-          const uint32_t xh = to_tf32(x);
-          ahp[e]            = xh;
-          alp[e]            = to_tf32(x - __uint_as_float(xh));
-          const float    y  = bv[4 * q + e];
-          const uint32_t yh = to_tf32(y);
-          bhp[e]            = yh;
-          blp[e]            = to_tf32(y - __uint_as_float(yh));
+  if (warp == 0) {
+    // ---------------- producer
+    if (lane == 0) {
+      int issued = 0;
+      for (int c = 0; c < nch; c++) {
+        const int s = c % kStages, round = c / kStages;
+        if (round > 0 && !wait_bounded(empty0 + 8 * s, (round - 1) & 1)) {
+          s_fail = 1;
+          break;
         }
-        *reinterpret_cast<uint4 *>(base + 0 * kOperandBytes + tid * 16 + q * kLBO) = ah;
-        *reinterpret_cast<uint4 *>(base + 1 * kOperandBytes + tid * 16 + q * kLBO) = al;
-        *reinterpret_cast<uint4 *>(base + 2 * kOperandBytes + tid * 16 + q * kLBO) = bh;
-        *reinterpret_cast<uint4 *>(base + 3 * kOperandBytes + tid * 16 + q * kLBO) = bl;
+        const uint32_t base = smem_u32(smem + s * C::kStage);
+        arrive_expect_tx(full0 + 8 * s, C::kTx);
+        bulk_load(base + C::kA, Ag + static_cast<int64_t>(c) * C::kKG * PackedFront::kGroupFloats,
+                  C::kRaw, full0 + 8 * s);
+        bulk_load(base + C::kB, Bg + static_cast<int64_t>(c) * C::kKG * PackedFront::kGroupFloats,
+                  C::kRaw, full0 + 8 * s);
+        bulk_load(base + C::kD, Dg + c * C::kKC, C::kKC * 4, full0 + 8 * s);
+        issued = c + 1;
       }
+      // No copy may still target shared memory at exit: the last stage issued
+      // into each slot has landed (no later round was issued into it).
+      for (int c = max(0, issued - kStages); c < issued; c++)
+        wait_bounded(full0 + 8 * (c % kStages), (c / kStages) & 1);
     }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
-    if (tid == 0) {
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t sbase = smem_u32(base);
-      // Each MMA consumes two 16-byte K-chunks (16 half-precision or 8 tf32).
-#pragma unroll
-      for (int s = 0; s < CHUNKS / 2; s++) {
-        const uint32_t off = s * 2 * kLBO;
-        if (HALF) {
-          mma(0, tmem, make_desc(sbase + off), make_desc(sbase + kOperandBytes + off), idesc,
-              (c > 0 || s > 0) ? 1u : 0u);
-        } else {
-          const uint64_t ahd = make_desc(sbase + 0 * kOperandBytes + off);
-          const uint64_t ald = make_desc(sbase + 1 * kOperandBytes + off);
-          const uint64_t bhd = make_desc(sbase + 2 * kOperandBytes + off);
-          const uint64_t bld = make_desc(sbase + 3 * kOperandBytes + off);
-          mma(1, tmem, ahd, bhd, idesc, (c > 0 || s > 0) ? 1u : 0u);
-          mma(1, tmem, ahd, bld, idesc, 1u);
-          mma(1, tmem, ald, bhd, idesc, 1u);
+    __syncwarp();
+  } else if (warp == 1) {
+    // ---------------- MMA issuer
+    if (lane == 0) {
+      const uint32_t idesc = make_idesc(MODE == 0 ? kFmtBF16 : MODE == 1 ? kFmtTF32 : kFmtF16);
+      for (int c = 0; c < nch; c++) {
+        const int s = c % kStages, round = c / kStages;
+        if (!wait_bounded(conv0 + 8 * s, round & 1)) {
+          s_fail = 1;
+          break;
         }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t base = smem_u32(smem + s * C::kStage);
+        // Each MMA consumes two K-groups: 8 tf32 or 16 16-bit columns.
+        constexpr int kSteps = MODE == 1 ? C::kKG / 2 : C::kKG / 4;
+#pragma unroll
+        for (int q = 0; q < kSteps; q++) {
+          const uint32_t off = q * 2 * kGroup;
+          const uint32_t acc = (c > 0 || q > 0) ? 1u : 0u;
+          if (MODE == 1) {
+            const uint64_t ahd = make_desc(base + C::kA + off);
+            const uint64_t bhd = make_desc(base + C::kB + off);
+            const uint64_t ald = make_desc(base + C::kAlo + off);
+            const uint64_t bld = make_desc(base + C::kBlo + off);
+            mma<true>(tmem, ahd, bhd, idesc, acc);
+            mma<true>(tmem, ahd, bld, idesc, 1u);
+            mma<true>(tmem, ald, bhd, idesc, 1u);
+          } else {
+            mma<false>(tmem, make_desc(base + C::kA + off), make_desc(base + C::kB + off), idesc,
+                       acc);
+          }
+        }
+        commit(empty0 + 8 * s);
       }
-      commit(smem_u32(&mbar[buf]));
+      // Tracks every MMA issued above (none: arrives at once).
+      commit(done);
     }
-  }
-  cp_async_wait<0>();  // no copy may still target shared memory at exit
-  // All MMAs done: the last commit tracks every earlier one of this thread.
-  if (ok && nch > 0) ok = wait_bounded(smem_u32(&mbar[(nch - 1) & 1]), ((nch - 1) >> 1) & 1);
-  ok = __syncthreads_and(ok);
-  if (!ok) {
-    if (tid == 0) atomicExch(&st->timeout, 1);
-    // Let any MMA still in flight finish before the memory is released.
-    if (nch > 0) wait_bounded(smem_u32(&mbar[(nch - 1) & 1]), ((nch - 1) >> 1) & 1);
-  }
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  if (ok) {
-    const int row  = m0 + warp * 32 + lane;
-    float    *Cout = (pb.c_in_u ? uarena : panel) + pb.c_ofs;
-    float    *W    = pb.splits > 1 ? ws + pb.ws_ofs +
-                                         (static_cast<int64_t>(tile) * pb.splits + sp) * (kTileM * kTileN)
-                                   : nullptr;
+    __syncwarp();
+  } else if (warp >= 4) {
+    // ---------------- converters, then the epilogue
+    const int m = tid - 128;
+    for (int c = 0; c < nch; c++) {
+      const int s = c % kStages, round = c / kStages;
+      if (!wait_bounded(full0 + 8 * s, round & 1)) {
+        s_fail = 1;
+        break;
+      }
+      convert_row<MODE>(smem + s * C::kStage, m);
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      arrive(conv0 + 8 * s);
+    }
+    bool ok = wait_bounded(done, 0);
+    if (!ok) s_fail = 1;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    ok = ok && s_fail == 0;
+    ok = __all_sync(0xffffffffu, ok);
+    if (ok) {
+      const int ew   = warp - 4;  // tensor-memory lanes 32 ew .. 32 ew + 31
+      const int lr   = ew * 32 + lane;
+      const int mrow = m0 + lr;
+      const int row  = mrow < M ? gemm_out_row(pb, mrow) : -1;
+      float    *Cout = (pb.c_in_u ? uarena : panel) + pb.c_ofs;
+      float    *W    = pb.splits > 1
+                           ? ws + pb.ws_ofs +
+                              (static_cast<int64_t>(tile) * pb.splits + sp) * (kTileM * kTileN)
+                           : nullptr;
 #pragma unroll
-    for (int cb = 0; cb < kTileN / 32; cb++) {
-      uint32_t       r[32];
-      const uint32_t taddr = tmem + (static_cast<uint32_t>(warp * 32) << 16) + cb * 32;
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-          "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-          "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
-            "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
-            "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]),
-            "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-            "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]),
-            "=r"(r[30]), "=r"(r[31])
-          : "r"(taddr));
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (nch == 0)  // an empty K range leaves the accumulator unwritten
+      for (int cb = 0; cb < kTileN / 32; cb++) {
+        uint32_t       r[32];
+        const uint32_t taddr = tmem + (static_cast<uint32_t>(ew * 32) << 16) + cb * 32;
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+            "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+            "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+              "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+              "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]),
+              "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+              "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]),
+              "=r"(r[30]), "=r"(r[31])
+            : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (nch == 0)  // an empty K range leaves the accumulator unwritten
 #pragma unroll
-        for (int q = 0; q < 32; q++) r[q] = 0u;
-      const int lr = warp * 32 + lane;
-      if (W) {
+          for (int q = 0; q < 32; q++) r[q] = 0u;
+        if (W) {
 #pragma unroll
-        for (int q = 0; q < 32; q++) W[lr + (cb * 32 + q) * kTileM] = __uint_as_float(r[q]);
-      } else if (row < M) {
+          for (int q = 0; q < 32; q++) W[lr + (cb * 32 + q) * kTileM] = __uint_as_float(r[q]);
+        } else if (row >= 0) {
 #pragma unroll
-        for (int q = 0; q < 32; q++) {
-          const int col = n0 + cb * 32 + q;
-          if (col < N && (!pb.lower || row >= col))
-            Cout[row + (int64_t)col * pb.ldc] -= __uint_as_float(r[q]);
+          for (int q = 0; q < 32; q++) {
+            const int col = n0 + cb * 32 + q;
+            if (col < N && (!pb.lower || row >= col))
+              Cout[row + (int64_t)col * pb.ldc] -= __uint_as_float(r[q]);
+          }
         }
       }
+    } else if (lane == 0) {
+      atomicExch(&st->timeout, 1);
+      // Let any MMA still in flight finish before the memory is released.
+      wait_bounded(done, 0);
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  if (warp == 0)
+  if (warp == 1)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                  "r"(kTmemCols) : "memory");
 }
 
 int tc_gemm_smem_bytes(int mode) {
-  const bool half = mode != 1;
-  const int  kc = half ? 32 : 16, chunks = kc * (half ? 2 : 4) / 16;
-  const int  parts = half ? 1 : 2;
-  // Two operand buffers of A and B parts, then the raw float32 stages; at
-  // least 48 KB so that no more than four CTAs (4 x 128 tensor-memory
-  // columns) share an SM.
-  const int bytes = 2 * 2 * parts * tc::kTileM * chunks * 16 +
-                    tc::stages_for(half) * 2 * tc::kTileM * kc * 4;
-  return bytes < 49152 ? 49152 : bytes;
+  const uint32_t stage = mode == 1 ? tc::Cfg<1>::kStage : tc::Cfg<0>::kStage;
+  return static_cast<int>(tc::kStages * stage);
 }
 
 template <int MODE>
-static void launch_mode(const GemmProb *probs, int nprob, int tiles, float *panel,
-                        float *uarena, const float *D, float *ws, FactorStatus *st,
-                        cudaStream_t s) {
+static void launch_mode(const GemmProb *probs, int nprob, int tiles, const float *pack,
+                        const float *packd, const float *packs, float *panel, float *uarena,
+                        float *ws, FactorStatus *st, cudaStream_t s) {
   static bool attr = false;
   const int   smem = tc_gemm_smem_bytes(MODE);
   if (!attr) {
@@ -400,14 +459,19 @@ static void launch_mode(const GemmProb *probs, int nprob, int tiles, float *pane
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     attr = true;
   }
-  launch(k_gemm_tc<MODE>, tiles, tc::kThreads, smem, s, probs, nprob, panel, uarena, D, ws, st);
+  launch(k_gemm_tc<MODE>, tiles, tc::kThreads, smem, s, probs, nprob, pack, packd, packs, panel,
+         uarena, ws, st);
 }
 
-void launch_gemm_tc(int mode, const GemmProb *probs, int nprob, int tiles, float *panel,
-                    float *uarena, const float *D, float *ws, FactorStatus *st, cudaStream_t s) {
-  if (mode == 0) launch_mode<0>(probs, nprob, tiles, panel, uarena, D, ws, st, s);
-  else if (mode == 1) launch_mode<1>(probs, nprob, tiles, panel, uarena, D, ws, st, s);
-  else launch_mode<2>(probs, nprob, tiles, panel, uarena, D, ws, st, s);
+void launch_gemm_tc(int mode, const GemmProb *probs, int nprob, int tiles, const float *pack,
+                    const float *packd, const float *packs, float *panel, float *uarena,
+                    float *ws, FactorStatus *st, cudaStream_t s) {
+  if (mode == 0)
+    launch_mode<0>(probs, nprob, tiles, pack, packd, packs, panel, uarena, ws, st, s);
+  else if (mode == 1)
+    launch_mode<1>(probs, nprob, tiles, pack, packd, packs, panel, uarena, ws, st, s);
+  else
+    launch_mode<2>(probs, nprob, tiles, pack, packd, packs, panel, uarena, ws, st, s);
 }
 
 }  // namespace mpir

@@ -189,10 +189,13 @@ def update_engine(monkeypatch):
     return set_engine
 
 
-def test_tf32x3_update_matches_reference(oracle_lib, ref_lib, update_engine):
-    """3xTF32 tensor-core trailing updates keep the float32 factor within the
-    same 1e-5 of the reference's float32 QDLDL factor."""
-    update_engine("tf32x3")
+@pytest.mark.parametrize("engine", ["tf32x3", "simt"])
+def test_update_engine_matches_reference(oracle_lib, ref_lib, update_engine, engine):
+    """3xTF32 tensor-core trailing updates (the float32 default) and the
+    float32 SIMT updates both keep the float32 factor within the same 1e-5 of
+    the reference's float32 QDLDL factor.  grid 12 has fronts wider than one
+    128-column block, so the left-looking updates and the split K run."""
+    update_engine(engine)
     s = kkt.grid3d(grid=12, seed=9)
     solver = mp.GmresLDLIR()
     solver.Compute(s.Ap, s.Ai, s.Ax)
