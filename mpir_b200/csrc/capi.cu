@@ -309,6 +309,12 @@ static int qdldl_solve_phases(int64_t n, const int64_t *Lp, const int64_t *Li, c
     MPIR_CUDA(cudaMemcpyAsync(xh.data(), xd.as<void>(), n * sizeof(double),
                               cudaMemcpyDeviceToHost, sg.s));
     MPIR_CUDA(cudaStreamSynchronize(sg.s));
+    int32_t wait_err = 0;
+    MPIR_CUDA(cudaMemcpy(&wait_err, ws.err.as<void>(), sizeof wait_err, cudaMemcpyDeviceToHost));
+    if (wait_err != 0) {
+      g_err = "a bounded device wait of the triangular solves ran out";
+      return MPIR_ERR_TIMEOUT;
+    }
     for (int64_t i = 0; i < n; i++) {
       if (x_prec == kF64)
         static_cast<double *>(x)[i] = xh[i];

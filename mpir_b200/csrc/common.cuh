@@ -52,16 +52,6 @@ struct StepDesc {
   int32_t trsm_tile0; // first TRSM row tile of this desc within the step
   int32_t upd_tile0;  // first update tile of this desc within the step
   int32_t upd_panel_tiles;
-  // Solve fields: the front's vector at zofs (h doubles) in the solve
-  // workspace; forward row tiles and backward row chunks of this desc within
-  // the step; backward partial sums at bpart (chunks x kNB doubles); the
-  // desc's global index (for its completion counter).
-  int64_t zofs;
-  int64_t bpart;
-  int32_t fsolve_tile0;
-  int32_t bsolve_chunk0;
-  int32_t bsolve_chunks;
-  int32_t id;
   // Packed copy of the front for the tensor-core updates (see PackedFront):
   // float offset of the front's packed rows and pivots, K-groups per row
   // tile, and the packed row of the first off-diagonal row.
@@ -69,6 +59,28 @@ struct StepDesc {
   int64_t pd;
   int32_t pk_g;
   int32_t pk_wt;
+};
+
+// One large front in the triangular solves.  The forward solve of a level
+// runs one CTA per row block of 128 rows of each front (front-major, row
+// blocks ascending); the backward solve one CTA per 128-row chunk of the
+// off-diagonal rows (partial sums for all columns) and then one CTA per
+// column block (front-major, last block first).  CTAs take their work in
+// ticket order, so every block they wait for belongs to an earlier ticket.
+struct SolveFront {
+  int64_t panel;   // panel offset (h x w, column-major)
+  int64_t zofs;    // front vector in the solve workspace (h doubles)
+  int64_t linv;    // float64 inverse of diagonal block 0 (block b at + b kNB^2)
+  int64_t part;    // backward chunk partials (chunks x w doubles)
+  int64_t rows;    // the front's row index set at srows[rows ..]
+  int64_t gptr;    // row i's child contributions: zbuf[gsrc[e]] for e in
+                   // gp[gptr + i] .. gp[gptr + i + 1], in child order
+  int32_t h, w, nb;
+  int32_t col0;    // permuted index of the front's first column
+  int32_t flag0;   // first of the front's nb ready flags
+  int32_t fwd0;    // first forward CTA of the front in its level
+  int32_t chunk0, chunks;  // backward chunk CTAs
+  int32_t own0;    // first backward column-block CTA
 };
 
 // Packed copy of a large front's L for the tensor-core updates.  Rows are
@@ -160,5 +172,9 @@ constexpr int64_t kZeroChunk = 16384;  // floats per zero-fill CTA
 constexpr int kSolveRows = 128;        // rows per forward-solve CTA
 constexpr int kSolveChunk = 128;       // rows per backward-solve CTA
 constexpr int kSolveThreads = 512;     // 4 column quarters x 128 rows
+// Fronts of at most this width and height are solved by one warp each
+// (column by column); larger ones by the SolveFront launches.
+constexpr int kWarpSolveW = 32;
+constexpr int kWarpSolveH = 256;
 
 }  // namespace mpir

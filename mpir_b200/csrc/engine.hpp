@@ -74,7 +74,7 @@ struct LevelPlan {
   };
   std::vector<Round> ea_rounds;
   struct Step {
-    int32_t begin, count, trsm_tiles, upd_tiles, fsolve_tiles, bsolve_chunks;
+    int32_t begin, count, trsm_tiles, upd_tiles;
     // left-looking update of this block column before its diagonal block
     int32_t ll_begin, ll_count, ll_tiles, ll_rtiles;
   };
@@ -82,7 +82,12 @@ struct LevelPlan {
   // update matrices of the level's large fronts, after their last step
   int32_t u_begin = 0, u_count = 0, u_tiles = 0, u_rtiles = 0;
   // Solve: large fronts' gather list = large list; small fronts handled by
-  // one thread block each.
+  // one warp each; large fronts by the SolveFront launches: fronts
+  // [sf_begin, sf_begin + sf_count), forward CTAs, backward chunk CTAs and
+  // backward column-block CTAs.
+  int32_t sf_begin = 0, sf_count = 0;
+  int32_t sw_begin = 0, sw_count = 0;  // warp-solved fronts (swarp list)
+  int32_t fwd_items = 0, bwd_chunk_items = 0, bwd_owner_items = 0;
 };
 
 // Everything the kernels need about one analysed pattern.
@@ -93,15 +98,22 @@ class Plan {
   int64_t                linv_elems = 0;
   int64_t                nnz_full   = 0;
   int64_t                ndesc      = 0;  // step descriptors in total
-  int64_t                bpart_elems = 0; // backward partial sums (doubles)
+  int64_t                spart_elems = 0; // backward chunk partials (doubles)
+  // Solve synchronisation words: 2 tickets per level, then the forward and
+  // the backward ready flags (nflags each); reset before every solve.
+  int64_t                nflags = 0, sync_elems = 0;
   double                 update_flops = 0, trsm_flops = 0, panel_read_bytes = 0;
   // Pattern arrays on the device.
   DeviceBuffer amap, arow, acol, diag_pos, Kp, Kj, Ksrc;
   DeviceBuffer sfirst, srowptr, srows, srel, slofs, uofs, zofs, child_ptr,
       child_list, perm;
-  DeviceBuffer small_list, large_list, steps, ea_tasks, zero_segs, linv_ofs_d, gemm_probs;
+  DeviceBuffer small_list, large_list, steps, ea_tasks, zero_segs, linv_ofs_d, gemm_probs,
+      solve_fronts, swarp_list, sblock_list, gp, gsrc;
   int64_t      ws_elems = 0;  // split-K partial tiles (floats)
   std::vector<int32_t> h_small, h_large;
+  // Solve lists: fronts solved by one warp, fronts with a SolveFront entry
+  // (same order as the SolveFront array).
+  std::vector<int32_t> h_swarp, h_sblock;
   std::vector<int64_t> linv_ofs;  // per supernode, -1 for small fronts
   // Packed fronts (PackedFront) of the large fronts: float offsets of the
   // packed rows and of the packed pivots per supernode (-1 for small

@@ -603,7 +603,12 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
   // Persistent Linv storage for the large fronts.
   linv_ofs.assign(ns, -1);
   linv_elems   = 0;
-  bpart_elems  = 0;
+  spart_elems  = 0;
+  nflags       = 0;
+  h_swarp.clear();
+  h_sblock.clear();
+  std::vector<int64_t> gp_h, gsrc_h;
+  std::vector<SolveFront> sfronts;
   update_flops = 0;
   trsm_flops   = 0;
   pk_ofs.assign(ns, -1);
@@ -726,9 +731,8 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
     for (int32_t q = L.large_begin; q < L.large_begin + L.large_count; q++)
       maxw = std::max(maxw, S.w(h_large[q]));
     for (int64_t kb = 0; kb < maxw; kb += kNB) {
-      LevelPlan::Step st{static_cast<int32_t>(descs.size()), 0, 0, 0, 0, 0,
+      LevelPlan::Step st{static_cast<int32_t>(descs.size()), 0, 0, 0,
                          static_cast<int32_t>(probs.size()), 0, 0, 0};
-      int64_t         bpart = 0;
       for (int32_t q = L.large_begin; q < L.large_begin + L.large_count; q++) {
         const int64_t J = h_large[q], w = S.w(J), h = S.h(J);
         if (w <= kb) continue;
@@ -774,25 +778,71 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
         d.pd           = pd_ofs[J];
         d.pk_g         = static_cast<int32_t>(pk_groups(J));
         d.pk_wt        = static_cast<int32_t>(pk_wt(J));
-        d.zofs         = S.zofs[J];
-        d.fsolve_tile0 = st.fsolve_tiles;
-        st.fsolve_tiles += static_cast<int32_t>(
-            std::max<int64_t>(1, (M + kSolveRows - 1) / kSolveRows));
-        d.bsolve_chunks  = static_cast<int32_t>(
-            std::max<int64_t>(1, (M + kSolveChunk - 1) / kSolveChunk));
-        d.bsolve_chunk0  = st.bsolve_chunks;
-        st.bsolve_chunks += d.bsolve_chunks;
-        d.bpart = bpart;
-        bpart += d.bsolve_chunks * (int64_t)kNB;
-        d.id    = static_cast<int32_t>(descs.size());
         descs.push_back(d);
         st.count++;
       }
       st.ll_count = static_cast<int32_t>(probs.size()) - st.ll_begin;
       finish_launch(st.ll_begin, st.ll_count, st.ll_tiles, st.ll_rtiles);
       L.steps.push_back(st);
-      bpart_elems = std::max(bpart_elems, bpart);
     }
+    // Solve work of the level: narrow, short fronts one warp each, the rest
+    // through SolveFront entries.
+    L.sw_begin = static_cast<int32_t>(h_swarp.size());
+    L.sf_begin = static_cast<int32_t>(sfronts.size());
+    for (int32_t q = L.small_begin; q < L.small_begin + L.small_count; q++)
+      h_swarp.push_back(h_small[q]);
+    int64_t spart = 0;
+    for (int32_t q = L.large_begin; q < L.large_begin + L.large_count; q++) {
+      const int64_t J = h_large[q], w = S.w(J), h = S.h(J);
+      if (w <= kWarpSolveW && h <= kWarpSolveH) {
+        h_swarp.push_back(J);
+        continue;
+      }
+      h_sblock.push_back(J);
+      SolveFront    f{};
+      // Child contributions per row, in child order (the forward solve adds
+      // them in this order).
+      f.rows = S.srowptr[J];
+      f.gptr = static_cast<int64_t>(gp_h.size());
+      {
+        std::vector<int64_t> cnt(h + 1, 0);
+        for (int64_t c = S.child_ptr[J]; c < S.child_ptr[J + 1]; c++) {
+          const int64_t C = S.child_list[c], wc = S.w(C), rc = S.h(C) - wc;
+          for (int64_t a = 0; a < rc; a++) cnt[S.srel[S.srowptr[C] + wc + a] + 1]++;
+        }
+        for (int64_t i = 0; i < h; i++) cnt[i + 1] += cnt[i];
+        const int64_t base = static_cast<int64_t>(gsrc_h.size());
+        for (int64_t i = 0; i <= h; i++) gp_h.push_back(base + cnt[i]);
+        gsrc_h.resize(base + cnt[h]);
+        for (int64_t c = S.child_ptr[J]; c < S.child_ptr[J + 1]; c++) {
+          const int64_t C = S.child_list[c], wc = S.w(C), rc = S.h(C) - wc;
+          for (int64_t a = 0; a < rc; a++)
+            gsrc_h[base + cnt[S.srel[S.srowptr[C] + wc + a]]++] = S.zofs[C] + wc + a;
+        }
+      }
+      f.panel  = S.slofs[J];
+      f.zofs   = S.zofs[J];
+      f.linv   = linv_ofs[J];
+      f.h      = static_cast<int32_t>(h);
+      f.w      = static_cast<int32_t>(w);
+      f.nb     = static_cast<int32_t>((w + kNB - 1) / kNB);
+      f.col0   = static_cast<int32_t>(S.sfirst[J]);
+      f.flag0  = static_cast<int32_t>(nflags);
+      nflags += f.nb;
+      f.fwd0   = L.fwd_items;
+      L.fwd_items += static_cast<int32_t>((h + kNB - 1) / kNB);
+      f.chunks = static_cast<int32_t>((h - w + kNB - 1) / kNB);
+      f.chunk0 = L.bwd_chunk_items;
+      L.bwd_chunk_items += f.chunks;
+      f.part   = spart;
+      spart += static_cast<int64_t>(f.chunks) * w;
+      f.own0   = L.bwd_owner_items;
+      L.bwd_owner_items += f.nb;
+      sfronts.push_back(f);
+    }
+    L.sf_count  = static_cast<int32_t>(sfronts.size()) - L.sf_begin;
+    L.sw_count  = static_cast<int32_t>(h_swarp.size()) - L.sw_begin;
+    spart_elems = std::max(spart_elems, spart);
     L.u_begin = static_cast<int32_t>(probs.size());
     for (int32_t q = L.large_begin; q < L.large_begin + L.large_count; q++) {
       const int64_t J = h_large[q], w = S.w(J), h = S.h(J), r = h - w;
@@ -849,6 +899,12 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
   zero_segs  = upload(segs, s);
   gemm_probs = upload(probs, s);
   linv_ofs_d = upload(linv_ofs, s);
+  solve_fronts = upload(sfronts, s);
+  swarp_list   = upload(h_swarp, s);
+  sblock_list  = upload(h_sblock, s);
+  gp           = upload(gp_h, s);
+  gsrc         = upload(gsrc_h, s);
+  sync_elems   = 2 * static_cast<int64_t>(levels.size()) + 2 * nflags;
   MPIR_CUDA(cudaStreamSynchronize(s));
 }
 

@@ -322,6 +322,15 @@ int Solver::solve_device(const double *d_b, double *d_x, Report *rep) {
   MPIR_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
   st.solve_ms  = ms;
   st.factor_ms = last_factor_ms;
+  // A ready-flag wait of the triangular solves that gave up (sticky word).
+  int32_t wait_err = 0;
+  MPIR_CUDA(cudaMemcpy(&wait_err, ws_.err.as<void>(), sizeof wait_err, cudaMemcpyDeviceToHost));
+  if (wait_err != 0) {
+    MPIR_CUDA(cudaMemset(ws_.err.as<void>(), 0, sizeof wait_err));
+    st.status = -5;
+    if (rep) *rep = st;
+    return -5;
+  }
   if (rep) *rep = st;
   return kOk;
 }

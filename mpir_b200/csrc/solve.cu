@@ -26,36 +26,73 @@
 namespace mpir {
 
 constexpr int kWarpsPerCta = 4;
-constexpr int kSmallH      = kSmallFront;
+constexpr int kSmallH      = kWarpSolveH;
 
 // ---------------------------------------------------------------------------
-// y = Linv z for one 128-column block with 512 threads: thread (q, i) adds
-// the 32 products of row i in column slice q (unrolled, independent loads);
-// slices are summed in order.  Linv is lower triangular, column-major.
-__device__ __forceinline__ double block_lower_apply(const double *Lv, const double *zb, int nb,
-                                                    double (*part)[kNB]) {
+// Products with the float64 inverse of one diagonal block (128 x 128), 512
+// threads: thread (q, i) takes row (or column) i and the 32 terms of slice q;
+// slices are summed in order.  Each thread first copies the inverse entries
+// it will use into shared memory with cp.async (asynchronous, no registers
+// held): a CTA does this when it starts, so the product at the end of its
+// wait chain reads shared memory only.  Forward layout: the lower triangle by
+// columns (column j from row j at 128 j - j (j - 1) / 2); backward layout: the
+// lower triangle by rows (row i at i (i + 1) / 2); both keep a warp's 32
+// accesses on consecutive addresses.
+constexpr int kTri = kNB * (kNB + 1) / 2;
+
+__device__ __forceinline__ void cp_async8(double *dst, const double *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(
+                   static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+               "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
+// Stage Linv (column-major, leading dimension kNB) for y = Linv z.
+__device__ __forceinline__ void stage_lower(const double *Lv, double *Ls, int nb) {
   const int tid = threadIdx.x, i = tid % kNB, q = tid / kNB;
-  double    acc = 0.0;
-#pragma unroll
   for (int jj = 0; jj < kNB / 4; jj++) {
     const int j = q * (kNB / 4) + jj;
-    if (j <= i && i < nb) acc += Lv[i + j * kNB] * zb[j];
+    if (j <= i && i < nb) cp_async8(Ls + kNB * j - j * (j - 1) / 2 + (i - j), Lv + i + j * kNB);
+  }
+}
+
+// y = Linv z from the staged copy.
+__device__ __forceinline__ double block_lower_apply(const double *Ls, const double *zb, int nb,
+                                                    double (*part)[kNB]) {
+  const int tid = threadIdx.x, i = tid % kNB, q = tid / kNB;
+  cp_async_wait_all();
+  double acc = 0.0;
+#pragma unroll 8
+  for (int jj = 0; jj < kNB / 4; jj++) {
+    const int j = q * (kNB / 4) + jj;
+    if (j <= i && i < nb) acc += Ls[kNB * j - j * (j - 1) / 2 + (i - j)] * zb[j];
   }
   part[q][i] = acc;
   __syncthreads();
   return (part[0][i] + part[1][i]) + (part[2][i] + part[3][i]);
 }
 
-// x = Linv^T v with the row-major copy Lt (Lt[i * kNB + j] = Linv[i][j]):
-// thread (q, j) adds rows i >= j of slice q.
-__device__ __forceinline__ double block_upper_apply(const double *Lt, const double *v, int nb,
-                                                    double (*part)[kNB]) {
+// Stage the row-major copy Lt (Lt[i * kNB + j] = Linv[i][j]) for x = Linv^T v.
+__device__ __forceinline__ void stage_upper(const double *Lt, double *Ls, int nb) {
   const int tid = threadIdx.x, j = tid % kNB, q = tid / kNB;
-  double    acc = 0.0;
-#pragma unroll
   for (int ii = 0; ii < kNB / 4; ii++) {
     const int i = q * (kNB / 4) + ii;
-    if (i >= j && i < nb) acc += Lt[i * kNB + j] * v[i];
+    if (i >= j && i < nb) cp_async8(Ls + i * (i + 1) / 2 + j, Lt + i * kNB + j);
+  }
+}
+
+// x = Linv^T v from the staged copy: thread (q, j) adds rows i >= j of slice q.
+__device__ __forceinline__ double block_upper_apply(const double *Ls, const double *v, int nb,
+                                                    double (*part)[kNB]) {
+  const int tid = threadIdx.x, j = tid % kNB, q = tid / kNB;
+  cp_async_wait_all();
+  double acc = 0.0;
+#pragma unroll 8
+  for (int ii = 0; ii < kNB / 4; ii++) {
+    const int i = q * (kNB / 4) + ii;
+    if (i >= j && i < nb) acc += Ls[i * (i + 1) / 2 + j] * v[i];
   }
   part[q][j] = acc;
   __syncthreads();
@@ -103,82 +140,133 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta)
   }
 }
 
-// Large fronts: right-hand side plus children's update vectors, then the
-// solution of the first column block, y_0 = Linv_0 z_0, stored into x.
-__global__ void __launch_bounds__(kSolveThreads)
-    k_fwd_gather(const int32_t *list, const int64_t *sfirst, const int64_t *srowptr,
-                 const int64_t *child_ptr, const int32_t *child_list, const int32_t *srel,
-                 const int64_t *zofs, const int64_t *linv_ofs, const double *linv64, double *x,
-                 double *zbuf) {
-  __shared__ double zb[kNB];
-  __shared__ double part[4][kNB];
-  const int     J = list[blockIdx.x];
-  const int64_t f = sfirst[J];
-  const int64_t w = sfirst[J + 1] - f;
-  const int64_t h = srowptr[J + 1] - srowptr[J];
-  double       *z = zbuf + zofs[J];
-  for (int64_t i = threadIdx.x; i < h; i += blockDim.x) z[i] = i < w ? x[f + i] : 0.0;
-  __syncthreads();
-  for (int64_t c = child_ptr[J]; c < child_ptr[J + 1]; c++) {
-    const int      C  = child_list[c];
-    const int64_t  wc = sfirst[C + 1] - sfirst[C];
-    const int64_t  rc = srowptr[C + 1] - srowptr[C] - wc;
-    const int32_t *rl = srel + srowptr[C] + wc;
-    const double  *zc = zbuf + zofs[C] + wc;
-    for (int64_t a = threadIdx.x; a < rc; a += blockDim.x) z[rl[a]] += zc[a];
-    __syncthreads();
+
+// Ready flags between the CTAs of one solve launch (release / acquire at GPU
+// scope).  A wait gives up after a few seconds, sets the sticky error word
+// and returns false; once that word is set every other wait returns false at
+// once, so one failure ends the launch quickly.
+__device__ __forceinline__ int32_t ld_acquire(const int32_t *p) {
+  int32_t v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(int32_t *p, int32_t v) {
+  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ bool wait_flag(const int32_t *p, int32_t *err) {
+  for (long it = 0; it < (1L << 22); it++) {
+    if (ld_acquire(p) != 0) return true;
+    if (*reinterpret_cast<volatile int32_t *>(err) != 0) return false;
+    if (it >= 64) __nanosleep(32);
   }
-  const int nb = static_cast<int>(w < kNB ? w : kNB);
-  if (threadIdx.x < nb) zb[threadIdx.x] = z[threadIdx.x];
-  __syncthreads();
-  const double y = block_lower_apply(linv64 + linv_ofs[J], zb, nb, part);
-  if (threadIdx.x < nb) x[f + threadIdx.x] = y;
+  atomicExch(err, 1);
+  return false;
 }
 
-// One column block of the large fronts.  The block's solution y is already
-// in x; each CTA updates its 128 rows below the block, z_r -= L_{r,b} y, with
-// the block's columns split in four quarters over the CTA's 512 threads.
-// The first CTA's rows are the next block, so once they are updated it
-// solves that block, y' = Linv_{b+1} z_{b+1}, into x for the next step.
-__global__ void __launch_bounds__(kSolveThreads)
-    k_fwd_step(const StepDesc *descs, int ndesc, const float *panel,
-               const double *linv64, double *x, double *zbuf) {
-  __shared__ double y[kNB];
-  __shared__ double part[4][kNB];
-  const int         t  = blockIdx.x;
-  int               lo = 0, hi = ndesc - 1;
+// CTA-wide ticket: the order in which CTAs of a launch take their work.
+__device__ __forceinline__ int take_ticket(int32_t *counter) {
+  __shared__ int s_ticket;
+  if (threadIdx.x == 0) s_ticket = atomicAdd(counter, 1);
+  __syncthreads();
+  return s_ticket;
+}
+
+__device__ __forceinline__ int find_front(const SolveFront *fr, int nfr, int item,
+                                          int SolveFront::*first) {
+  int lo = 0, hi = nfr - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) / 2;
-    if (descs[mid].fsolve_tile0 <= t) lo = mid; else hi = mid - 1;
+    if (fr[mid].*first <= item) lo = mid; else hi = mid - 1;
   }
-  const StepDesc d     = descs[lo];
-  const int      local = t - d.fsolve_tile0;
-  const int      tid   = threadIdx.x;
-  const int64_t  h     = d.h;
-  double        *z     = zbuf + d.zofs;
-  if (tid < d.nbk) y[tid] = x[(int64_t)d.col0 + d.kb + tid];
-  __syncthreads();
-  const int     rr = tid % kSolveRows, qq = tid / kSolveRows;
-  const int64_t r  = (int64_t)d.kb + d.nbk + (int64_t)local * kSolveRows + rr;
-  double        acc = 0.0;
-  if (r < h) {
-    const float *P  = panel + d.panel + r + (int64_t)d.kb * h;
-    const int    k1 = min(d.nbk, (qq + 1) * (kNB / 4));
-    for (int k = qq * (kNB / 4); k < k1; k++)
-      acc += static_cast<double>(P[(int64_t)k * h]) * y[k];
+  return lo;
+}
+
+// Forward solve of the large fronts of one level: one CTA per 128-row block
+// R of a front.  z_R -= L_{R,b} y_b for the column blocks b left of R, in
+// order, each as soon as y_b is ready: thread (q, i) takes row i and the
+// columns 32q .. 32q+31 of each tile, loads its L values before the wait, and
+// each warp waits for the flag and stages y_b on its own (no CTA barrier per
+// tile); the four quarters are added in order at the end.  A diagonal row
+// block then solves y_R = Linv_R z_R into x and releases flag R; rows at or
+// past w are the front's update vector for its parent.
+__global__ void __launch_bounds__(kSolveThreads, 1)
+    k_fwd_fronts(const SolveFront *fr, int nfr, const float *panel, const double *linv64,
+                 const int64_t *gp, const int64_t *gsrc, double *x, double *zbuf,
+                 int32_t *tickets, int32_t *flags, int32_t *err) {
+  extern __shared__ double tri[];  // kTri doubles: the staged Linv_R
+  __shared__ double ys[kNB];
+  __shared__ double yw[kSolveThreads / 32][32];
+  __shared__ double part[4][kNB];
+  const int         item = take_ticket(tickets);
+  const SolveFront  F    = fr[find_front(fr, nfr, item, &SolveFront::fwd0)];
+  const int         R    = item - F.fwd0;
+  if (R < F.nb)
+    stage_lower(linv64 + F.linv + static_cast<int64_t>(R) * kNB * kNB, tri,
+                min(kNB, F.w - R * kNB));
+  const int         tid = threadIdx.x, rr = tid % kNB, qq = tid / kNB;
+  const int         warp = tid / 32, lane = tid % 32;
+  const int64_t     h = F.h;
+  const int         w = F.w;
+  const int64_t     r = static_cast<int64_t>(R) * kNB + rr;
+  const float      *P  = panel + F.panel;
+  int32_t          *fl = flags + F.flag0;
+  const int         tiles = min(R, F.nb);
+  // Right-hand side of this row: its entry of x (rows < w), then the
+  // children's update vectors in child order.
+  double zr = 0.0;
+  if (qq == 0 && r < h) {
+    zr = r < w ? x[F.col0 + r] : 0.0;
+    for (int64_t e = gp[F.gptr + r]; e < gp[F.gptr + r + 1]; e++) zr += zbuf[gsrc[e]];
+  }
+  double            acc   = 0.0;
+  for (int b = 0; b < tiles; b++) {
+    const int c0 = b * kNB + qq * 32;
+    float     lv[32];
+#pragma unroll
+    for (int k = 0; k < 32; k++)
+      lv[k] = (r < h && c0 + k < w) ? __ldg(P + r + static_cast<int64_t>(c0 + k) * h) : 0.0f;
+    if (lane == 0) wait_flag(fl + b, err);
+    __syncwarp();
+    yw[warp][lane] = c0 + lane < w ? __ldcg(x + F.col0 + c0 + lane) : 0.0;
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < 32; k++) acc += static_cast<double>(lv[k]) * yw[warp][k];
+    __syncwarp();
   }
   part[qq][rr] = acc;
   __syncthreads();
-  if (qq == 0 && r < h) z[r] -= (part[0][rr] + part[1][rr]) + (part[2][rr] + part[3][rr]);
-  const int kn = d.kb + d.nbk;
-  if (local == 0 && kn < d.w) {
+  double z = 0.0;
+  if (qq == 0 && r < h) z = zr - ((part[0][rr] + part[1][rr]) + (part[2][rr] + part[3][rr]));
+  if (R < F.nb) {
+    const int nbk = min(kNB, w - R * kNB);
     __syncthreads();
-    const int nb = d.w - kn < kNB ? d.w - kn : kNB;
-    if (tid < nb) y[tid] = z[kn + tid];  // the next block's right-hand side
+    if (tid < kNB) ys[tid] = tid < nbk ? z : 0.0;
     __syncthreads();
-    const double yn = block_lower_apply(linv64 + d.linv + (int64_t)kNB * kNB, y, nb, part);
-    if (tid < nb) x[(int64_t)d.col0 + kn + tid] = yn;
+    const double y = block_lower_apply(tri, ys, nbk, part);
+    if (tid < nbk) x[F.col0 + R * kNB + tid] = y;
+    if ((R + 1) * kNB > w && h > w) {
+      // Rows of this block at or past w: their product with the block.
+      __syncthreads();
+      if (tid < kNB) ys[tid] = tid < nbk ? y : 0.0;
+      __syncthreads();
+      double a2 = 0.0;
+      if (r >= w && r < h)
+        for (int k = qq * 32; k < min(nbk, qq * 32 + 32); k++)
+          a2 += static_cast<double>(P[r + static_cast<int64_t>(R * kNB + k) * h]) * ys[k];
+      part[qq][rr] = a2;
+      __syncthreads();
+      if (qq == 0 && r >= w && r < h)
+        z -= (part[0][rr] + part[1][rr]) + (part[2][rr] + part[3][rr]);
+    }
+    // The CTA's writes of y happen before thread 0's release (bar.sync,
+    // then a cumulative fence and the release store).
+    __syncthreads();
+    if (tid == 0) {
+      __threadfence();
+      st_release(fl + R, 1);
+    }
   }
+  if (qq == 0 && r >= w && r < h) zbuf[F.zofs + r] = z;
 }
 
 __global__ void k_dscale(int64_t n, const float *Dinv, double *x) {
@@ -217,84 +305,122 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta)
   for (int i = lane; i < w; i += 32) x[f + i] = z[i];
 }
 
-__global__ void k_bwd_gather(const int32_t *list, const int64_t *sfirst,
-                             const int64_t *srowptr, const int32_t *srows,
-                             const int64_t *zofs, const double *x,
-                             double *zbuf) {
-  const int      J  = list[blockIdx.x];
-  const int64_t  f  = sfirst[J];
-  const int64_t  w  = sfirst[J + 1] - f;
-  const int64_t  h  = srowptr[J + 1] - srowptr[J];
-  const int32_t *rw = srows + srowptr[J];
-  double        *z  = zbuf + zofs[J];
-  for (int64_t i = threadIdx.x; i < h; i += blockDim.x)
-    z[i] = i < w ? x[f + i] : x[rw[i]];
-}
 
-// One column block, backward: partial sums t_k = sum_r L_{r,kb+k} z_r over a
-// chunk of 128 rows below the block (each warp takes 8 of the block's
-// columns); the last chunk to finish adds the partials in chunk order and
-// solves x_b = Linv^T (z_b - t) with the row-major copy of the inverse.
+// Backward solve, off-diagonal rows: CTA c takes rows w + 128c .. of one
+// front and writes t_k = sum_r L_{r,k} z_r for every column k of the front
+// (warp per column, rows over the lanes, shuffle reduction) to its partials.
 __global__ void __launch_bounds__(kSolveThreads)
-    k_bwd_step(const StepDesc *descs, int ndesc, const float *panel,
-               const double *linv64t, double *x, double *zbuf, double *part,
-               int32_t *counter) {
-  __shared__ double zr[kSolveChunk];
-  __shared__ double v[kNB];
-  __shared__ double red[4][kNB];
-  __shared__ int    last;
-  const int         t  = blockIdx.x;
-  int               lo = 0, hi = ndesc - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) / 2;
-    if (descs[mid].bsolve_chunk0 <= t) lo = mid; else hi = mid - 1;
-  }
-  const StepDesc d     = descs[lo];
-  const int      chunk = t - d.bsolve_chunk0;
-  const int      tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
-  const int64_t  h   = d.h;
-  double        *z   = zbuf + d.zofs;
-  const int64_t  r0  = (int64_t)d.kb + d.nbk + (int64_t)chunk * kSolveChunk;
-  const int64_t  r1  = min(r0 + kSolveChunk, h);
-  if (tid < kSolveChunk) zr[tid] = r0 + tid < r1 ? z[r0 + tid] : 0.0;
+    k_bwd_chunks(const SolveFront *fr, int nfr, const float *panel, const int32_t *srows,
+                 const double *x, double *part) {
+  __shared__ double zr[kNB];
+  const SolveFront  F = fr[find_front(fr, nfr, blockIdx.x, &SolveFront::chunk0)];
+  const int         c = blockIdx.x - F.chunk0;
+  const int         tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+  const int64_t     h = F.h, w = F.w;
+  const int64_t     r0 = w + static_cast<int64_t>(c) * kNB;
+  const int         nr = static_cast<int>(h - r0 < kNB ? h - r0 : kNB);
+  if (tid < kNB) zr[tid] = tid < nr ? x[srows[F.rows + r0 + tid]] : 0.0;
   __syncthreads();
-  const float *P  = panel + d.panel;
-  double      *pp = part + d.bpart + (int64_t)chunk * kNB;
+  const float  *P  = panel + F.panel + r0;
+  double       *pp = part + F.part + static_cast<int64_t>(c) * w;
   constexpr int kWarps = kSolveThreads / 32;
-  for (int k = warp; k < d.nbk; k += kWarps) {
-    const float *col = P + (int64_t)(d.kb + k) * h;
+#pragma unroll 2
+  for (int64_t k = warp; k < w; k += kWarps) {
+    const float *col = P + k * h;
     double       s   = 0.0;
-    for (int64_t r = r0 + lane; r < r1; r += 32)
-      s += static_cast<double>(col[r]) * zr[r - r0];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const int rr = lane + 32 * i;
+      if (rr < nr) s += static_cast<double>(__ldg(col + rr)) * zr[rr];
+    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if (lane == 0) pp[k] = s;
   }
-  __threadfence();
-  __syncthreads();
-  if (tid == 0) last = atomicAdd(counter + d.id, 1) == d.bsolve_chunks - 1;
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
+}
+
+// Backward solve, column blocks of the large fronts of one level: one CTA
+// per column block b (last first).  t = (sum of the chunk partials, in chunk
+// order) + (sum over the row blocks R > b of the diagonal part, last first,
+// each as soon as x_R is ready); then x_b = Linv_b^T (z_b - t) into x and the
+// front vector, and flag b is released.  In a tile, warp v takes the
+// block's columns 8v .. 8v+7 and the lanes the rows.
+__global__ void __launch_bounds__(kSolveThreads, 1)
+    k_bwd_fronts(const SolveFront *fr, int nfr, const float *panel, const double *linv64t,
+                 double *x, const double *part, int32_t *tickets,
+                 int32_t *flags, int32_t *err) {
+  extern __shared__ double tri[];  // kTri doubles: the staged Linv_b^T
+  __shared__ double v[kNB];
+  __shared__ double ts[kNB];
+  __shared__ double red[4][kNB];
+  const int         item = take_ticket(tickets);
+  const SolveFront  F    = fr[find_front(fr, nfr, item, &SolveFront::own0)];
+  const int         b    = F.nb - 1 - (item - F.own0);
+  stage_upper(linv64t + F.linv + static_cast<int64_t>(b) * kNB * kNB, tri,
+              min(kNB, F.w - b * kNB));
+  const int         tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+  const int64_t     h = F.h;
+  const int         w = F.w;
+  const int         nbk = min(kNB, w - b * kNB);
+  const float      *P   = panel + F.panel;
+  int32_t          *fl  = flags + F.flag0;
   {
-    // Partials of column k: thread (q, k) adds chunks q, q + 4, ...; the
-    // four sums are then added in order.
+    // Chunk partials of column k (no wait needed): thread (q, k) adds chunks
+    // q, q + 4, ...; the four sums are added in order below.
     const int k = tid % kNB, q = tid / kNB;
     double    s = 0.0;
-    if (k < d.nbk)
-      for (int c = q; c < d.bsolve_chunks; c += 4)
-        s += __ldcg(part + d.bpart + (int64_t)c * kNB + k);
+    if (k < nbk)
+      for (int c = q; c < F.chunks; c += 4)
+        s += part[F.part + static_cast<int64_t>(c) * w + b * kNB + k];
     red[q][k] = s;
   }
+  double acc[8];
+#pragma unroll
+  for (int j = 0; j < 8; j++) acc[j] = 0.0;
+  for (int R = F.nb - 1; R > b; R--) {
+    const int64_t rb   = static_cast<int64_t>(R) * kNB;
+    const int     rows = min(kNB, w - R * kNB);
+    float lv[8][4];
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      const int c = warp * 8 + j;
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const int rr = lane + 32 * i;
+        lv[j][i]     = (c < nbk && rr < rows)
+                           ? __ldg(P + rb + rr + static_cast<int64_t>(b * kNB + c) * h)
+                           : 0.0f;
+      }
+    }
+    if (lane == 0) wait_flag(fl + R, err);
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const int    rr = lane + 32 * i;
+      const double zv = rr < rows ? __ldcg(x + F.col0 + rb + rr) : 0.0;
+#pragma unroll
+      for (int j = 0; j < 8; j++) acc[j] += static_cast<double>(lv[j][i]) * zv;
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    double s = acc[j];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) ts[warp * 8 + j] = s;
+  }
   __syncthreads();
-  if (tid < d.nbk)
-    v[tid] = z[d.kb + tid] - ((red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]));
+  if (tid < nbk)
+    v[tid] = x[F.col0 + b * kNB + tid] -
+             (((red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid])) + ts[tid]);
   __syncthreads();
   // Lt[i * kNB + j] = Linv[i][j]
-  const double xb = block_upper_apply(linv64t + d.linv, v, d.nbk, red);
-  if (tid < d.nbk) {
-    z[d.kb + tid]                    = xb;
-    x[(int64_t)d.col0 + d.kb + tid] = xb;
+  const double xb = block_upper_apply(tri, v, nbk, red);
+  if (tid < nbk) x[F.col0 + b * kNB + tid] = xb;
+  __syncthreads();
+  if (tid == 0) {
+    __threadfence();
+    st_release(fl + b, 1);
   }
 }
 
@@ -302,8 +428,10 @@ __global__ void __launch_bounds__(kSolveThreads)
 void SolveWorkspace::allocate(const Plan &P) {
   release_graph();
   zbuf.resize(std::max<int64_t>(P.S.z_elems, 1) * sizeof(double));
-  part.resize(std::max<int64_t>(P.bpart_elems, 1) * sizeof(double));
-  counters.resize(std::max<int64_t>(P.ndesc, 1) * sizeof(int32_t));
+  part.resize(std::max<int64_t>(P.spart_elems, 1) * sizeof(double));
+  sync.resize(std::max<int64_t>(P.sync_elems, 1) * sizeof(int32_t));
+  err.resize(sizeof(int32_t));
+  MPIR_CUDA(cudaMemset(err.as<void>(), 0, sizeof(int32_t)));
   xbuf.resize(std::max<int64_t>(P.S.n, 1) * sizeof(double));
 }
 
@@ -347,55 +475,57 @@ void ldlt_solve(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
   const double *lv  = F.linv64.as<double>();
   double      *zbuf = ws.zbuf.as<double>();
   const int    nl   = static_cast<int>(P.levels.size());
+  // Tickets (2 per level), then the forward and backward ready flags.
+  int32_t          *sync = ws.sync.as<int32_t>();
+  int32_t          *ffl  = sync + 2 * nl;
+  int32_t          *bfl  = ffl + P.nflags;
+  int32_t          *err  = ws.err.as<int32_t>();
+  const SolveFront *sf   = P.solve_fronts.as<SolveFront>();
+  if (P.nflags > 0)
+    MPIR_CUDA(cudaMemsetAsync(sync, 0, P.sync_elems * sizeof(int32_t), s));
+  static bool attr = false;
+  if (!attr) {
+    MPIR_CUDA(cudaFuncSetAttribute(k_fwd_fronts, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(kTri * sizeof(double))));
+    MPIR_CUDA(cudaFuncSetAttribute(k_bwd_fronts, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(kTri * sizeof(double))));
+    attr = true;
+  }
   kt.begin(kKcSolveFwd, s);
   for (int t = 0; t < nl && (phases & kForward); t++) {
     const LevelPlan &L = P.levels[t];
-    if (L.small_count > 0)
-      launch(k_fwd_small, (L.small_count + kWarpsPerCta - 1) / kWarpsPerCta,
-                    32 * kWarpsPerCta, 0, s, 
-          P.small_list.as<int32_t>() + L.small_begin, L.small_count,
-          P.sfirst.as<int64_t>(), P.srowptr.as<int64_t>(), P.slofs.as<int64_t>(),
-          P.child_ptr.as<int64_t>(), P.child_list.as<int32_t>(),
-          P.srel.as<int32_t>(), P.zofs.as<int64_t>(), pan, x, zbuf);
-    if (L.large_count > 0) {
-      launch(k_fwd_gather, L.large_count, kSolveThreads, 0, s,
-             P.large_list.as<int32_t>() + L.large_begin, P.sfirst.as<int64_t>(),
-             P.srowptr.as<int64_t>(), P.child_ptr.as<int64_t>(),
-             P.child_list.as<int32_t>(), P.srel.as<int32_t>(), P.zofs.as<int64_t>(),
-             P.linv_ofs_d.as<int64_t>(), lv, x, zbuf);
-      for (const auto &st : L.steps)
-        launch(k_fwd_step, st.fsolve_tiles, kSolveThreads, 0, s, 
-            P.steps.as<StepDesc>() + st.begin, st.count, pan, lv, x, zbuf);
+    if (L.sw_count > 0)
+      launch(k_fwd_small, (L.sw_count + kWarpsPerCta - 1) / kWarpsPerCta, 32 * kWarpsPerCta, 0,
+             s, P.swarp_list.as<int32_t>() + L.sw_begin, L.sw_count, P.sfirst.as<int64_t>(),
+             P.srowptr.as<int64_t>(), P.slofs.as<int64_t>(), P.child_ptr.as<int64_t>(),
+             P.child_list.as<int32_t>(), P.srel.as<int32_t>(), P.zofs.as<int64_t>(), pan, x,
+             zbuf);
+    if (L.sf_count > 0) {
+      launch(k_fwd_fronts, L.fwd_items, kSolveThreads, kTri * sizeof(double), s, sf + L.sf_begin,
+             L.sf_count, pan, lv, P.gp.as<int64_t>(), P.gsrc.as<int64_t>(), x, zbuf, sync + 2 * t, ffl, err);
     }
   }
   if (phases & kDiagonal)
-    launch(k_dscale, static_cast<unsigned>((S.n + 255) / 256), 256, 0, s, 
-        S.n, F.Dinv.as<float>(), x);
+    launch(k_dscale, static_cast<unsigned>((S.n + 255) / 256), 256, 0, s,
+           S.n, F.Dinv.as<float>(), x);
   kt.end(s);
   if (!(phases & kBackward)) return;
   MPIR_CHECK_LAUNCH();
   kt.begin(kKcSolveBwd, s);
-  MPIR_CUDA(cudaMemsetAsync(ws.counters.as<void>(), 0,
-                            std::max<int64_t>(P.ndesc, 1) * sizeof(int32_t), s));
   for (int t = nl - 1; t >= 0; t--) {
     const LevelPlan &L = P.levels[t];
-    if (L.small_count > 0)
-      launch(k_bwd_small, (L.small_count + kWarpsPerCta - 1) / kWarpsPerCta,
-                    32 * kWarpsPerCta, 0, s, 
-          P.small_list.as<int32_t>() + L.small_begin, L.small_count,
-          P.sfirst.as<int64_t>(), P.srowptr.as<int64_t>(), P.srows.as<int32_t>(),
-          P.slofs.as<int64_t>(), pan, x);
-    if (L.large_count > 0) {
-      launch(k_bwd_gather, L.large_count, 256, 0, s, 
-          P.large_list.as<int32_t>() + L.large_begin, P.sfirst.as<int64_t>(),
-          P.srowptr.as<int64_t>(), P.srows.as<int32_t>(), P.zofs.as<int64_t>(), x,
-          zbuf);
-      for (size_t q = L.steps.size(); q-- > 0;) {
-        const auto &st = L.steps[q];
-        launch(k_bwd_step, st.bsolve_chunks, kSolveThreads, 0, s,
-               P.steps.as<StepDesc>() + st.begin, st.count, pan, F.linv64t.as<double>(), x,
-               zbuf, ws.part.as<double>(), ws.counters.as<int32_t>());
-      }
+    if (L.sw_count > 0)
+      launch(k_bwd_small, (L.sw_count + kWarpsPerCta - 1) / kWarpsPerCta, 32 * kWarpsPerCta, 0,
+             s, P.swarp_list.as<int32_t>() + L.sw_begin, L.sw_count, P.sfirst.as<int64_t>(),
+             P.srowptr.as<int64_t>(), P.srows.as<int32_t>(), P.slofs.as<int64_t>(), pan, x);
+    if (L.sf_count > 0) {
+      if (L.bwd_chunk_items > 0)
+        launch(k_bwd_chunks, L.bwd_chunk_items, kSolveThreads, 0, s, sf + L.sf_begin,
+               L.sf_count, pan, P.srows.as<int32_t>(), static_cast<const double *>(x),
+               ws.part.as<double>());
+      launch(k_bwd_fronts, L.bwd_owner_items, kSolveThreads, kTri * sizeof(double), s,
+             sf + L.sf_begin, L.sf_count, pan, F.linv64t.as<double>(), x,
+             static_cast<const double *>(ws.part.as<double>()), sync + 2 * t + 1, bfl, err);
     }
   }
   kt.end(s);
