@@ -162,6 +162,10 @@ void launch_gemm_tc(int mode, const GemmProb *probs, int nprob, int tiles, const
                     const float *packd, const float *packs, float *panel, float *uarena,
                     float *ws, FactorStatus *st, cudaStream_t s);
 int  tc_gemm_smem_bytes(int mode);
+// Tensor-core GEMM CTAs resident per SM (shared-memory bound).
+int  tc_ctas_per_sm();
+// Streaming multiprocessors of a B200.
+constexpr int kSMs = 148;
 
 // Kernel-class timer used by the benchmark's roofline figures.
 struct KernelTimer {

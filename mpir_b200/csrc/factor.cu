@@ -180,13 +180,30 @@ __global__ void k_extend_add(const EaTask *tasks, int ntasks,
   const int      rp  = tk.hp - tk.wp;
   for (int b = b0; b < b1; b++) {
     const int cb = rl[b];
-    for (int a = b + threadIdx.x; a < tk.rc; a += blockDim.x) {
-      const int   ra  = rl[a];
-      const float val = U[a + (int64_t)b * tk.rc];
-      if (cb < tk.wp)
-        Pp[ra + (int64_t)cb * tk.hp] += val;
-      else
-        uarena[tk.parent_u + (ra - tk.wp) + (int64_t)(cb - tk.wp) * rp] += val;
+    // Column cb of the parent: in its panel (rows from 0) or in its update
+    // matrix (rows from wp).
+    const int off = cb < tk.wp ? 0 : tk.wp;
+    float    *dst = cb < tk.wp ? Pp + (int64_t)cb * tk.hp
+                               : uarena + tk.parent_u + (int64_t)(cb - tk.wp) * rp;
+    const float *Ub = U + (int64_t)b * tk.rc;
+    // Four rows per thread at a time: all loads first (the source and the
+    // destination both may lie in the update arena, so the compiler would
+    // not reorder them itself).
+    for (int a0 = b + threadIdx.x; a0 < tk.rc; a0 += 4 * blockDim.x) {
+      int   ra[4];
+      float v[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const int a = a0 + u * blockDim.x;
+        ra[u]       = a < tk.rc ? rl[a] : -1;
+        v[u]        = a < tk.rc ? Ub[a] : 0.0f;
+      }
+      float o[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) o[u] = ra[u] >= 0 ? dst[ra[u] - off] : 0.0f;
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+        if (ra[u] >= 0) dst[ra[u] - off] = o[u] + v[u];
     }
   }
 }
@@ -519,9 +536,12 @@ __global__ void __launch_bounds__(kGemmThreads)
   }
 }
 
-// C -= sum of the split partials of one tile, added in split order.
-__global__ void k_split_reduce(const GemmProb *probs, int nprob, float *panel, float *uarena,
-                               const float *ws) {
+// C -= sum of the split partials of one tile, added in split order.  Thread
+// t takes 4 consecutive rows of a column (one float4 of each partial) and
+// four such groups at once, so 16 loads per split are in flight.
+__global__ void __launch_bounds__(256)
+    k_split_reduce(const GemmProb *probs, int nprob, float *panel, float *uarena,
+                   const float *ws) {
   const int t  = blockIdx.x;
   int       lo = 0, hi = nprob - 1;
   while (lo < hi) {
@@ -533,13 +553,36 @@ __global__ void k_split_reduce(const GemmProb *probs, int nprob, float *panel, f
   locate_tile(pb, (t - pb.rtile0) * pb.splits, sp, tile, m0, n0);
   float       *C = (pb.c_in_u ? uarena : panel) + pb.c_ofs;
   const float *W = ws + pb.ws_ofs + static_cast<int64_t>(tile) * pb.splits * (kBM * kBN);
-  for (int e = threadIdx.x; e < kBM * kBN; e += blockDim.x) {
-    const int m = m0 + e % kBM, c = n0 + e / kBM;
-    const int r = m < pb.M ? gemm_out_row(pb, m) : -1;
-    if (r < 0 || c >= pb.N || (pb.lower && r < c)) continue;
-    float acc = 0.0f;
-    for (int q = 0; q < pb.splits; q++) acc += W[static_cast<int64_t>(q) * (kBM * kBN) + e];
-    C[r + (int64_t)c * pb.ldc] -= acc;
+  constexpr int kGroups = kBM * kBN / 4;  // float4 groups of a tile
+#pragma unroll 1
+  for (int g0 = threadIdx.x; g0 < kGroups; g0 += 4 * 256) {
+    float4 acc[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) acc[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int q = 0; q < pb.splits; q++) {
+      const float4 *Wq = reinterpret_cast<const float4 *>(W + static_cast<int64_t>(q) * (kBM * kBN));
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const float4 v = __ldcs(Wq + g0 + u * 256);
+        acc[u].x += v.x;
+        acc[u].y += v.y;
+        acc[u].z += v.z;
+        acc[u].w += v.w;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int   e  = 4 * (g0 + u * 256);
+      const int   c  = n0 + e / kBM;
+      const float a[4] = {acc[u].x, acc[u].y, acc[u].z, acc[u].w};
+#pragma unroll
+      for (int v = 0; v < 4; v++) {
+        const int m = m0 + e % kBM + v;
+        const int r = m < pb.M ? gemm_out_row(pb, m) : -1;
+        if (r < 0 || c >= pb.N || (pb.lower && r < c)) continue;
+        C[r + (int64_t)c * pb.ldc] -= a[v];
+      }
+    }
   }
 }
 
@@ -646,14 +689,28 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
       const double Mr = g.M, Nc = g.N;
       update_flops += 2.0 * g.K * (g.lower ? Nc * Mr - Nc * (Nc - 1) / 2 : Nc * Mr);
     }
-    constexpr int64_t kTarget = 296;
+    // Splits of K: the count s (at least 256 of K per split) that minimises
+    // waves(total tiles x s over the resident CTAs) x (K / s + a fixed cost
+    // per CTA of about 128 columns of K); partial tiles are reduced after.
+    const int64_t resident = static_cast<int64_t>(kSMs) * tc_ctas_per_sm();
+    int64_t       kmax     = 0;
+    for (int32_t q = begin; q < begin + count; q++) kmax = std::max<int64_t>(kmax, probs[q].K);
+    int64_t best_s = 1;
+    double  best_c = 1e300;
+    for (int64_t sp = 1; sp <= std::max<int64_t>(1, kmax / 256); sp++) {
+      const double waves = static_cast<double>((total * sp + resident - 1) / resident);
+      const double c     = waves * (static_cast<double>((kmax + sp - 1) / sp) + 128.0);
+      if (c < best_c - 1e-9) {
+        best_c = c;
+        best_s = sp;
+      }
+    }
     int64_t t0 = 0, r0 = 0, w0 = 0;
     for (int32_t q = begin; q < begin + count; q++) {
       GemmProb &g = probs[q];
       g.splits    = 1;
-      if (total < kTarget) {
-        const int64_t want = std::max<int64_t>(
-            1, std::min<int64_t>((kTarget + total - 1) / total, g.K / 256));
+      const int64_t want = std::max<int64_t>(1, std::min<int64_t>(best_s, g.K / 256));
+      if (want > 1) {
         // Split length as the kernels compute it (a multiple of 32); then as
         // many splits as that length needs, so no split is empty.
         const int64_t ks = ((g.K + want - 1) / want + 31) / 32 * 32;
@@ -958,16 +1015,15 @@ void Numeric::run(const Plan &P, const double *d_Ax, double eps, cudaStream_t s)
       Korig.as<double>());
   kt.end(s);
   MPIR_CHECK_LAUNCH();
-  static bool attr = false;
-  const int   diag_smem = (2 * kNB * (kNB + 1) + kNB) * sizeof(float);
-  if (!attr) {
-    MPIR_CUDA(cudaFuncSetAttribute(k_diag_block,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   diag_smem));
-    attr = true;
-  }
   float        *pan = panel.as<float>(), *ua = uarena.as<float>();
   FactorStatus *st  = status.as<FactorStatus>();
+  static bool   diag_attr = false;
+  const int     diag_smem = (2 * kNB * (kNB + 1) + kNB) * sizeof(float);
+  if (!diag_attr) {
+    MPIR_CUDA(cudaFuncSetAttribute(k_diag_block, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   diag_smem));
+    diag_attr = true;
+  }
   for (const LevelPlan &L : P.levels) {
     if (L.zero_count > 0) {
       kt.begin(kKcZero, s);

@@ -44,7 +44,10 @@ namespace tc {
 constexpr int      kTileM     = 128;
 constexpr int      kTileN     = 128;
 constexpr int      kThreads   = 256;
-constexpr int      kStages    = 6;
+#ifndef MPIR_TC_STAGES
+#define MPIR_TC_STAGES 3
+#endif
+constexpr int      kStages    = MPIR_TC_STAGES;
 constexpr uint32_t kTmemCols  = 128;
 constexpr uint32_t kGroup     = 2048;  // bytes of one K-group (128 rows x 16 B)
 constexpr uint32_t kLBO       = 2048;  // bytes between K-adjacent core matrices
@@ -237,7 +240,7 @@ __device__ __forceinline__ void convert_row(uint8_t *stage, int m) {
 
 // MODE 0: bfloat16 single pass; MODE 1: 3xTF32; MODE 2: float16 single pass.
 template <int MODE>
-__global__ void __launch_bounds__(tc::kThreads, 1)
+__global__ void __launch_bounds__(tc::kThreads, tc::kStages <= 3 ? 2 : 1)
     k_gemm_tc(const GemmProb *probs, int nprob, const float *pack, const float *packd,
               const float *packs, float *panel, float *uarena, float *ws, FactorStatus *st) {
   using namespace tc;
@@ -442,6 +445,8 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                  "r"(kTmemCols) : "memory");
 }
+
+int tc_ctas_per_sm() { return tc::kStages <= 3 ? 2 : 1; }
 
 int tc_gemm_smem_bytes(int mode) {
   const uint32_t stage = mode == 1 ? tc::Cfg<1>::kStage : tc::Cfg<0>::kStage;
