@@ -209,74 +209,159 @@ __global__ void k_extend_add(const EaTask *tasks, int ntasks,
 }
 
 // ---------------------------------------------------------------------------
-// Diagonal block of one step: LDL^T of the nbk x nbk block in shared memory,
-// together with the inverse of its unit-lower factor (right-looking forward
-// substitution on the identity, done in the same sweep).
+// Diagonal block of one step: LDL^T of the nbk x nbk block (nbk <= 128) and
+// the inverse X = L^{-1} of its unit-lower factor, blocked by 32 columns, in
+// shared memory (row-major copies of the block and of X):
+//   panel p (columns 32p .. 32p+31): thread (i, c) = (tid % 128, tid / 128)
+//     holds row i of the panel's columns 32p + c + 4t (t < 8) in registers;
+//     pivot k: the holders of column k publish it (double-buffered, one
+//     barrier per pivot) and each thread applies
+//     F[i][j] -= (F[i][k] / d_k) F[j][k] to its columns k < j <= i;
+//   after the panel: its multipliers L = F / d and its unscaled columns G go
+//     to shared memory, and the columns right of the panel take the rank-32
+//     update F[i][j] -= sum_k L[i][k] G[j][k] (no barrier inside);
+//   X: the four 32 x 32 diagonal blocks by forward substitution (one warp
+//     each, lane = column), then the blocks below them in three rounds,
+//     X_ab = -X_aa sum_{b <= c < a} L_ac X_cb.
+constexpr int kDiagLD = kNB + 1, kDiagLG = 33;
+constexpr int kDiagSmemFloats = 2 * kNB * kDiagLD + kNB * kDiagLG + 3 * 32 * kDiagLG;
+
 __global__ void __launch_bounds__(kDiagThreads)
     k_diag_block(const StepDesc *descs, float *panel, float *linv, float *D, float *Dinv,
                  float *packd, float *packs, FactorStatus *st) {
+  static_assert(kDiagThreads == 4 * kNB, "diag kernel thread mapping");
+  constexpr int LD = kDiagLD, LG = kDiagLG;
   extern __shared__ float sm[];
-  constexpr int           LD = kNB + 1;
-  float                  *F  = sm;
-  float                  *X  = sm + kNB * LD;
-  float                  *wv = X + kNB * LD;
-  __shared__ int          s_npos;
-  const StepDesc          d   = descs[blockIdx.x];
-  const int               n   = d.nbk;
-  const int64_t           h   = d.h;
-  const int               tid = threadIdx.x, bd = blockDim.x;
-  float                  *P   = panel + d.panel + d.kb + (int64_t)d.kb * h;
-  if (tid == 0) s_npos = 0;
-  for (int idx = tid; idx < n * n; idx += bd) {
-    const int i = idx % n, j = idx / n;
-    F[i * LD + j] = i >= j ? P[i + (int64_t)j * h] : 0.0f;
-    X[i * LD + j] = i == j ? 1.0f : 0.0f;
+  float          *Fs = sm;                // the block, row-major
+  float          *Xs = Fs + kNB * LD;     // X, row-major
+  float          *Gs = Xs + kNB * LD;     // unscaled columns of the current panel
+  float          *Ts = Gs + kNB * LG;     // 3 scratch 32 x 32 blocks
+  __shared__ float col[2][kNB];
+  __shared__ float dinv_s[kNB];
+  const StepDesc   d   = descs[blockIdx.x];
+  const int        n   = d.nbk;
+  const int64_t    h   = d.h;
+  const int        tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+  const int        ri  = tid % kNB, c = tid / kNB;
+  float           *P   = panel + d.panel + d.kb + (int64_t)d.kb * h;
+  for (int idx = tid; idx < kNB * kNB; idx += kDiagThreads) {
+    const int i = idx % kNB, j = idx / kNB;
+    Fs[i * LD + j] = (i >= j && i < n && j < n) ? P[i + (int64_t)j * h] : 0.0f;
+    Xs[i * LD + j] = 0.0f;
   }
   __syncthreads();
-  // Thread t owns row i = t % kNB and the columns j = t / kNB (mod 4): no
-  // index arithmetic per element and an even split of each rank-1 update.
-  static_assert(kDiagThreads == 4 * kNB, "diag kernel thread mapping");
-  const int ri = tid % kNB, cj = tid / kNB;
-  int       npos = 0;
-  for (int k = 0; k < n; k++) {
-    const float dk = F[k * LD + k];
-    if (tid > k && tid < n) wv[tid] = F[tid * LD + k];
-    __syncthreads();
-    const float dinv = 1.0f / dk;
-    if (ri > k && ri < n) {
-      const float li = wv[ri] * dinv;
-      // trailing update, columns k < j <= i
-      int j0 = k + 1 + ((cj - (k + 1)) % 4 + 4) % 4;
-      for (int j = j0; j <= ri; j += 4) F[ri * LD + j] -= li * wv[j];
-      // inverse of the unit-lower factor (float32, for the panel solve;
-      // the float64 inverses the triangular solves use are formed after
-      // the whole factorization by k_invert_blocks): columns j <= k
-      for (int j = cj; j <= k; j += 4) X[ri * LD + j] -= li * X[k * LD + j];
+  int npos = 0;
+  for (int c0 = 0; c0 < n; c0 += 32) {
+    float r[8];
+#pragma unroll
+    for (int t = 0; t < 8; t++) r[t] = Fs[ri * LD + c0 + c + 4 * t];
+#pragma unroll
+    for (int kk = 0; kk < 32; kk++) {
+      const int k = c0 + kk;
+      if (k >= n) break;
+      const int b = kk & 1;
+      if (c == (kk & 3)) col[b][ri] = r[kk >> 2];
+      __syncthreads();
+      const float dk = col[b][k];
+      const float dv = 1.0f / dk;
+      if (ri > k && ri < n) {
+        const float s = col[b][ri] * dv;  // L[i][k]
+#pragma unroll
+        for (int t = 0; t < 8; t++) {
+          const int jj = c + 4 * t;
+          if (jj > kk && c0 + jj <= ri) r[t] -= s * col[b][c0 + jj];
+        }
+      }
+      if (tid == 0) {
+        const int64_t cidx = (int64_t)d.col0 + d.kb + k;
+        dinv_s[k]          = dv;
+        D[cidx]            = dk;
+        Dinv[cidx]         = dv;
+        if (packd != nullptr && d.pd >= 0) {
+          packd[d.pd + d.kb + k] = dk;
+          packs[d.pd + d.kb + k] = copysignf(sqrtf(fabsf(dk)), dk);
+        }
+        note_pivot(st, static_cast<int32_t>(cidx), dk, &npos);
+      }
     }
     __syncthreads();
-    if (ri > k && ri < n && cj == 0) F[ri * LD + k] = wv[ri] * dinv;
-    if (tid == 0) {
-      const int64_t col = (int64_t)d.col0 + d.kb + k;
-      D[col]            = dk;
-      Dinv[col]         = dinv;
-      if (packd != nullptr && d.pd >= 0) {
-        packd[d.pd + d.kb + k] = dk;
-        packs[d.pd + d.kb + k] = copysignf(sqrtf(fabsf(dk)), dk);
+    // The panel back: multipliers below the diagonal, pivots on it; the
+    // unscaled values for the trailing update.
+#pragma unroll
+    for (int t = 0; t < 8; t++) {
+      const int jj = c + 4 * t, j = c0 + jj;
+      if (j < n) {
+        Gs[ri * LG + jj] = r[t];
+        Fs[ri * LD + j]  = ri > j ? r[t] * dinv_s[j] : r[t];
       }
-      note_pivot(st, static_cast<int32_t>(col), dk, &npos);
+    }
+    __syncthreads();
+    if (c0 + 32 < n) {
+      if (ri >= c0 + 32 && ri < n) {
+        float lrow[32];
+#pragma unroll
+        for (int kk = 0; kk < 32; kk++) lrow[kk] = Fs[ri * LD + c0 + kk];
+        for (int j = c0 + 32 + c; j <= ri; j += 4) {
+          float acc = 0.0f;
+#pragma unroll
+          for (int kk = 0; kk < 32; kk++) acc += lrow[kk] * Gs[j * LG + kk];
+          Fs[ri * LD + j] -= acc;
+        }
+      }
+      __syncthreads();
+    }
+  }
+  if (tid == 0) atomicAdd(&st->npos, npos);
+  // X: diagonal 32 x 32 blocks, one warp each (lane = column).
+  if (warp < 4 && 32 * warp < n) {
+    const int p0 = 32 * warp, j = p0 + lane;
+    float     xc[32];
+#pragma unroll
+    for (int ii = 0; ii < 32; ii++) {
+      const int i   = p0 + ii;
+      float     acc = 0.0f;
+#pragma unroll
+      for (int kk = 0; kk < ii; kk++) acc += Fs[i * LD + p0 + kk] * xc[kk];
+      xc[ii] = ii == lane ? 1.0f : (ii > lane ? -acc : 0.0f);
+    }
+#pragma unroll
+    for (int ii = 0; ii < 32; ii++) Xs[(p0 + ii) * LD + j] = xc[ii];
+  }
+  __syncthreads();
+  // X below the diagonal blocks, by block distance dd.
+  const int nblk = (n + 31) / 32;
+  for (int dd = 1; dd < nblk; dd++) {
+    const int npair = nblk - dd;  // pairs (a, b) = (b + dd, b)
+    // T_e = sum_{b <= cb < a} L_{a,cb} X_{cb,b}
+    for (int e = tid; e < npair * 1024; e += kDiagThreads) {
+      const int pr = e / 1024, rr = (e % 1024) / 32, cc = e % 32;
+      const int bb = pr, aa = pr + dd;
+      float     acc = 0.0f;
+      for (int k = 32 * bb; k < 32 * aa; k++)
+        acc += Fs[(32 * aa + rr) * LD + k] * Xs[k * LD + 32 * bb + cc];
+      Ts[pr * 32 * LG + rr * LG + cc] = acc;
+    }
+    __syncthreads();
+    // X_ab = -X_aa T
+    for (int e = tid; e < npair * 1024; e += kDiagThreads) {
+      const int pr = e / 1024, rr = (e % 1024) / 32, cc = e % 32;
+      const int bb = pr, aa = pr + dd;
+      float     acc = 0.0f;
+#pragma unroll 8
+      for (int kk = 0; kk < 32; kk++)
+        acc += Xs[(32 * aa + rr) * LD + 32 * aa + kk] * Ts[pr * 32 * LG + kk * LG + cc];
+      Xs[(32 * aa + rr) * LD + 32 * bb + cc] = -acc;
     }
     __syncthreads();
   }
-  if (tid == 0) atomicAdd(&st->npos, npos);
-  float *Lv = linv + d.linv;
-  for (int idx = tid; idx < kNB * kNB; idx += bd) {
+  for (int idx = tid; idx < kNB * kNB; idx += kDiagThreads) {
     const int i = idx % kNB, j = idx / kNB;
-    if (i < n && j < n) {
-      if (i >= j) P[i + (int64_t)j * h] = F[i * LD + j];
-      Lv[i + j * kNB] = X[i * LD + j];
-    } else {
-      Lv[i + j * kNB] = 0.0f;
-    }
+    if (i >= j && i < n && j < n) P[i + (int64_t)j * h] = Fs[i * LD + j];
+  }
+  float *Lv = linv + d.linv;
+  for (int idx = tid; idx < kNB * kNB; idx += kDiagThreads) {
+    const int i = idx % kNB, j = idx / kNB;
+    Lv[i + j * kNB] = (i < n && j < n) ? Xs[i * LD + j] : 0.0f;
   }
 }
 
@@ -1018,7 +1103,7 @@ void Numeric::run(const Plan &P, const double *d_Ax, double eps, cudaStream_t s)
   float        *pan = panel.as<float>(), *ua = uarena.as<float>();
   FactorStatus *st  = status.as<FactorStatus>();
   static bool   diag_attr = false;
-  const int     diag_smem = (2 * kNB * (kNB + 1) + kNB) * sizeof(float);
+  const int     diag_smem = kDiagSmemFloats * sizeof(float);
   if (!diag_attr) {
     MPIR_CUDA(cudaFuncSetAttribute(k_diag_block, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    diag_smem));
