@@ -655,18 +655,28 @@ __global__ void __launch_bounds__(256)
         acc[u].w += v.w;
       }
     }
+    // All loads of C first, then the stores (one memory latency, not 16).
+    int64_t at[16];
+    float   cv[16];
 #pragma unroll
     for (int u = 0; u < 4; u++) {
-      const int   e  = 4 * (g0 + u * 256);
-      const int   c  = n0 + e / kBM;
-      const float a[4] = {acc[u].x, acc[u].y, acc[u].z, acc[u].w};
+      const int e = 4 * (g0 + u * 256);
+      const int c = n0 + e / kBM;
 #pragma unroll
       for (int v = 0; v < 4; v++) {
         const int m = m0 + e % kBM + v;
         const int r = m < pb.M ? gemm_out_row(pb, m) : -1;
-        if (r < 0 || c >= pb.N || (pb.lower && r < c)) continue;
-        C[r + (int64_t)c * pb.ldc] -= a[v];
+        at[4 * u + v] = (r < 0 || c >= pb.N || (pb.lower && r < c)) ? -1
+                                                                       : r + (int64_t)c * pb.ldc;
+        cv[4 * u + v] = at[4 * u + v] >= 0 ? C[at[4 * u + v]] : 0.0f;
       }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const float a[4] = {acc[u].x, acc[u].y, acc[u].z, acc[u].w};
+#pragma unroll
+      for (int v = 0; v < 4; v++)
+        if (at[4 * u + v] >= 0) C[at[4 * u + v]] = cv[4 * u + v] - a[v];
     }
   }
 }

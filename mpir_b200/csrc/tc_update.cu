@@ -238,60 +238,81 @@ __device__ __forceinline__ void convert_row(uint8_t *stage, int m) {
 
 }  // namespace tc
 
+// One unit of work: a 128 x 128 tile of one problem over one split of K.
+struct Unit {
+  const GemmProb *pb;
+  int             tile, sp, mt, j, k_lo, nch;
+};
+
+// Units of a launch in order: problem by binary search on the problems'
+// first units (kept in shared memory when they fit), then the tile of the
+// (lower) tile pattern and the split.
+template <int KC>
+__device__ __forceinline__ Unit locate_unit(const GemmProb *probs, int nprob, const int *t0s,
+                                            int u) {
+  int lo = 0, hi = nprob - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    const int t0  = t0s ? t0s[mid] : probs[mid].tile0;
+    if (t0 <= u) lo = mid; else hi = mid - 1;
+  }
+  Unit U;
+  U.pb            = probs + lo;
+  const int local = u - U.pb->tile0;
+  const int splits = U.pb->splits, ntm = U.pb->ntm, K = U.pb->K;
+  U.sp   = local % splits;
+  int tl = local / splits;
+  U.tile = tl;
+  int j  = 0;
+  if (U.pb->lower) {
+    while (tl >= ntm - j) {
+      tl -= ntm - j;
+      j++;
+    }
+  } else {
+    j  = tl / ntm;
+    tl = tl % ntm;
+  }
+  U.mt          = U.pb->lower ? j + tl : tl;
+  U.j           = j;
+  const int ks  = ((K + splits - 1) / splits + 31) / 32 * 32;
+  U.k_lo        = U.sp * ks;
+  const int khi = min(K, U.k_lo + ks);
+  U.nch         = khi > U.k_lo ? (khi - U.k_lo + KC - 1) / KC : 0;
+  return U;
+}
+
+constexpr int kMaxProbSmem = 2048;  // problems whose first units go to shared memory
+
 // MODE 0: bfloat16 single pass; MODE 1: 3xTF32; MODE 2: float16 single pass.
+// Persistent: CTA b takes units b, b + gridDim.x, ...; the ring stages run on
+// across units (the producer loads the next unit's first stages while the
+// epilogue drains the accumulator of the current one); the accumulator is
+// handed between the MMA issuer and the epilogue by the acc_full / acc_free
+// mbarriers.
 template <int MODE>
 __global__ void __launch_bounds__(tc::kThreads, tc::kStages <= 3 ? 2 : 1)
-    k_gemm_tc(const GemmProb *probs, int nprob, const float *pack, const float *packd,
-              const float *packs, float *panel, float *uarena, float *ws, FactorStatus *st) {
+    k_gemm_tc(const GemmProb *probs, int nprob, int units, const float *pack,
+              const float *packd, const float *packs, float *panel, float *uarena, float *ws,
+              FactorStatus *st) {
   using namespace tc;
   using C = Cfg<MODE>;
   extern __shared__ __align__(1024) uint8_t smem[];
-  // full[kStages], conv[kStages], empty[kStages], done
-  __shared__ __align__(8) uint64_t bars[3 * kStages + 1];
+  // full[kStages], conv[kStages], empty[kStages], acc_full, acc_free, drain
+  __shared__ __align__(8) uint64_t bars[3 * kStages + 3];
   __shared__ uint32_t tmem_slot;
   __shared__ volatile int s_fail;
 
   const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
-  // ---- locate problem, tile and K split
-  const int t  = blockIdx.x;
-  int       lo = 0, hi = nprob - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) / 2;
-    if (probs[mid].tile0 <= t) lo = mid; else hi = mid - 1;
-  }
-  const GemmProb pb    = probs[lo];
-  const int      local = t - pb.tile0;
-  const int      sp    = local % pb.splits;
-  int            tl    = local / pb.splits;
-  const int      tile  = tl;
-  int            j     = 0;
-  if (pb.lower) {
-    while (tl >= pb.ntm - j) {
-      tl -= pb.ntm - j;
-      j++;
-    }
-  } else {
-    j  = tl / pb.ntm;
-    tl = tl % pb.ntm;
-  }
-  const int mt = pb.lower ? j + tl : tl;  // row tile of A
-  const int m0 = mt * kTileM;
-  const int n0 = j * kTileN;
-  const int M = pb.M, N = pb.N, K = pb.K;
-  const int ks   = ((K + pb.splits - 1) / pb.splits + 31) / 32 * 32;
-  const int k_lo = sp * ks, k_hi = min(K, k_lo + ks);
-  const int nch  = k_hi > k_lo ? (k_hi - k_lo + C::kKC - 1) / C::kKC : 0;
-  // Stage c reads packed K-groups k_lo/4 + c kKG ..: one contiguous block of
-  // A's row tile, one of B's, and kKC pivots.
-  const float *Ag = pack + pb.pa + static_cast<int64_t>(mt) * pb.prow +
-                    static_cast<int64_t>(k_lo / 4) * PackedFront::kGroupFloats;
-  const float *Bg = pack + pb.pb + static_cast<int64_t>(j) * pb.prow +
-                    static_cast<int64_t>(k_lo / 4) * PackedFront::kGroupFloats;
-  const float *Dg = (C::kHalf ? packs : packd) + pb.pd + k_lo;
-
+  int      *t0s = nprob <= kMaxProbSmem
+                      ? reinterpret_cast<int *>(smem + kStages * C::kStage)
+                      : nullptr;
   const uint32_t full0 = smem_u32(&bars[0]), conv0 = smem_u32(&bars[kStages]),
-                 empty0 = smem_u32(&bars[2 * kStages]), done = smem_u32(&bars[3 * kStages]);
-  // ---- tensor memory and barriers
+                 empty0 = smem_u32(&bars[2 * kStages]),
+                 acc_full = smem_u32(&bars[3 * kStages]),
+                 acc_free = smem_u32(&bars[3 * kStages + 1]),
+                 drain = smem_u32(&bars[3 * kStages + 2]);
+  // ---- tensor memory, barriers, problem table
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
                  ::"r"(smem_u32(&tmem_slot)), "r"(kTmemCols) : "memory");
@@ -304,9 +325,13 @@ __global__ void __launch_bounds__(tc::kThreads, tc::kStages <= 3 ? 2 : 1)
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;" ::"r"(conv0 + 8 * s) : "memory");
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(empty0 + 8 * s) : "memory");
     }
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(done) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(acc_full) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;" ::"r"(acc_free) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(drain) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
+  if (t0s)
+    for (int q = tid; q < nprob; q += kThreads) t0s[q] = probs[q].tile0;
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -315,93 +340,134 @@ __global__ void __launch_bounds__(tc::kThreads, tc::kStages <= 3 ? 2 : 1)
   if (warp == 0) {
     // ---------------- producer
     if (lane == 0) {
-      int issued = 0;
-      for (int c = 0; c < nch; c++) {
-        const int s = c % kStages, round = c / kStages;
-        if (round > 0 && !wait_bounded(empty0 + 8 * s, (round - 1) & 1)) {
-          s_fail = 1;
-          break;
+      long g = 0;
+      for (int u = blockIdx.x; u < units && !s_fail; u += gridDim.x) {
+        const Unit   U  = locate_unit<C::kKC>(probs, nprob, t0s, u);
+        const float *Ag = pack + U.pb->pa + static_cast<int64_t>(U.mt) * U.pb->prow +
+                          static_cast<int64_t>(U.k_lo / 4) * PackedFront::kGroupFloats;
+        const float *Bg = pack + U.pb->pb + static_cast<int64_t>(U.j) * U.pb->prow +
+                          static_cast<int64_t>(U.k_lo / 4) * PackedFront::kGroupFloats;
+        const float *Dg = (C::kHalf ? packs : packd) + U.pb->pd + U.k_lo;
+        for (int c = 0; c < U.nch; c++, g++) {
+          const int s = static_cast<int>(g % kStages);
+          const int round = static_cast<int>(g / kStages);
+          if (round > 0 && !wait_bounded(empty0 + 8 * s, (round - 1) & 1)) {
+            s_fail = 1;
+            break;
+          }
+          const uint32_t base = smem_u32(smem + s * C::kStage);
+          arrive_expect_tx(full0 + 8 * s, C::kTx);
+          bulk_load(base + C::kA,
+                    Ag + static_cast<int64_t>(c) * C::kKG * PackedFront::kGroupFloats, C::kRaw,
+                    full0 + 8 * s);
+          bulk_load(base + C::kB,
+                    Bg + static_cast<int64_t>(c) * C::kKG * PackedFront::kGroupFloats, C::kRaw,
+                    full0 + 8 * s);
+          bulk_load(base + C::kD, Dg + c * C::kKC, C::kKC * 4, full0 + 8 * s);
         }
-        const uint32_t base = smem_u32(smem + s * C::kStage);
-        arrive_expect_tx(full0 + 8 * s, C::kTx);
-        bulk_load(base + C::kA, Ag + static_cast<int64_t>(c) * C::kKG * PackedFront::kGroupFloats,
-                  C::kRaw, full0 + 8 * s);
-        bulk_load(base + C::kB, Bg + static_cast<int64_t>(c) * C::kKG * PackedFront::kGroupFloats,
-                  C::kRaw, full0 + 8 * s);
-        bulk_load(base + C::kD, Dg + c * C::kKC, C::kKC * 4, full0 + 8 * s);
-        issued = c + 1;
       }
       // No copy may still target shared memory at exit: the last stage issued
       // into each slot has landed (no later round was issued into it).
-      for (int c = max(0, issued - kStages); c < issued; c++)
-        wait_bounded(full0 + 8 * (c % kStages), (c / kStages) & 1);
+      for (long c = g > kStages ? g - kStages : 0; c < g; c++)
+        wait_bounded(full0 + 8 * static_cast<int>(c % kStages),
+                     static_cast<uint32_t>(c / kStages) & 1);
     }
     __syncwarp();
   } else if (warp == 1) {
     // ---------------- MMA issuer
     if (lane == 0) {
       const uint32_t idesc = make_idesc(MODE == 0 ? kFmtBF16 : MODE == 1 ? kFmtTF32 : kFmtF16);
-      for (int c = 0; c < nch; c++) {
-        const int s = c % kStages, round = c / kStages;
-        if (!wait_bounded(conv0 + 8 * s, round & 1)) {
+      long           g     = 0;
+      int            jn    = 0;
+      for (int u = blockIdx.x; u < units && !s_fail; u += gridDim.x, jn++) {
+        const Unit U = locate_unit<C::kKC>(probs, nprob, t0s, u);
+        // the epilogue has read the previous unit's accumulator
+        if (jn > 0 && !wait_bounded(acc_free, (jn - 1) & 1)) {
           s_fail = 1;
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t base = smem_u32(smem + s * C::kStage);
-        // Each MMA consumes two K-groups: 8 tf32 or 16 16-bit columns.
-        constexpr int kSteps = MODE == 1 ? C::kKG / 2 : C::kKG / 4;
-#pragma unroll
-        for (int q = 0; q < kSteps; q++) {
-          const uint32_t off = q * 2 * kGroup;
-          const uint32_t acc = (c > 0 || q > 0) ? 1u : 0u;
-          if (MODE == 1) {
-            const uint64_t ahd = make_desc(base + C::kA + off);
-            const uint64_t bhd = make_desc(base + C::kB + off);
-            const uint64_t ald = make_desc(base + C::kAlo + off);
-            const uint64_t bld = make_desc(base + C::kBlo + off);
-            mma<true>(tmem, ahd, bhd, idesc, acc);
-            mma<true>(tmem, ahd, bld, idesc, 1u);
-            mma<true>(tmem, ald, bhd, idesc, 1u);
-          } else {
-            mma<false>(tmem, make_desc(base + C::kA + off), make_desc(base + C::kB + off), idesc,
-                       acc);
+        bool ok = true;
+        for (int c = 0; c < U.nch; c++, g++) {
+          const int s = static_cast<int>(g % kStages);
+          const int round = static_cast<int>(g / kStages);
+          if (!wait_bounded(conv0 + 8 * s, round & 1)) {
+            ok = false;
+            break;
           }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t base = smem_u32(smem + s * C::kStage);
+          // Each MMA consumes two K-groups: 8 tf32 or 16 16-bit columns.
+          constexpr int kSteps = MODE == 1 ? C::kKG / 2 : C::kKG / 4;
+#pragma unroll
+          for (int q = 0; q < kSteps; q++) {
+            const uint32_t off = q * 2 * kGroup;
+            const uint32_t acc = (c > 0 || q > 0) ? 1u : 0u;
+            if (MODE == 1) {
+              const uint64_t ahd = make_desc(base + C::kA + off);
+              const uint64_t bhd = make_desc(base + C::kB + off);
+              const uint64_t ald = make_desc(base + C::kAlo + off);
+              const uint64_t bld = make_desc(base + C::kBlo + off);
+              mma<true>(tmem, ahd, bhd, idesc, acc);
+              mma<true>(tmem, ahd, bld, idesc, 1u);
+              mma<true>(tmem, ald, bhd, idesc, 1u);
+            } else {
+              mma<false>(tmem, make_desc(base + C::kA + off), make_desc(base + C::kB + off),
+                         idesc, acc);
+            }
+          }
+          commit(empty0 + 8 * s);
         }
-        commit(empty0 + 8 * s);
+        if (!ok) {
+          s_fail = 1;
+          break;
+        }
+        commit(acc_full);  // tracks every MMA issued so far
       }
-      // Tracks every MMA issued above (none: arrives at once).
-      commit(done);
+      // Every MMA of this CTA has completed before the memory is released.
+      commit(drain);
+      wait_bounded(drain, 0);
     }
     __syncwarp();
   } else if (warp >= 4) {
-    // ---------------- converters, then the epilogue
-    const int m = tid - 128;
-    for (int c = 0; c < nch; c++) {
-      const int s = c % kStages, round = c / kStages;
-      if (!wait_bounded(full0 + 8 * s, round & 1)) {
+    // ---------------- converters, then the epilogue of each unit
+    const int m  = tid - 128;
+    const int ew = warp - 4;  // tensor-memory lanes 32 ew .. 32 ew + 31
+    long      g  = 0;
+    int       jn = 0;
+    for (int u = blockIdx.x; u < units && !s_fail; u += gridDim.x, jn++) {
+      const Unit U  = locate_unit<C::kKC>(probs, nprob, t0s, u);
+      bool       ok = true;
+      for (int c = 0; c < U.nch; c++, g++) {
+        const int s = static_cast<int>(g % kStages);
+        const int round = static_cast<int>(g / kStages);
+        if (!wait_bounded(full0 + 8 * s, round & 1)) {
+          ok = false;
+          break;
+        }
+        convert_row<MODE>(smem + s * C::kStage, m);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        arrive(conv0 + 8 * s);
+      }
+      ok = ok && wait_bounded(acc_full, jn & 1);
+      ok = __all_sync(0xffffffffu, ok);
+      if (!ok) {
         s_fail = 1;
         break;
       }
-      convert_row<MODE>(smem + s * C::kStage, m);
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      arrive(conv0 + 8 * s);
-    }
-    bool ok = wait_bounded(done, 0);
-    if (!ok) s_fail = 1;
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    ok = ok && s_fail == 0;
-    ok = __all_sync(0xffffffffu, ok);
-    if (ok) {
-      const int ew   = warp - 4;  // tensor-memory lanes 32 ew .. 32 ew + 31
-      const int lr   = ew * 32 + lane;
-      const int mrow = m0 + lr;
-      const int row  = mrow < M ? gemm_out_row(pb, mrow) : -1;
-      float    *Cout = (pb.c_in_u ? uarena : panel) + pb.c_ofs;
-      float    *W    = pb.splits > 1
-                           ? ws + pb.ws_ofs +
-                              (static_cast<int64_t>(tile) * pb.splits + sp) * (kTileM * kTileN)
-                           : nullptr;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const GemmProb &pb   = *U.pb;
+      const int       lr   = ew * 32 + lane;
+      const int       mrow = U.mt * kTileM + lr;
+      const int       row  = mrow < pb.M ? gemm_out_row(pb, mrow) : -1;
+      const int       n0   = U.j * kTileN;
+      float          *Cout = (pb.c_in_u ? uarena : panel) + pb.c_ofs;
+      float          *W    = pb.splits > 1
+                                 ? ws + pb.ws_ofs +
+                                    (static_cast<int64_t>(U.tile) * pb.splits + U.sp) *
+                                        (kTileM * kTileN)
+                                 : nullptr;
+      const int       N = pb.N, ldc = pb.ldc, lower = pb.lower;
 #pragma unroll
       for (int cb = 0; cb < kTileN / 32; cb++) {
         uint32_t       r[32];
@@ -418,27 +484,39 @@ __global__ void __launch_bounds__(tc::kThreads, tc::kStages <= 3 ? 2 : 1)
               "=r"(r[30]), "=r"(r[31])
             : "r"(taddr));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (nch == 0)  // an empty K range leaves the accumulator unwritten
+        if (U.nch == 0)  // an empty K range leaves the accumulator unwritten
 #pragma unroll
           for (int q = 0; q < 32; q++) r[q] = 0u;
         if (W) {
 #pragma unroll
           for (int q = 0; q < 32; q++) W[lr + (cb * 32 + q) * kTileM] = __uint_as_float(r[q]);
         } else if (row >= 0) {
+          // Loads of 16 columns first, then their stores: one memory latency
+          // per 16 columns (as a read-modify-write loop the loads could not
+          // move above the preceding stores).
 #pragma unroll
-          for (int q = 0; q < 32; q++) {
-            const int col = n0 + cb * 32 + q;
-            if (col < N && (!pb.lower || row >= col))
-              Cout[row + (int64_t)col * pb.ldc] -= __uint_as_float(r[q]);
+          for (int hh = 0; hh < 2; hh++) {
+            float cv[16];
+#pragma unroll
+            for (int q = 0; q < 16; q++) {
+              const int col = n0 + cb * 32 + 16 * hh + q;
+              cv[q] = (col < N && (!lower || row >= col)) ? Cout[row + (int64_t)col * ldc] : 0.0f;
+            }
+#pragma unroll
+            for (int q = 0; q < 16; q++) {
+              const int col = n0 + cb * 32 + 16 * hh + q;
+              if (col < N && (!lower || row >= col))
+                Cout[row + (int64_t)col * ldc] = cv[q] - __uint_as_float(r[16 * hh + q]);
+            }
           }
         }
       }
-    } else if (lane == 0) {
-      atomicExch(&st->timeout, 1);
-      // Let any MMA still in flight finish before the memory is released.
-      wait_bounded(done, 0);
+      // The accumulator may be overwritten by the next unit's MMAs.
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      arrive(acc_free);
     }
   }
+  if (tid == 0 && s_fail) atomicExch(&st->timeout, 1);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 1)
@@ -450,11 +528,12 @@ int tc_ctas_per_sm() { return tc::kStages <= 3 ? 2 : 1; }
 
 int tc_gemm_smem_bytes(int mode) {
   const uint32_t stage = mode == 1 ? tc::Cfg<1>::kStage : tc::Cfg<0>::kStage;
-  return static_cast<int>(tc::kStages * stage);
+  // stages, then the problems' first units
+  return static_cast<int>(tc::kStages * stage + kMaxProbSmem * sizeof(int));
 }
 
 template <int MODE>
-static void launch_mode(const GemmProb *probs, int nprob, int tiles, const float *pack,
+static void launch_mode(const GemmProb *probs, int nprob, int units, const float *pack,
                         const float *packd, const float *packs, float *panel, float *uarena,
                         float *ws, FactorStatus *st, cudaStream_t s) {
   static bool attr = false;
@@ -464,19 +543,21 @@ static void launch_mode(const GemmProb *probs, int nprob, int tiles, const float
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     attr = true;
   }
-  launch(k_gemm_tc<MODE>, tiles, tc::kThreads, smem, s, probs, nprob, pack, packd, packs, panel,
-         uarena, ws, st);
+  const int grid = std::min(units, kSMs * tc_ctas_per_sm());
+  launch(k_gemm_tc<MODE>, grid, tc::kThreads, smem, s, probs, nprob, units, pack, packd, packs,
+         panel, uarena, ws, st);
 }
 
-void launch_gemm_tc(int mode, const GemmProb *probs, int nprob, int tiles, const float *pack,
+void launch_gemm_tc(int mode, const GemmProb *probs, int nprob, int units, const float *pack,
                     const float *packd, const float *packs, float *panel, float *uarena,
                     float *ws, FactorStatus *st, cudaStream_t s) {
+  if (units <= 0) return;
   if (mode == 0)
-    launch_mode<0>(probs, nprob, tiles, pack, packd, packs, panel, uarena, ws, st, s);
+    launch_mode<0>(probs, nprob, units, pack, packd, packs, panel, uarena, ws, st, s);
   else if (mode == 1)
-    launch_mode<1>(probs, nprob, tiles, pack, packd, packs, panel, uarena, ws, st, s);
+    launch_mode<1>(probs, nprob, units, pack, packd, packs, panel, uarena, ws, st, s);
   else
-    launch_mode<2>(probs, nprob, tiles, pack, packd, packs, panel, uarena, ws, st, s);
+    launch_mode<2>(probs, nprob, units, pack, packd, packs, panel, uarena, ws, st, s);
 }
 
 }  // namespace mpir
