@@ -88,6 +88,8 @@ struct LevelPlan {
   int32_t sf_begin = 0, sf_count = 0;
   int32_t sw_begin = 0, sw_count = 0;  // warp-solved fronts (swarp list)
   int32_t fwd_items = 0, bwd_chunk_items = 0, bwd_owner_items = 0;
+  // Offsets of the level's item -> front maps (front index within the level).
+  int64_t fwd_map0 = 0, chunk_map0 = 0, own_map0 = 0;
 };
 
 // Everything the kernels need about one analysed pattern.
@@ -108,7 +110,7 @@ class Plan {
   DeviceBuffer sfirst, srowptr, srows, srel, slofs, uofs, zofs, child_ptr,
       child_list, perm;
   DeviceBuffer small_list, large_list, steps, ea_tasks, zero_segs, linv_ofs_d, gemm_probs,
-      solve_fronts, swarp_list, sblock_list, gp, gsrc;
+      solve_fronts, swarp_list, sblock_list, gp, gsrc, fwd_map, chunk_map, own_map;
   int64_t      ws_elems = 0;  // split-K partial tiles (floats)
   std::vector<int32_t> h_small, h_large;
   // Solve lists: fronts solved by one warp, fronts with a SolveFront entry

@@ -746,6 +746,7 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
   h_swarp.clear();
   h_sblock.clear();
   std::vector<int64_t> gp_h, gsrc_h;
+  std::vector<int32_t> fwd_map_h, chunk_map_h, own_map_h;
   std::vector<SolveFront> sfronts;
   update_flops = 0;
   trsm_flops   = 0;
@@ -993,6 +994,16 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
       sfronts.push_back(f);
     }
     L.sf_count  = static_cast<int32_t>(sfronts.size()) - L.sf_begin;
+    // Item -> front maps of the level's solve launches.
+    L.fwd_map0   = static_cast<int64_t>(fwd_map_h.size());
+    L.chunk_map0 = static_cast<int64_t>(chunk_map_h.size());
+    L.own_map0   = static_cast<int64_t>(own_map_h.size());
+    for (int32_t q = 0; q < L.sf_count; q++) {
+      const SolveFront &f = sfronts[L.sf_begin + q];
+      for (int64_t i = 0; i < (f.h + kNB - 1) / kNB; i++) fwd_map_h.push_back(q);
+      for (int32_t i = 0; i < f.chunks; i++) chunk_map_h.push_back(q);
+      for (int32_t i = 0; i < f.nb; i++) own_map_h.push_back(q);
+    }
     L.sw_count  = static_cast<int32_t>(h_swarp.size()) - L.sw_begin;
     spart_elems = std::max(spart_elems, spart);
     L.u_begin = static_cast<int32_t>(probs.size());
@@ -1056,6 +1067,9 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
   sblock_list  = upload(h_sblock, s);
   gp           = upload(gp_h, s);
   gsrc         = upload(gsrc_h, s);
+  fwd_map      = upload(fwd_map_h, s);
+  chunk_map    = upload(chunk_map_h, s);
+  own_map      = upload(own_map_h, s);
   sync_elems   = 2 * static_cast<int64_t>(levels.size()) + 2 * nflags;
   MPIR_CUDA(cudaStreamSynchronize(s));
 }

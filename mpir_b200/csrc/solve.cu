@@ -126,12 +126,39 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta)
     for (int a = lane; a < rc; a += 32) z[rl[a]] += zc[a];
     __syncwarp();
   }
-  const float *P = panel + slofs[J];
-  for (int k = 0; k < w; k++) {
-    const double zk = z[k];
-    for (int i = k + 1 + lane; i < h; i += 32)
-      z[i] -= static_cast<double>(P[i + (int64_t)k * h]) * zk;
-    __syncwarp();
+  // Columns four at a time; the next four columns' entries of this lane's
+  // rows (lane + 32 t) are loaded while the current four are applied.
+  const float  *P  = panel + slofs[J];
+  constexpr int RT = kSmallH / 32;
+  float         cur[4][RT], nxt[4][RT];
+  auto          load4 = [&](float (*buf)[RT], int k0) {
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+#pragma unroll
+      for (int t = 0; t < RT; t++) {
+        const int k = k0 + u, i = lane + 32 * t;
+        buf[u][t]   = (k < w && i > k && i < h) ? P[i + (int64_t)k * h] : 0.0f;
+      }
+  };
+  load4(cur, 0);
+  for (int k0 = 0; k0 < w; k0 += 4) {
+    if (k0 + 4 < w) load4(nxt, k0 + 4);
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int k = k0 + u;
+      if (k >= w) break;
+      const double zk = z[k];
+#pragma unroll
+      for (int t = 0; t < RT; t++) {
+        const int i = lane + 32 * t;
+        if (i > k && i < h) z[i] -= static_cast<double>(cur[u][t]) * zk;
+      }
+      __syncwarp();
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+#pragma unroll
+      for (int t = 0; t < RT; t++) cur[u][t] = nxt[u][t];
   }
   double *zo = zbuf + zofs[J];
   for (int i = lane; i < h; i += 32) {
@@ -171,15 +198,6 @@ __device__ __forceinline__ int take_ticket(int32_t *counter) {
   return s_ticket;
 }
 
-__device__ __forceinline__ int find_front(const SolveFront *fr, int nfr, int item,
-                                          int SolveFront::*first) {
-  int lo = 0, hi = nfr - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) / 2;
-    if (fr[mid].*first <= item) lo = mid; else hi = mid - 1;
-  }
-  return lo;
-}
 
 // Forward solve of the large fronts of one level: one CTA per 128-row block
 // R of a front.  z_R -= L_{R,b} y_b for the column blocks b left of R, in
@@ -190,7 +208,8 @@ __device__ __forceinline__ int find_front(const SolveFront *fr, int nfr, int ite
 // block then solves y_R = Linv_R z_R into x and releases flag R; rows at or
 // past w are the front's update vector for its parent.
 __global__ void __launch_bounds__(kSolveThreads, 1)
-    k_fwd_fronts(const SolveFront *fr, int nfr, const float *panel, const double *linv64,
+    k_fwd_fronts(const SolveFront *fr, const int32_t *fmap, const float *panel,
+                 const double *linv64,
                  const int64_t *gp, const int64_t *gsrc, double *x, double *zbuf,
                  int32_t *tickets, int32_t *flags, int32_t *err) {
   extern __shared__ double tri[];  // kTri doubles: the staged Linv_R
@@ -198,7 +217,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   __shared__ double yw[kSolveThreads / 32][32];
   __shared__ double part[4][kNB];
   const int         item = take_ticket(tickets);
-  const SolveFront  F    = fr[find_front(fr, nfr, item, &SolveFront::fwd0)];
+  const SolveFront  F    = fr[fmap[item]];
   const int         R    = item - F.fwd0;
   if (R < F.nb)
     stage_lower(linv64 + F.linv + static_cast<int64_t>(R) * kNB * kNB, tri,
@@ -258,13 +277,10 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
       if (qq == 0 && r >= w && r < h)
         z -= (part[0][rr] + part[1][rr]) + (part[2][rr] + part[3][rr]);
     }
-    // The CTA's writes of y happen before thread 0's release (bar.sync,
-    // then a cumulative fence and the release store).
+    // The CTA's writes of y happen before thread 0's release store (bar.sync,
+    // then the release, which is cumulative).
     __syncthreads();
-    if (tid == 0) {
-      __threadfence();
-      st_release(fl + R, 1);
-    }
+    if (tid == 0) st_release(fl + R, 1);
   }
   if (qq == 0 && r >= w && r < h) zbuf[F.zofs + r] = z;
 }
@@ -292,15 +308,42 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta)
   double        *z  = zs[warp];
   for (int i = lane; i < h; i += 32) z[i] = i < w ? x[f + i] : x[rw[i]];
   __syncwarp();
-  const float *P = panel + slofs[J];
-  for (int k = w - 1; k >= 0; k--) {
-    double s = 0.0;
-    for (int i = k + 1 + lane; i < h; i += 32)
-      s += static_cast<double>(P[i + (int64_t)k * h]) * z[i];
+  // Columns four at a time from the last; the next four columns' entries of
+  // this lane's rows (lane + 32 t) are loaded while the current four are used.
+  const float  *P  = panel + slofs[J];
+  constexpr int RT = kSmallH / 32;
+  float         cur[4][RT], nxt[4][RT];
+  auto          load4 = [&](float (*buf)[RT], int k0) {  // columns k0, k0-1, ..
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) z[k] -= s;
-    __syncwarp();
+    for (int u = 0; u < 4; u++)
+#pragma unroll
+      for (int t = 0; t < RT; t++) {
+        const int k = k0 - u, i = lane + 32 * t;
+        buf[u][t]   = (k >= 0 && i > k && i < h) ? P[i + (int64_t)k * h] : 0.0f;
+      }
+  };
+  load4(cur, w - 1);
+  for (int k0 = w - 1; k0 >= 0; k0 -= 4) {
+    if (k0 - 4 >= 0) load4(nxt, k0 - 4);
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int k = k0 - u;
+      if (k < 0) break;
+      double s = 0.0;
+#pragma unroll
+      for (int t = 0; t < RT; t++) {
+        const int i = lane + 32 * t;
+        if (i > k && i < h) s += static_cast<double>(cur[u][t]) * z[i];
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      if (lane == 0) z[k] -= s;
+      __syncwarp();
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+#pragma unroll
+      for (int t = 0; t < RT; t++) cur[u][t] = nxt[u][t];
   }
   for (int i = lane; i < w; i += 32) x[f + i] = z[i];
 }
@@ -310,10 +353,11 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta)
 // front and writes t_k = sum_r L_{r,k} z_r for every column k of the front
 // (warp per column, rows over the lanes, shuffle reduction) to its partials.
 __global__ void __launch_bounds__(kSolveThreads)
-    k_bwd_chunks(const SolveFront *fr, int nfr, const float *panel, const int32_t *srows,
+    k_bwd_chunks(const SolveFront *fr, const int32_t *fmap, const float *panel,
+                 const int32_t *srows,
                  const double *x, double *part) {
   __shared__ double zr[kNB];
-  const SolveFront  F = fr[find_front(fr, nfr, blockIdx.x, &SolveFront::chunk0)];
+  const SolveFront  F = fr[fmap[blockIdx.x]];
   const int         c = blockIdx.x - F.chunk0;
   const int         tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
   const int64_t     h = F.h, w = F.w;
@@ -346,7 +390,8 @@ __global__ void __launch_bounds__(kSolveThreads)
 // front vector, and flag b is released.  In a tile, warp v takes the
 // block's columns 8v .. 8v+7 and the lanes the rows.
 __global__ void __launch_bounds__(kSolveThreads, 1)
-    k_bwd_fronts(const SolveFront *fr, int nfr, const float *panel, const double *linv64t,
+    k_bwd_fronts(const SolveFront *fr, const int32_t *fmap, const float *panel,
+                 const double *linv64t,
                  double *x, const double *part, int32_t *tickets,
                  int32_t *flags, int32_t *err) {
   extern __shared__ double tri[];  // kTri doubles: the staged Linv_b^T
@@ -354,7 +399,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   __shared__ double ts[kNB];
   __shared__ double red[4][kNB];
   const int         item = take_ticket(tickets);
-  const SolveFront  F    = fr[find_front(fr, nfr, item, &SolveFront::own0)];
+  const SolveFront  F    = fr[fmap[item]];
   const int         b    = F.nb - 1 - (item - F.own0);
   stage_upper(linv64t + F.linv + static_cast<int64_t>(b) * kNB * kNB, tri,
               min(kNB, F.w - b * kNB));
@@ -418,10 +463,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   const double xb = block_upper_apply(tri, v, nbk, red);
   if (tid < nbk) x[F.col0 + b * kNB + tid] = xb;
   __syncthreads();
-  if (tid == 0) {
-    __threadfence();
-    st_release(fl + b, 1);
-  }
+  if (tid == 0) st_release(fl + b, 1);
 }
 
 // ---------------------------------------------------------------------------
@@ -502,7 +544,8 @@ void ldlt_solve(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
              zbuf);
     if (L.sf_count > 0) {
       launch(k_fwd_fronts, L.fwd_items, kSolveThreads, kTri * sizeof(double), s, sf + L.sf_begin,
-             L.sf_count, pan, lv, P.gp.as<int64_t>(), P.gsrc.as<int64_t>(), x, zbuf, sync + 2 * t, ffl, err);
+             P.fwd_map.as<int32_t>() + L.fwd_map0, pan, lv, P.gp.as<int64_t>(),
+             P.gsrc.as<int64_t>(), x, zbuf, sync + 2 * t, ffl, err);
     }
   }
   if (phases & kDiagonal)
@@ -521,10 +564,12 @@ void ldlt_solve(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
     if (L.sf_count > 0) {
       if (L.bwd_chunk_items > 0)
         launch(k_bwd_chunks, L.bwd_chunk_items, kSolveThreads, 0, s, sf + L.sf_begin,
-               L.sf_count, pan, P.srows.as<int32_t>(), static_cast<const double *>(x),
+               P.chunk_map.as<int32_t>() + L.chunk_map0, pan, P.srows.as<int32_t>(),
+               static_cast<const double *>(x),
                ws.part.as<double>());
       launch(k_bwd_fronts, L.bwd_owner_items, kSolveThreads, kTri * sizeof(double), s,
-             sf + L.sf_begin, L.sf_count, pan, F.linv64t.as<double>(), x,
+             sf + L.sf_begin, P.own_map.as<int32_t>() + L.own_map0, pan,
+             F.linv64t.as<double>(), x,
              static_cast<const double *>(ws.part.as<double>()), sync + 2 * t + 1, bfl, err);
     }
   }
