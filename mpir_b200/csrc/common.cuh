@@ -62,8 +62,9 @@ struct StepDesc {
 };
 
 // One large front in the triangular solves.  The forward solve of a level
-// runs one CTA per row block of 128 rows of each front (front-major, row
-// blocks ascending); the backward solve one CTA per 128-row chunk of the
+// runs one CTA per row block of 128 rows of each front (first the diagonal
+// row blocks of all fronts, front-major, then the off-diagonal ones); the
+// backward solve one CTA per 128-row chunk of the
 // off-diagonal rows (partial sums for all columns) and then one CTA per
 // column block (front-major, last block first).  CTAs take their work in
 // ticket order, so every block they wait for belongs to an earlier ticket.
@@ -78,7 +79,6 @@ struct SolveFront {
   int32_t h, w, nb;
   int32_t col0;    // permuted index of the front's first column
   int32_t flag0;   // first of the front's nb ready flags
-  int32_t fwd0;    // first forward CTA of the front in its level
   int32_t chunk0, chunks;  // backward chunk CTAs
   int32_t own0;    // first backward column-block CTA
 };

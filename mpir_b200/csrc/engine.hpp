@@ -110,7 +110,7 @@ class Plan {
   DeviceBuffer sfirst, srowptr, srows, srel, slofs, uofs, zofs, child_ptr,
       child_list, perm;
   DeviceBuffer small_list, large_list, steps, ea_tasks, zero_segs, linv_ofs_d, gemm_probs,
-      solve_fronts, swarp_list, sblock_list, gp, gsrc, fwd_map, chunk_map, own_map;
+      solve_fronts, swarp_list, sblock_list, gp, gsrc, fwd_map, fwd_row, chunk_map, own_map;
   int64_t      ws_elems = 0;  // split-K partial tiles (floats)
   std::vector<int32_t> h_small, h_large;
   // Solve lists: fronts solved by one warp, fronts with a SolveFront entry

@@ -746,7 +746,7 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
   h_swarp.clear();
   h_sblock.clear();
   std::vector<int64_t> gp_h, gsrc_h;
-  std::vector<int32_t> fwd_map_h, chunk_map_h, own_map_h;
+  std::vector<int32_t> fwd_map_h, fwd_row_h, chunk_map_h, own_map_h;
   std::vector<SolveFront> sfronts;
   update_flops = 0;
   trsm_flops   = 0;
@@ -982,7 +982,6 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
       f.col0   = static_cast<int32_t>(S.sfirst[J]);
       f.flag0  = static_cast<int32_t>(nflags);
       nflags += f.nb;
-      f.fwd0   = L.fwd_items;
       L.fwd_items += static_cast<int32_t>((h + kNB - 1) / kNB);
       f.chunks = static_cast<int32_t>((h - w + kNB - 1) / kNB);
       f.chunk0 = L.bwd_chunk_items;
@@ -998,9 +997,24 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
     L.fwd_map0   = static_cast<int64_t>(fwd_map_h.size());
     L.chunk_map0 = static_cast<int64_t>(chunk_map_h.size());
     L.own_map0   = static_cast<int64_t>(own_map_h.size());
+    // Forward: every front's diagonal row blocks first (their chains start
+    // together), then the off-diagonal row blocks, which wait on them.
     for (int32_t q = 0; q < L.sf_count; q++) {
       const SolveFront &f = sfronts[L.sf_begin + q];
-      for (int64_t i = 0; i < (f.h + kNB - 1) / kNB; i++) fwd_map_h.push_back(q);
+      for (int32_t i = 0; i < f.nb; i++) {
+        fwd_map_h.push_back(q);
+        fwd_row_h.push_back(i);
+      }
+    }
+    for (int32_t q = 0; q < L.sf_count; q++) {
+      const SolveFront &f = sfronts[L.sf_begin + q];
+      for (int32_t i = f.nb; i < (f.h + kNB - 1) / kNB; i++) {
+        fwd_map_h.push_back(q);
+        fwd_row_h.push_back(i);
+      }
+    }
+    for (int32_t q = 0; q < L.sf_count; q++) {
+      const SolveFront &f = sfronts[L.sf_begin + q];
       for (int32_t i = 0; i < f.chunks; i++) chunk_map_h.push_back(q);
       for (int32_t i = 0; i < f.nb; i++) own_map_h.push_back(q);
     }
@@ -1068,6 +1082,7 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
   gp           = upload(gp_h, s);
   gsrc         = upload(gsrc_h, s);
   fwd_map      = upload(fwd_map_h, s);
+  fwd_row      = upload(fwd_row_h, s);
   chunk_map    = upload(chunk_map_h, s);
   own_map      = upload(own_map_h, s);
   sync_elems   = 2 * static_cast<int64_t>(levels.size()) + 2 * nflags;

@@ -208,7 +208,8 @@ __device__ __forceinline__ int take_ticket(int32_t *counter) {
 // block then solves y_R = Linv_R z_R into x and releases flag R; rows at or
 // past w are the front's update vector for its parent.
 __global__ void __launch_bounds__(kSolveThreads, 1)
-    k_fwd_fronts(const SolveFront *fr, const int32_t *fmap, const float *panel,
+    k_fwd_fronts(const SolveFront *fr, const int32_t *fmap, const int32_t *frow,
+                 const float *panel,
                  const double *linv64,
                  const int64_t *gp, const int64_t *gsrc, double *x, double *zbuf,
                  int32_t *tickets, int32_t *flags, int32_t *err) {
@@ -218,7 +219,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   __shared__ double part[4][kNB];
   const int         item = take_ticket(tickets);
   const SolveFront  F    = fr[fmap[item]];
-  const int         R    = item - F.fwd0;
+  const int         R    = frow[item];
   if (R < F.nb)
     stage_lower(linv64 + F.linv + static_cast<int64_t>(R) * kNB * kNB, tri,
                 min(kNB, F.w - R * kNB));
@@ -544,7 +545,8 @@ void ldlt_solve(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
              zbuf);
     if (L.sf_count > 0) {
       launch(k_fwd_fronts, L.fwd_items, kSolveThreads, kTri * sizeof(double), s, sf + L.sf_begin,
-             P.fwd_map.as<int32_t>() + L.fwd_map0, pan, lv, P.gp.as<int64_t>(),
+             P.fwd_map.as<int32_t>() + L.fwd_map0, P.fwd_row.as<int32_t>() + L.fwd_map0, pan,
+             lv, P.gp.as<int64_t>(),
              P.gsrc.as<int64_t>(), x, zbuf, sync + 2 * t, ffl, err);
     }
   }
