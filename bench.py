@@ -66,11 +66,31 @@ def workload_name(grid):
             f"refactorization + f64 GMRES-IR solve, 1 RHS")
 
 
+def gemm_traffic(args):
+    """DRAM bytes per launch of the tensor-core update kernel, from the ncu
+    capture summarised under profiles/ (taken on the grid3d-48 float32
+    workload only; None for other workloads)."""
+    if args.grid != 48 or args.uf != "f32":
+        return None
+    path = os.path.join(ROOT, "profiles", "k_gemm_tc_grid3d48_dram.md")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
 def load_peaks():
+    """HBM GB/s and dense bf16 TFLOP/s.  The updates run inside a long step,
+    so the sustained bf16 figure is the one they are held against."""
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
         d = json.load(open(p))
-        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
+        bf16 = d.get("bf16_tflops_sustained", d.get("bf16_tflops", 1590.0))
+        return d.get("hbm_gbs", 6650.0), bf16, "measured (bf16 sustained)"
     return 6650.0, 1590.0, "fallback"
 
 
@@ -460,9 +480,19 @@ def run_gpu(args):
     bound, amount, unit, peak = work.get(dom, ("hbm", float("nan"), "GB/s", hbm))
     dom_s = cls_ms[dom] / 1e3
     achieved = amount / dom_s if dom_s > 0 else float("nan")
-    roofline = {"bound": bound, "kernel": dom, "achieved": achieved, "peak": peak,
+    kernel_names = {"trailing_update": "k_gemm_tc (tensor-core updates) + k_split_reduce",
+                    "solve_forward": "k_fwd_fronts / k_fwd_small",
+                    "solve_backward": "k_bwd_fronts / k_bwd_chunks / k_bwd_small"}
+    roofline = {"bound": bound, "kernel": kernel_names.get(dom, dom), "class": dom,
+                "achieved": achieved, "peak": peak,
                 "unit": unit, "frac": achieved / peak, "peak_source": peak_kind,
-                "traffic": None,
+                "traffic": gemm_traffic(args) if dom == "trailing_update" else None,
+                "traffic_unit": "bytes per launch (DRAM read + write, one ncu capture)",
+                # 3xTF32: three tf32 MMAs per float32 product, tf32 at half
+                # the bf16 rate, so its own ceiling is peak / 6.
+                "frac_of_tf32x3_ceiling": (achieved / (peak / 6.0)
+                                           if dom == "trailing_update" and args.uf == "f32"
+                                           else None),
                 "class_ms": {k: round(v, 3) for k, v in cls_ms.items() if v > 0},
                 "class_launches": {k: v[1] for k, v in kt.items() if v[1] > 0}}
 
