@@ -183,6 +183,35 @@ int mpir_solver_solve(mpir_solver s, const double *b, double *x,
 int mpir_solver_solve_device(mpir_solver s, const double *d_b, double *d_x,
                              mpir_report *rep);
 
+/* nrhs right-hand sides with the current factor: B and X hold nrhs
+ * contiguous vectors of length n (column-major n x nrhs, host memory); one
+ * GMRES-IR solve per column, each exactly as mpir_solver_solve; reps (NULL,
+ * or nrhs reports) receives each solve's report.  Stops at the first error.
+ * The reference solves one right-hand side per GmresLDLIR::Solve call
+ * (gmres_ir.hpp:534); this entry point is that loop. */
+int mpir_solver_solve_many(mpir_solver s, int64_t nrhs, const double *B,
+                           double *X, mpir_report *reps);
+
+/* Plain iterative refinement with the LDL^T factor, LUIR_QDLDL
+ * (qdldl-luir/luir.hpp:33-241) with float64 residual, working and solution
+ * vectors: x0 = solve(b); r = b - A x; d = solve(r / |r|) |r|; x += d, until
+ * |d| / |x_old| <= 10 eps(float64) or |d| / |d_prev| >= 1/2 (at most
+ * maxiter steps; maxiter = 0: the single solve).  The right-hand side and
+ * result of each solve are rounded to the factor's type, as the reference
+ * keeps them in FACTPREC.  rep->ir_iterations = the reference's
+ * num_refinement_steps_, rep->residual_norm = its relative_residual_
+ * (|b - A x|_inf / |b|_inf), rep->precond_applies = solves.
+ * mpir_solver_luir[_device] use the solver's current factor;
+ * mpir_luir_qdldl analyses and factors A (upper CSC, caller order) first,
+ * as the reference does, with fact_prec MPIR_F32, MPIR_BF16 or MPIR_F16. */
+int mpir_solver_luir(mpir_solver s, const double *b, double *x, int maxiter,
+                     mpir_report *rep);
+int mpir_solver_luir_device(mpir_solver s, const double *d_b, double *d_x,
+                            int maxiter, mpir_report *rep);
+int mpir_luir_qdldl(int64_t n, const int64_t *Ap, const int64_t *Ai,
+                    const double *Ax, const double *b, double *x,
+                    int fact_prec, int maxiter, mpir_report *rep, int device);
+
 /* Launch the solver's work on a caller stream (a cudaStream_t; NULL
  * restores the solver's own stream). */
 int mpir_solver_set_stream(mpir_solver s, void *stream);

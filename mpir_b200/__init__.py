@@ -99,6 +99,10 @@ def lib():
         "mpir_solver_solve": (i32, [vp, vp, vp, vp]),
         "mpir_solver_solve_device": (i32, [vp, vp, vp, vp]),
         "mpir_solver_set_stream": (i32, [vp, vp]),
+        "mpir_solver_solve_many": (i32, [vp, i64, vp, vp, vp]),
+        "mpir_solver_luir": (i32, [vp, vp, vp, i32, vp]),
+        "mpir_solver_luir_device": (i32, [vp, vp, vp, i32, vp]),
+        "mpir_luir_qdldl": (i32, [i64, vp, vp, vp, vp, vp, i32, i32, vp, i32]),
         "mpir_solver_info": (i32, [vp, vp]),
         "mpir_solver_symbolic": (i32, [vp, vp, vp, vp, vp, vp, vp]),
         "mpir_solver_export_factor": (i32, [vp, vp, vp, vp, vp, vp]),
@@ -196,6 +200,22 @@ def QDLDL_solve(n, Lp, Li, Lx, Dinv, x, fact_prec="f32", device=0):
     return x
 
 
+def LUIR_QDLDL(n, Ap, Ai, Ax, b, fact_prec="f32", maxiter=10, device=0):
+    """LUIR_QDLDL<FACTPREC, double, double, double> (qdldl-luir/luir.hpp):
+    factor A (upper CSC) in ``fact_prec`` and refine, all on the GPU.
+    Returns (x, stats) with the reference's Stats fields
+    num_refinement_steps_, relative_residual_ and Lnz_, plus the report."""
+    Ap, Ai, Ax, b = _i64(Ap), _i64(Ai), _f64(Ax), _f64(b)
+    x = np.zeros(n, np.float64)
+    rep = Report()
+    _check(lib().mpir_luir_qdldl(n, _p(Ap), _p(Ai), _p(Ax), _p(b), _p(x), _PREC[fact_prec],
+                                 int(maxiter), C.byref(rep), device))
+    r = rep.as_dict()
+    stats = {"num_refinement_steps_": r["ir_iterations"],
+             "relative_residual_": r["residual_norm"], "report": r}
+    return x, stats
+
+
 def QDLDL_solve_noalloc(n, Lp, Li, Lx, Dinv, x, device=0):
     """QDLDL_solve for callers that cannot allocate device memory (inside an
     open stream capture, or under a process-wide pooling allocator): float32
@@ -279,6 +299,30 @@ class GmresLDLIR:
         x = np.zeros(self.n, np.float64)
         rep = Report()
         _check(lib().mpir_solver_solve(self._h, _p(b), _p(x), C.byref(rep)))
+        self.last_report = rep.as_dict()
+        return x
+
+    def SolveMany(self, B):
+        """B: (nrhs, n) right-hand sides (one per row); returns X of the
+        same shape, one GMRES-IR solve per row; reports in last_reports."""
+        B = np.ascontiguousarray(B, dtype=np.float64)
+        if B.ndim != 2 or B.shape[1] != self.n:
+            return np.zeros((0, self.n), np.float64)
+        X = np.zeros_like(B)
+        reps = (Report * max(B.shape[0], 1))()
+        _check(lib().mpir_solver_solve_many(self._h, B.shape[0], _p(B), _p(X), reps))
+        self.last_reports = [reps[k].as_dict() for k in range(B.shape[0])]
+        return X
+
+    def luir(self, b, maxiter=10):
+        """Plain iterative refinement with the current factor (LUIR_QDLDL's
+        loop, qdldl-luir/luir.hpp:182-232); the report's ir_iterations and
+        residual_norm are the reference's num_refinement_steps_ and
+        relative_residual_."""
+        b = _f64(b)
+        x = np.zeros(self.n, np.float64)
+        rep = Report()
+        _check(lib().mpir_solver_luir(self._h, _p(b), _p(x), int(maxiter), C.byref(rep)))
         self.last_report = rep.as_dict()
         return x
 

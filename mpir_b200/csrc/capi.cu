@@ -465,6 +465,66 @@ int mpir_solver_solve_device(mpir_solver s, const double *d_b, double *d_x, mpir
   });
 }
 
+int mpir_solver_solve_many(mpir_solver s, int64_t nrhs, const double *B, double *X,
+                           mpir_report *reps) {
+  MPIR_NEED(s);
+  return guard([&]() -> int {
+    if (nrhs < 0 || (nrhs > 0 && (!B || !X)))
+      throw StatusError(MPIR_ERR_ARGUMENT, "invalid argument");
+    const int64_t n = s->impl->plan().S.n;
+    for (int64_t k = 0; k < nrhs; k++) {
+      const int rc = s->impl->solve(B + k * n, X + k * n,
+                                    reps ? reinterpret_cast<Report *>(reps + k) : nullptr);
+      if (rc != MPIR_OK) return rc;
+    }
+    return MPIR_OK;
+  });
+}
+
+int mpir_solver_luir(mpir_solver s, const double *b, double *x, int maxiter, mpir_report *rep) {
+  MPIR_NEED(s);
+  return guard([&]() -> int {
+    if (maxiter < 0) throw StatusError(MPIR_ERR_ARGUMENT, "maxiter must be >= 0");
+    return s->impl->luir(b, x, maxiter, reinterpret_cast<Report *>(rep));
+  });
+}
+
+int mpir_solver_luir_device(mpir_solver s, const double *d_b, double *d_x, int maxiter,
+                            mpir_report *rep) {
+  MPIR_NEED(s);
+  return guard([&]() -> int {
+    if (maxiter < 0) throw StatusError(MPIR_ERR_ARGUMENT, "maxiter must be >= 0");
+    return s->impl->luir_device(d_b, d_x, maxiter, reinterpret_cast<Report *>(rep));
+  });
+}
+
+int mpir_luir_qdldl(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *Ax,
+                    const double *b, double *x, int fact_prec, int maxiter, mpir_report *rep,
+                    int device) {
+  return guard([&]() -> int {
+    if (n < 0 || !Ap || !Ai || !Ax || !b || !x || maxiter < 0)
+      throw StatusError(MPIR_ERR_ARGUMENT, "invalid argument");
+    if (fact_prec != kF32 && fact_prec != kBF16 && fact_prec != kF16)
+      throw StatusError(MPIR_ERR_UNSUPPORTED, "provided factor types: F32, BF16, F16");
+    for (int64_t j = 0; j < n; j++) {
+      if (Ap[j + 1] <= Ap[j])
+        throw StatusError(MPIR_ERR_INPUT, "empty column " + std::to_string(j));
+      for (int64_t p = Ap[j]; p < Ap[j + 1]; p++)
+        if (Ai[p] > j)
+          throw StatusError(MPIR_ERR_INPUT, "entry below the diagonal in column " + std::to_string(j));
+    }
+    Solver sv(fact_prec, kF64, kF64, device);
+    sv.analyze(n, Ap, Ai, Ax, MPIR_ORDER_AUTO);
+    const int fr = sv.factor(Ax);
+    if (fr == kBadInput) {
+      g_err = "zero pivot";
+      return fr;
+    }
+    if (fr != kOk) return fr;
+    return sv.luir(b, x, maxiter, reinterpret_cast<Report *>(rep));
+  });
+}
+
 int mpir_solver_set_stream(mpir_solver s, void *stream) {
   MPIR_NEED(s);
   s->impl->set_stream(static_cast<cudaStream_t>(stream));

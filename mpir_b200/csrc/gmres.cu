@@ -335,6 +335,113 @@ int Solver::solve_device(const double *d_b, double *d_x, Report *rep) {
   return kOk;
 }
 
+// Plain iterative refinement with the LDL^T factor, as LUIR_QDLDL
+// (qdldl-luir/luir.hpp:157-236) with residual, working and solution vectors
+// in float64: x0 = solve(b); then r = b - A x, d = solve(r / |r|) |r|,
+// x += d, until |d| / |x_old| <= 10 eps(float64) or |d| / |d_prev| >= 1/2,
+// at most maxiter steps.  The right-hand side of every solve and its result
+// are rounded to the factor's type, as the reference keeps them in FACTPREC.
+// Runs on the scaled, permuted system; the norms of the stop test are those
+// of the unscaled vectors.
+int Solver::luir_device(const double *d_b, double *d_x, int maxiter, Report *rep) {
+  if (!plan_) throw std::logic_error("solve before analyze");
+  if (!num_.valid) throw std::logic_error("solve before factor");
+  MPIR_CUDA(cudaSetDevice(device));
+  ensure_vectors();
+  Report        st;
+  const Plan   &P = *plan_;
+  const int64_t n = P.S.n;
+  cudaStream_t  s = stream_;
+  MPIR_CUDA(cudaEventRecord(ev0_, s));
+  if (n == 0) {
+    if (rep) *rep = st;
+    return kOk;
+  }
+  const int64_t *Kp = P.Kp.as<int64_t>();
+  const int32_t *Kj = P.Kj.as<int32_t>();
+  const double  *Kv = num_.Kval.as<double>();
+  double *bs = bs_.as<double>(), *x = x_.as<double>(), *r = r_.as<double>(),
+         *ADp = ADp_.as<double>();
+  vec_.rhs_in(P.perm.as<int64_t>(), num_.AD.as<double>(), d_b, bs, ADp, bp_.as<double>(), s);
+  MPIR_CUDA(cudaMemcpyAsync(x, bs, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  vec_.round_to(uf, x, s);
+  ldlt_solve_graph(P, num_, x, ws_, s, own_stream_);
+  st.precond_applies++;
+  vec_.round_to(uf, x, s);
+  const double eps = eps_of(kF64);
+  double       d0  = DBL_MAX;
+  for (int it = 1; it <= maxiter; it++) {
+    vec_.residual(Kp, Kj, Kv, x, bs, r, false, 0, s);
+    st.spmv_count++;
+    vec_.round_to(uf, r, s);
+    double rn;
+    vec_.read_inf(&rn, 0, 1, s);
+    if (rn == 0.0) {
+      st.stop_reason = 3;
+      break;
+    }
+    if (!std::isfinite(rn)) {
+      st.stop_reason = 4;
+      break;
+    }
+    vec_.scale(r, 1.0 / rn, r, s);
+    vec_.round_to(uf, r, s);
+    ldlt_solve_graph(P, num_, r, ws_, s, own_stream_);
+    st.precond_applies++;
+    vec_.round_to(uf, r, s);
+    vec_.ir_update(r, rn, x, s, ADp);
+    double nrm[2];
+    vec_.read_inf(nrm, 1, 2, s);
+    st.ir_iterations = it;
+    if (nrm[0] / nrm[1] <= 10 * eps) {
+      st.stop_reason = 1;
+      break;
+    }
+    if (nrm[0] / d0 >= 0.5) {
+      st.stop_reason = 2;
+      break;
+    }
+    d0 = nrm[0];
+  }
+  vec_.sol_out(P.perm.as<int64_t>(), ADp, x, d_x, s);
+  vec_.backward_terms(Kp, Kj, num_.Korig.as<double>(), x, ADp, bp_.as<double>(), s);
+  double be[4];
+  vec_.read_inf(be, 4, 4, s);
+  const double den   = be[1] * be[2] + be[3];
+  st.backward_error  = den > 0 ? be[0] / den : be[0];
+  st.residual_norm   = be[3] > 0 ? be[0] / be[3] : be[0];  // |b - A x| / |b|
+  MPIR_CUDA(cudaEventRecord(ev1_, s));
+  MPIR_CUDA(cudaEventSynchronize(ev1_));
+  float ms = 0;
+  MPIR_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
+  st.solve_ms  = ms;
+  st.factor_ms = last_factor_ms;
+  int32_t wait_err = 0;
+  MPIR_CUDA(cudaMemcpy(&wait_err, ws_.err.as<void>(), sizeof wait_err, cudaMemcpyDeviceToHost));
+  if (wait_err != 0) {
+    MPIR_CUDA(cudaMemset(ws_.err.as<void>(), 0, sizeof wait_err));
+    st.status = -5;
+    if (rep) *rep = st;
+    return -5;
+  }
+  if (rep) *rep = st;
+  return kOk;
+}
+
+int Solver::luir(const double *b, double *x, int maxiter, Report *rep) {
+  if (!plan_) throw std::logic_error("solve before analyze");
+  MPIR_CUDA(cudaSetDevice(device));
+  ensure_vectors();
+  const int64_t n = plan_->S.n;
+  MPIR_CUDA(cudaMemcpyAsync(hb_.as<void>(), b, n * sizeof(double), cudaMemcpyHostToDevice,
+                            stream_));
+  const int rc = luir_device(hb_.as<double>(), hx_.as<double>(), maxiter, rep);
+  MPIR_CUDA(cudaMemcpyAsync(x, hx_.as<void>(), n * sizeof(double), cudaMemcpyDeviceToHost,
+                            stream_));
+  MPIR_CUDA(cudaStreamSynchronize(stream_));
+  return rc;
+}
+
 int Solver::solve(const double *b, double *x, Report *rep) {
   if (!plan_) throw std::logic_error("solve before analyze");
   MPIR_CUDA(cudaSetDevice(device));

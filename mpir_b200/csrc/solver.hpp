@@ -47,6 +47,10 @@ class Solver {
   // Device entry points (caller arrays already on this device).
   int factor_device(const double *d_Ax);
   int solve_device(const double *d_b, double *d_x, Report *rep);
+  // Plain iterative refinement with the factor (LUIR_QDLDL); host and
+  // device vectors.
+  int luir(const double *b, double *x, int maxiter, Report *rep);
+  int luir_device(const double *d_b, double *d_x, int maxiter, Report *rep);
 
   void set_stream(cudaStream_t s) { stream_ = s ? s : own_stream_; }
   cudaStream_t stream() const { return stream_; }

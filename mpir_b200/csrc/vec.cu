@@ -9,6 +9,9 @@
 #include <cfloat>
 #include <cmath>
 
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
 #include "common.cuh"
 #include "vec.hpp"
 
@@ -275,18 +278,32 @@ __global__ void k_combine(int64_t n, const double *V, int64_t ldv, int k,
 // d *= scale; inf[0] = max|d|; inf[1] = max|x_old|; x += d
 // (gmres_ir.hpp:574-577).
 __global__ void k_ir_update(int64_t n, double *d, double scale, double *x,
-                            unsigned long long *inf) {
+                            const double *w, unsigned long long *inf) {
   const int64_t i   = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const bool    act = i < n;
-  double        di = 0.0, xi = 0.0;
+  double        di = 0.0, xi = 0.0, wi = 1.0;
   if (act) {
     di   = d[i] * scale;
     xi   = x[i];
     d[i] = di;
     x[i] = xi + di;
+    if (w) wi = w[i];
   }
-  warp_max_abs(inf + 0, di, act);
-  warp_max_abs(inf + 1, xi, act);
+  warp_max_abs(inf + 0, di * wi, act);
+  warp_max_abs(inf + 1, xi * wi, act);
+}
+
+// x <- x rounded to float32 (1), bfloat16 (2) or float16 (3).
+__global__ void k_round_to(int64_t n, int prec, double *x) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double v = x[i];
+  if (prec == 1)
+    x[i] = static_cast<double>(__double2float_rn(v));
+  else if (prec == 2)
+    x[i] = static_cast<double>(__bfloat162float(__double2bfloat16(v)));
+  else if (prec == 3)
+    x[i] = static_cast<double>(__half2float(__double2half(v)));
 }
 
 // bs[i] = b[perm[i]] * AD[perm[i]]; ADp[i] = AD[perm[i]]; bp[i] = b[perm[i]];
@@ -372,10 +389,15 @@ void VecOps::combine(const double *V, int64_t ldv, int k, const double *y, doubl
   launch(k_combine, blocks_for(n, 256), 256, 0, s, n, V, ldv, k, y, res);
 }
 
-void VecOps::ir_update(double *d, double scale, double *x, cudaStream_t s) {
+void VecOps::ir_update(double *d, double scale, double *x, cudaStream_t s, const double *w) {
   unsigned long long *inf = infbits.as<unsigned long long>() + 1;
   MPIR_CUDA(cudaMemsetAsync(inf, 0, 2 * sizeof(unsigned long long), s));
-  launch(k_ir_update, blocks_for(n, 256), 256, 0, s, n, d, scale, x, inf);
+  launch(k_ir_update, blocks_for(n, 256), 256, 0, s, n, d, scale, x, w, inf);
+}
+
+void VecOps::round_to(int prec, double *x, cudaStream_t s) {
+  if (prec < 1 || prec > 3) return;
+  launch(k_round_to, blocks_for(n, 256), 256, 0, s, n, prec, x);
 }
 
 void VecOps::rhs_in(const int64_t *perm, const double *AD, const double *b, double *bs,

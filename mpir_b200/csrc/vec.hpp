@@ -29,7 +29,13 @@ class VecOps {
   void scale(const double *x, double a, double *y, cudaStream_t s);
   void combine(const double *V, int64_t ldv, int k, const double *y, double *res,
                cudaStream_t s);
-  void ir_update(double *d, double scale, double *x, cudaStream_t s);
+  // d *= scale, x += d; infinity norms of d and of the old x (each entry
+  // times w[i] when w is given: the norms of the unscaled vectors).
+  void ir_update(double *d, double scale, double *x, cudaStream_t s,
+                 const double *w = nullptr);
+  // x <- x rounded to the factor's storage type (1 float32, 2 bfloat16,
+  // 3 float16; float64 leaves x unchanged).
+  void round_to(int prec, double *x, cudaStream_t s);
   void rhs_in(const int64_t *perm, const double *AD, const double *b, double *bs,
               double *ADp, double *bp, cudaStream_t s);
   void sol_out(const int64_t *perm, const double *ADp, const double *x, double *out,

@@ -165,6 +165,18 @@ class Oracle(_Common):
         self.lib.oracle_scale(n, _i(Ap), _i(Ai), _d(Ax), eps_uf, AD, Axs)
         return AD, Axs
 
+    def luir(self, n, Ap, Ai, Ax, b, maxiter=10):
+        """LUIR_QDLDL<float,double,double,double> restated: returns (x, info)
+        with info = {steps, relres, nnzL}."""
+        L = self.lib
+        L.oracle_luir_f32.restype = C.c_int
+        L.oracle_luir_f32.argtypes = [_i64, _i64p, _i64p, _f64p, _f64p, _f64p, C.c_int, _f64p]
+        x = np.zeros(n, np.float64)
+        info = np.zeros(3, np.float64)
+        if L.oracle_luir_f32(n, _i(Ap), _i(Ai), _d(Ax), _d(b), x, int(maxiter), info) != 0:
+            raise RuntimeError("oracle luir failed")
+        return x, dict(zip(("steps", "relres", "nnzL"), info.tolist()))
+
     def gmres_ir(self, n, Ap, Ai, Ax, b, uf=np.float32, form=0, ir_iter=10,
                  gmres_iter=10, tol=1e-10):
         """Full GMRES-IR: scaling, QDLDL factor in ``uf``, then Solve.
@@ -291,6 +303,18 @@ class Reference(_Common):
         c = np.zeros(a.size, np.float64)
         self.lib.ref_vector_op(op, a.size, a, b, c)
         return c
+
+    def luir(self, n, Ap, Ai, Ax, b, maxiter=10):
+        """The reference's LUIR_QDLDL<float,double,double,double>: returns
+        (x, info) with info = {steps, relres, nnzL}."""
+        L = self.lib
+        L.ref_luir_qdldl_f32.restype = C.c_int
+        L.ref_luir_qdldl_f32.argtypes = [_i64, _i64p, _i64p, _f64p, _f64p, _f64p, C.c_int,
+                                         _f64p]
+        x = np.zeros(n, np.float64)
+        info = np.zeros(3, np.float64)
+        L.ref_luir_qdldl_f32(n, _i(Ap), _i(Ai), _d(Ax), _d(b), x, int(maxiter), info)
+        return x, dict(zip(("steps", "relres", "nnzL"), info.tolist()))
 
     def gmres_ir(self, n, Ap, Ai, Ax, b, uf=np.float32, ir_iter=10, gmres_iter=10, tol=1e-10):
         """GmresLDLIR<UF,double,double>::Solve preconditioned by QDLDL<UF>.

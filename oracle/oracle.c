@@ -464,3 +464,92 @@ int oracle_gmres_ir(oi n, const oi *Ap, const oi *Ai, const double *Axs,
   free(g.Ux);
   return 0;
 }
+
+/* ------------------------------------------------------------------------
+ * LUIR_QDLDL<float, double, double, double> (qdldl-luir/luir.hpp:33-241):
+ * QDLDL factor of A in float (natural order), then plain iterative
+ * refinement.  The residual (qdldl-luir/residual.hpp:15-41: the same loop as
+ * MatrixMultiply, in double) is stored in float, scaled by 1/|r|, solved in
+ * float and scaled back; x += d in double; stop when |d|/|x| <= 10 eps(double)
+ * or |d|/|d_prev| >= 0.5.  info = {steps, |b - A x|/|b| (residual stored in
+ * float, as the reference), nnz(L)}.  Returns -1 on a structural error or
+ * zero pivot. */
+static double inf_norm_f(oi n, const float *x) {
+  float m = 0.0f;
+  for (oi i = 0; i < n; i++) {
+    const float a = x[i] >= 0 ? x[i] : -x[i];
+    if (a > m) m = a;
+  }
+  return (double)m;
+}
+
+static double inf_norm_d(oi n, const double *x) {
+  double m = 0.0;
+  for (oi i = 0; i < n; i++) {
+    const double a = x[i] >= 0 ? x[i] : -x[i];
+    if (a > m) m = a;
+  }
+  return m;
+}
+
+/* residual (float) = b - A x, accumulated in double */
+static void residual_f(oi n, const oi *Ap, const oi *Ai, const double *Ax,
+                       const double *x, const double *b, double *work, float *res) {
+  oracle_matmul(n, Ap, Ai, Ax, x, work);
+  for (oi i = 0; i < n; i++) res[i] = (float)(b[i] - work[i]);
+}
+
+int oracle_luir_f32(oi n, const oi *Ap, const oi *Ai, const double *Ax,
+                    const double *b, double *x, int maxiter, double *info) {
+  oi *iwork = malloc(sizeof(oi) * 3 * (size_t)(n > 0 ? n : 1));
+  oi *Lnz = malloc(sizeof(oi) * (size_t)(n > 0 ? n : 1));
+  oi *et = malloc(sizeof(oi) * (size_t)(n > 0 ? n : 1));
+  const oi sum = oracle_etree(n, Ap, Ai, iwork, Lnz, et);
+  if (sum < 0) {
+    free(iwork); free(Lnz); free(et);
+    return -1;
+  }
+  oi    *Lp = malloc(sizeof(oi) * (size_t)(n + 1));
+  oi    *Li = malloc(sizeof(oi) * (size_t)(sum > 0 ? sum : 1));
+  float *Lx = malloc(sizeof(float) * (size_t)(sum > 0 ? sum : 1));
+  float *D = malloc(sizeof(float) * (size_t)(n > 0 ? n : 1));
+  float *Dinv = malloc(sizeof(float) * (size_t)(n > 0 ? n : 1));
+  const oi pos = oracle_factor_f32(n, Ap, Ai, Ax, Lp, Li, Lx, D, Dinv, Lnz, et);
+  float  *cf = malloc(sizeof(float) * (size_t)(n > 0 ? n : 1));
+  double *work = malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+  int     steps = 0, rc = pos < 0 ? -1 : 0;
+  if (rc == 0) {
+    if (maxiter == 0) {
+      /* luir.hpp:171-179: one solve with x in double */
+      for (oi i = 0; i < n; i++) x[i] = b[i];
+      oracle_solve_f32_f64(n, Lp, Li, Lx, Dinv, x);
+    } else {
+      /* luir.hpp:182-232 */
+      for (oi i = 0; i < n; i++) cf[i] = (float)b[i];
+      oracle_solve_f32_f32(n, Lp, Li, Lx, Dinv, cf);
+      for (oi i = 0; i < n; i++) x[i] = (double)cf[i];
+      const double eps = 2.220446049250313e-16, thresh = 0.5;
+      double       d0 = 1.7976931348623157e308;
+      for (int it = 1; it <= maxiter; it++) {
+        residual_f(n, Ap, Ai, Ax, x, b, work, cf);
+        const double nc = inf_norm_f(n, cf);
+        for (oi i = 0; i < n; i++) cf[i] *= 1. / nc;
+        oracle_solve_f32_f32(n, Lp, Li, Lx, Dinv, cf);
+        for (oi i = 0; i < n; i++) cf[i] *= nc;
+        const double dn = inf_norm_f(n, cf), xn = inf_norm_d(n, x);
+        const int    stop = dn / xn <= 10 * eps || dn / d0 >= thresh;
+        steps = it;
+        for (oi i = 0; i < n; i++) x[i] = (double)cf[i] + x[i];
+        if (stop) break;
+        d0 = dn;
+      }
+    }
+    residual_f(n, Ap, Ai, Ax, x, b, work, cf);
+    info[1] = inf_norm_f(n, cf) / inf_norm_d(n, b);
+  }
+  info[0] = steps;
+  info[2] = (double)sum;
+  free(iwork); free(Lnz); free(et); free(Lp); free(Li); free(Lx); free(D); free(Dinv);
+  free(cf); free(work);
+  return rc;
+}

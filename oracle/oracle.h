@@ -56,4 +56,8 @@ int oracle_gmres_ir(oi n, const oi *Ap, const oi *Ai, const double *Axs,
                     int form, int uf32, const double *b, double *x,
                     oi ir_iter, oi gmres_iter, double tol, double *stats);
 
+/* qdldl-luir/luir.hpp:33-241, FACTPREC = float */
+int oracle_luir_f32(oi n, const oi *Ap, const oi *Ai, const double *Ax,
+                    const double *b, double *x, int maxiter, double *info);
+
 #endif

@@ -6,7 +6,9 @@
 //   include/MPIR/qdldl.hpp      QDLDL_etree / QDLDL_factor / QDLDL_solve
 //   include/MPIR/ops.hpp        MatrixMultiply, Dnrm2, InfNrm, VectorDot
 //   include/MPIR/gmres_ir.hpp   GmresLDLIR<UF,UW,UR>::Compute / Solve
-// of the reference tree, with oracle/shim/print standing in for <print>.
+//   include/qdldl-luir/luir.hpp LUIR_QDLDL (plain iterative refinement)
+// of the reference tree, with oracle/shim/print standing in for <print> and
+// oracle/shim/qd/ for the QD library's headers (not installed).
 //
 // GmresLDLIR keeps its factor in private members and its shipped Compute
 // builds an FGPILU factor (gmres_ir.hpp:365-531).  The harness runs Compute
@@ -33,6 +35,7 @@
 #include "MPIR/gmres_ir.hpp"
 #include "MPIR/ops.hpp"
 #include "MPIR/qdldl.hpp"
+#include "qdldl-luir/luir.hpp"
 
 using I = int64_t;
 
@@ -332,5 +335,19 @@ int ref_gmres_ir_f64(I n, const I *Ap, const I *Ai, const double *Ax,
                      double tol, double *AD_out, double *info) {
   return gmres_ir<S64>(n, Ap, Ai, Ax, b, x, ir_iter, gmres_iter, tol, AD_out,
                        info);
+}
+}  // extern "C"
+
+extern "C" {
+// LUIR_QDLDL<float, double, double, double> on A (upper CSC, natural order).
+// info = {num_refinement_steps_, relative_residual_, Lnz_}.
+int ref_luir_qdldl_f32(I n, const I *Ap, const I *Ai, const double *Ax, const double *b,
+                       double *x, int maxiter, double *info) {
+  Stats st;
+  LUIR_QDLDL<float, double, double, double, I>(n, Ap, Ai, Ax, b, x, &st, maxiter);
+  info[0] = st.num_refinement_steps_;
+  info[1] = st.relative_residual_;
+  info[2] = static_cast<double>(st.Lnz_);
+  return 0;
 }
 }  // extern "C"

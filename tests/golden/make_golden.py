@@ -10,6 +10,9 @@ its outputs:
   small2d_gmres.npz     GmresLDLIR<float,double,double>::Solve preconditioned
                         by the QDLDL factor: x, AD, refinement steps
   small2d_solve.npz     QDLDL_solve<float,double> of b with that factor
+  small2d_luir.npz      LUIR_QDLDL<float,double,double,double> (plain
+                        iterative refinement, at most 10 steps): x, steps,
+                        relative residual
 
 Usage: python tests/golden/make_golden.py   (needs oracle/_ref built)
 """
@@ -44,6 +47,9 @@ def main():
     xg, AD, info = R.gmres_ir(s.n, s.Ap, s.Ai, s.Ax, s.b)
     np.savez_compressed(os.path.join(HERE, "small2d_gmres.npz"), x=xg, AD=AD,
                         ir_steps=info["ir_steps"], npos=info["npos"])
+    xl, li = R.luir(s.n, s.Ap, s.Ai, s.Ax, s.b, 10)
+    np.savez_compressed(os.path.join(HERE, "small2d_luir.npz"), x=xl, steps=li["steps"],
+                        relres=li["relres"])
     print("wrote fixtures to", HERE)
 
 

@@ -41,3 +41,16 @@ def test_cpp_dropin_headers_compile(tmp_path):
     r = subprocess.run(["g++", "-std=c++20", "-fsyntax-only", f"-I{ROOT}/include", str(src)],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_cpp_luir_header_compiles(tmp_path):
+    src = tmp_path / "l.cpp"
+    src.write_text(
+        '#include "qdldl-luir/luir.hpp"\n'
+        "int main() { Stats st; long n = 1; long Ap[2] = {0, 1}; long Ai[1] = {0};\n"
+        "  double Ax[1] = {2.0}, b[1] = {1.0}, x[1];\n"
+        "  if (false) LUIR_QDLDL<float, double, double, double>(n, Ap, Ai, Ax, b, x, &st, 10);\n"
+        "  return st.get_num_refinement_steps(); }\n")
+    r = subprocess.run(["g++", "-std=c++23", "-fsyntax-only", f"-I{ROOT}/include", str(src)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr

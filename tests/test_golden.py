@@ -49,3 +49,14 @@ def test_generator_is_stable():
     assert sha(s.Ai) == sha(kkt.small2d().Ai)
     g = np.load(os.path.join(GOLD, "small2d_natural.npz"))
     assert int(g["sumLnz"]) == 271978
+
+
+def test_oracle_matches_golden_luir(oracle_lib):
+    """LUIR_QDLDL restated: the reference's x, step count and relative
+    residual, bit for bit."""
+    g = np.load(os.path.join(GOLD, "small2d_luir.npz"))
+    s = kkt.small2d()
+    x, info = oracle_lib.luir(s.n, s.Ap, s.Ai, s.Ax, s.b, 10)
+    np.testing.assert_array_equal(x, g["x"])
+    assert info["steps"] == float(g["steps"])
+    assert info["relres"] == float(g["relres"])

@@ -181,6 +181,57 @@ def test_tiny_systems():
         np.testing.assert_allclose(x, 1.0 / Ax, rtol=1e-15)
 
 
+# ---------------------------------------------------------------- several right-hand sides
+def test_same_pattern_batch_many_rhs():
+    """The same-pattern batch (several instances sharing Ap/Ai, each with
+    several right-hand sides): one analysis, a refactorization per instance,
+    SolveMany per instance; every column at backward error <= 1e-14 and equal
+    to the single-right-hand-side solve of that column."""
+    batch = kkt.batch2d(instances=3, grid=24, nrhs=4, seed=6)
+    solver = mp.GmresLDLIR()
+    solver.analyze(batch[0].Ap, batch[0].Ai, batch[0].Ax)
+    for s in batch:
+        assert solver.factor(s.Ax) == 0
+        X = solver.SolveMany(s.b)
+        assert X.shape == s.b.shape
+        for k in range(s.b.shape[0]):
+            assert kkt.backward_error(s.n, s.Ap, s.Ai, s.Ax, X[k], s.b[k]) <= 1e-14
+        np.testing.assert_array_equal(X[1], solver.Solve(s.b[1]))
+        assert len(solver.last_reports) == s.b.shape[0]
+
+
+# ---------------------------------------------------------------- plain IR
+@pytest.mark.parametrize("name,s", list(small_systems())[:3])
+def test_luir_matches_reference(ref_lib, name, s):
+    """LUIR_QDLDL on the GPU against the reference's LUIR_QDLDL on the same
+    system: both refine to a relative residual at float64 rounding level; the
+    GPU factor (permuted, scaled, different summation order) may take one
+    refinement step more or less; solutions agree to the reference's forward
+    error."""
+    x, st = mp.LUIR_QDLDL(s.n, s.Ap, s.Ai, s.Ax, s.b, fact_prec="f32", maxiter=10)
+    xr, ir = ref_lib.luir(s.n, s.Ap, s.Ai, s.Ax, s.b, 10)
+    rel = kkt.backward_error(s.n, s.Ap, s.Ai, s.Ax, x, s.b)
+    assert st["relative_residual_"] <= max(10 * ir["relres"], 1e-14), (st, ir)
+    assert rel <= 1e-14
+    assert abs(st["num_refinement_steps_"] - ir["steps"]) <= 1, (st, ir)
+    fe_gpu, fe_ref = kkt.forward_error(x, s.x_true), kkt.forward_error(xr, s.x_true)
+    assert fe_gpu <= max(10 * fe_ref, 1e-12), (fe_gpu, fe_ref)
+
+
+def test_luir_single_solve_and_solver_handle():
+    """maxiter = 0 is one solve (no refinement step); the solver handle's
+    luir() refines with the factor it holds."""
+    s = kkt.small2d()
+    x0, st0 = mp.LUIR_QDLDL(s.n, s.Ap, s.Ai, s.Ax, s.b, maxiter=0)
+    assert st0["num_refinement_steps_"] == 0
+    assert st0["relative_residual_"] < 1e-4
+    solver = mp.GmresLDLIR()
+    solver.Compute(s.Ap, s.Ai, s.Ax)
+    x = solver.luir(s.b, maxiter=10)
+    assert solver.last_report["ir_iterations"] >= 1
+    assert kkt.backward_error(s.n, s.Ap, s.Ai, s.Ax, x, s.b) <= 1e-14
+
+
 # ---------------------------------------------------------------- tensor cores
 @pytest.fixture
 def update_engine(monkeypatch):

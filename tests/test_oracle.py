@@ -119,3 +119,15 @@ def test_oracle_error_codes(oracle_lib, ref_lib):
     Ax = np.array([1.0, 1.0, 1.0])
     for L in (oracle_lib, ref_lib):
         assert L.factor(2, Ap, Ai, Ax, np.float64)[0] == -1
+
+
+@pytest.mark.parametrize("maxiter", [0, 1, 10])
+def test_oracle_luir_bitexact(oracle_lib, ref_lib, maxiter):
+    """LUIR_QDLDL<float,double,double,double> (qdldl-luir/luir.hpp): the
+    restatement equals the compiled reference bit for bit, including the
+    stop test's step count."""
+    for s in (kkt.small2d(), kkt.grid3d(grid=6, seed=3)):
+        xo, io = oracle_lib.luir(s.n, s.Ap, s.Ai, s.Ax, s.b, maxiter)
+        xr, ir = ref_lib.luir(s.n, s.Ap, s.Ai, s.Ax, s.b, maxiter)
+        np.testing.assert_array_equal(xo, xr)
+        assert io == ir
