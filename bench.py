@@ -306,6 +306,27 @@ def reference_counts(grid, seed):
 
 # ----------------------------------------------------------------------------
 
+def rank_max(pg, v, device):
+    """Max of v over the ranks of process group module pg (None: one rank)."""
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(world, steps, max_ms):
+    """Whole-job solves/s: every rank solves `steps` systems of its own; the
+    job takes the slowest rank's time."""
+    return world * steps / (max_ms / 1e3)
+
+
+def replica_seed(seed, rank):
+    """Each rank (replica) solves its own seeded system."""
+    return seed + rank
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -376,13 +397,9 @@ def run_gpu(args):
             pg.barrier()
 
     def max_over_ranks(v):
-        if pg is None:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        return float(t.item())
+        return rank_max(pg, v, dev)
 
-    s = kkt.grid3d(seed=args.seed + rank, grid=args.grid)
+    s = kkt.grid3d(seed=replica_seed(args.seed, rank), grid=args.grid)
     solver = mp.GmresLDLIR(uf=args.uf, device=local)
     low = args.uf != "f32"
     solver.SetMaxGmresIterations(args.gmres_iter or (50 if low else 10))
@@ -427,7 +444,7 @@ def run_gpu(args):
     barrier()
     lat = [a.elapsed_time(b) for a, b in evs]
     total_ms = max_over_ranks(t_all0.elapsed_time(t_all1))
-    value = world * args.steps / (total_ms / 1e3)
+    value = aggregate_rate(world, args.steps, total_ms)
     be = max(r["backward_error"] for r in reps)
     assert be <= BE_TOL, f"backward error {be} above {BE_TOL}"
 
@@ -456,7 +473,7 @@ def run_gpu(args):
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1))
     assert be_e2e <= BE_TOL
-    e2e_value = world * args.steps / (e2e_ms / 1e3)
+    e2e_value = aggregate_rate(world, args.steps, e2e_ms)
     h2d = s.Ax.nbytes + s.b.nbytes
     d2h = s.n * 8
 
