@@ -17,6 +17,9 @@
 //    double-double type (mpir::double_double, or the QD library's dd_real
 //    with MPIR_USE_QD).  Other combinations throw from Compute.
 //  * LastReport() gives the iteration counts and the backward error.
+//  * DumpLogText() returns the solver log as JSON text (the schema of the
+//    reference's DumpLog, gmres_ir.hpp:305-313); with VERBOSE defined and
+//    nlohmann/json available, DumpLog() returns it parsed, as the reference.
 #pragma once
 #ifndef MPIR_B200_GMRES_IR_HPP
 #define MPIR_B200_GMRES_IR_HPP
@@ -28,6 +31,11 @@
 #include <string>
 #include <type_traits>
 #include <vector>
+
+#if defined(VERBOSE) && __has_include(<nlohmann/json.hpp>)
+#include <nlohmann/json.hpp>
+#define MPIR_DROPIN_HAS_JSON 1
+#endif
 
 #include "../mpir_b200.h"
 #include "fp_concepts.hpp"
@@ -120,6 +128,20 @@ class GmresLDLIR {
   }
 
   const mpir_report &LastReport() const { return last_; }
+
+  // The log of the solves since the previous call, as JSON text; clears it.
+  std::string DumpLogText() {
+    if (!h_) return "{}";
+    int64_t len = 0;
+    check(mpir_solver_dump_log(h_, nullptr, 0, &len), "DumpLog");
+    std::string out(static_cast<size_t>(len), '\0');
+    check(mpir_solver_dump_log(h_, out.data(), len, &len), "DumpLog");
+    out.resize(static_cast<size_t>(len > 0 ? len - 1 : 0));
+    return out;
+  }
+#ifdef MPIR_DROPIN_HAS_JSON
+  nlohmann::json DumpLog() { return nlohmann::json::parse(DumpLogText()); }
+#endif
 };
 
 #endif

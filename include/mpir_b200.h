@@ -183,6 +183,17 @@ int mpir_solver_solve(mpir_solver s, const double *b, double *x,
 int mpir_solver_solve_device(mpir_solver s, const double *d_b, double *d_x,
                              mpir_report *rep);
 
+/* The solver's log of the GMRES-IR solves since the previous dump, as JSON
+ * text with the schema of the reference's GmresLDLIR::DumpLog under VERBOSE
+ * (gmres_ir.hpp:305-313; one "gmres_ir" event per solve with
+ * initial_residual, per refinement step {iteration, residual, d_norm,
+ * timestamp_ms, inner_time_ms}, stop_reason, stop_reason_detail,
+ * total_iterations, total_time_ms; then max_outer_iterations,
+ * max_inner_iterations, tolerance).  *len receives the size including the
+ * terminating NUL; when buf is NULL or cap < *len nothing is copied (call
+ * again with a large enough buffer); a completed copy clears the log. */
+int mpir_solver_dump_log(mpir_solver s, char *buf, int64_t cap, int64_t *len);
+
 /* nrhs right-hand sides with the current factor: B and X hold nrhs
  * contiguous vectors of length n (column-major n x nrhs, host memory); one
  * GMRES-IR solve per column, each exactly as mpir_solver_solve; reps (NULL,

@@ -100,6 +100,7 @@ def lib():
         "mpir_solver_solve_device": (i32, [vp, vp, vp, vp]),
         "mpir_solver_set_stream": (i32, [vp, vp]),
         "mpir_solver_solve_many": (i32, [vp, i64, vp, vp, vp]),
+        "mpir_solver_dump_log": (i32, [vp, vp, i64, vp]),
         "mpir_solver_luir": (i32, [vp, vp, vp, i32, vp]),
         "mpir_solver_luir_device": (i32, [vp, vp, vp, i32, vp]),
         "mpir_luir_qdldl": (i32, [i64, vp, vp, vp, vp, vp, i32, i32, vp, i32]),
@@ -301,6 +302,16 @@ class GmresLDLIR:
         _check(lib().mpir_solver_solve(self._h, _p(b), _p(x), C.byref(rep)))
         self.last_report = rep.as_dict()
         return x
+
+    def DumpLog(self):
+        """The log of the solves since the last call (the reference's
+        GmresLDLIR::DumpLog schema under VERBOSE) as a dict; clears it."""
+        import json
+        n = C.c_int64(0)
+        _check(lib().mpir_solver_dump_log(self._h, None, 0, C.byref(n)))
+        buf = C.create_string_buffer(n.value)
+        _check(lib().mpir_solver_dump_log(self._h, buf, n.value, C.byref(n)))
+        return json.loads(buf.value.decode())
 
     def SolveMany(self, B):
         """B: (nrhs, n) right-hand sides (one per row); returns X of the

@@ -176,7 +176,8 @@ void invert_diag_blocks(const Plan &P, Numeric &F, cudaStream_t s);
 using namespace mpir;
 
 struct mpir_solver_s {
-  Solver *impl;
+  Solver     *impl;
+  std::string pending_log;  // rendered log awaiting mpir_solver_dump_log's copy
 };
 
 extern "C" {
@@ -358,7 +359,7 @@ int mpir_solver_create(mpir_solver *out, int uf, int uw, int ur, int device) {
     if ((uf != kF32 && uf != kBF16 && uf != kF16) || uw != kF64 || (ur != kF64 && ur != kDD))
       throw StatusError(MPIR_ERR_UNSUPPORTED,
                         "provided precisions: UF=F32/BF16/F16, UW=F64, UR=F64 or DD");
-    auto *h = new mpir_solver_s{nullptr};
+    auto *h = new mpir_solver_s{nullptr, {}};
     try {
       h->impl = new Solver(uf, uw, ur, device);
     } catch (...) {
@@ -477,6 +478,19 @@ int mpir_solver_solve_many(mpir_solver s, int64_t nrhs, const double *B, double 
                                     reps ? reinterpret_cast<Report *>(reps + k) : nullptr);
       if (rc != MPIR_OK) return rc;
     }
+    return MPIR_OK;
+  });
+}
+
+int mpir_solver_dump_log(mpir_solver s, char *buf, int64_t cap, int64_t *len) {
+  MPIR_NEED(s);
+  return guard([&]() -> int {
+    if (!len) throw StatusError(MPIR_ERR_ARGUMENT, "len is NULL");
+    if (s->pending_log.empty()) s->pending_log = s->impl->dump_log();
+    *len = static_cast<int64_t>(s->pending_log.size()) + 1;
+    if (!buf || cap < *len) return MPIR_OK;
+    std::memcpy(buf, s->pending_log.c_str(), static_cast<size_t>(*len));
+    s->pending_log.clear();
     return MPIR_OK;
   });
 }

@@ -4,6 +4,8 @@
 // permuted order; the host keeps the small Hessenberg least-squares problem
 // and its Givens rotations, reading back one column of H per inner step.
 #include <cfloat>
+#include <chrono>
+#include <cstdio>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -271,11 +273,18 @@ int Solver::solve_device(const double *d_b, double *d_x, Report *rep) {
               bp_.as<double>(), s);
   double bs_inf;
   vec_.read_inf(&bs_inf, 3, 1, s);
+  const auto t_outer = std::chrono::steady_clock::now();
+  auto       ms_since = [](std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
+        .count();
+  };
   precond_gmres(bs, x, st);
   vec_.residual(Kp, Kj, Kv, x, bs, r, dd, 0, s);
   st.spmv_count++;
   double r_inf;
   vec_.read_inf(&r_inf, 0, 1, s);
+  IrEvent ev;
+  ev.initial_residual = r_inf;
   double r_prev = DBL_MAX, r_norm = r_inf / bs_inf;
   const double eps_w = eps_of(uw);
   for (int64_t iter = 1; iter <= ir_iter; iter++) {
@@ -289,15 +298,18 @@ int Solver::solve_device(const double *d_b, double *d_x, Report *rep) {
       break;
     }
     vec_.scale(r, 1.0 / scale, t, s);
+    const auto t_inner = std::chrono::steady_clock::now();
     precond_gmres(t, d, st);
     vec_.ir_update(d, scale, x, s);
     double nrm[2];
     vec_.read_inf(nrm, 1, 2, s);
+    const double inner_ms = ms_since(t_inner);
     vec_.residual(Kp, Kj, Kv, x, bs, r, dd, 0, s);
     st.spmv_count++;
     vec_.read_inf(&r_inf, 0, 1, s);
     r_norm           = r_inf / bs_inf;
     st.ir_iterations = static_cast<int32_t>(iter);
+    ev.iterations.push_back({iter, r_norm, nrm[0], ms_since(t_outer), inner_ms});
     if (nrm[0] <= nrm[1] * (10 * eps_w)) {
       st.stop_reason = 1;
       break;
@@ -309,6 +321,10 @@ int Solver::solve_device(const double *d_b, double *d_x, Report *rep) {
     r_prev = r_norm;
   }
   st.residual_norm = r_norm;
+  ev.stop_reason      = st.stop_reason;
+  ev.total_iterations = st.ir_iterations;
+  ev.total_time_ms    = ms_since(t_outer);
+  log_.push_back(std::move(ev));
   vec_.sol_out(P.perm.as<int64_t>(), ADp_.as<double>(), x, d_x, s);
   vec_.backward_terms(Kp, Kj, num_.Korig.as<double>(), x, ADp_.as<double>(),
                       bp_.as<double>(), s);
@@ -440,6 +456,47 @@ int Solver::luir(const double *b, double *x, int maxiter, Report *rep) {
                             stream_));
   MPIR_CUDA(cudaStreamSynchronize(stream_));
   return rc;
+}
+
+// The solver log as JSON, the schema of GmresLDLIR::DumpLog
+// (gmres_ir.hpp:305-313, events of gmres_ir.hpp:539-632); clears the events.
+std::string Solver::dump_log() {
+  static const char *reasons[] = {"max_iterations_reached", "converged_small_update",
+                                  "converged_residual_stagnation", "exact_residual",
+                                  "non_finite_residual"};
+  static const char *details[] = {"", "d_norm <= x_norm * (10*eps)",
+                                  "abs(r_norm - r_norm_prev) < tol", "r == 0",
+                                  "r is not finite"};
+  auto num = [](double v) {
+    if (!std::isfinite(v)) return std::string("null");
+    char b[64];
+    std::snprintf(b, sizeof b, "%.17g", v);
+    return std::string(b);
+  };
+  std::string j = "{\"events\":[";
+  for (size_t e = 0; e < log_.size(); e++) {
+    const IrEvent &ev = log_[e];
+    const int      rs = ev.stop_reason >= 0 && ev.stop_reason <= 4 ? ev.stop_reason : 0;
+    j += e ? "," : "";
+    j += "{\"name\":\"gmres_ir\",\"initial_residual\":" + num(ev.initial_residual) +
+         ",\"iterations\":[";
+    for (size_t i = 0; i < ev.iterations.size(); i++) {
+      const IrIter &it = ev.iterations[i];
+      j += i ? "," : "";
+      j += "{\"iteration\":" + std::to_string(it.iteration) + ",\"residual\":" +
+           num(it.residual) + ",\"d_norm\":" + num(it.d_norm) + ",\"timestamp_ms\":" +
+           num(it.timestamp_ms) + ",\"inner_time_ms\":" + num(it.inner_time_ms) + "}";
+    }
+    j += "],\"stop_reason\":\"" + std::string(reasons[rs]) + "\"";
+    if (rs != 0) j += ",\"stop_reason_detail\":\"" + std::string(details[rs]) + "\"";
+    j += ",\"total_iterations\":" + std::to_string(ev.total_iterations) +
+         ",\"total_time_ms\":" + num(ev.total_time_ms) + "}";
+  }
+  j += "],\"max_outer_iterations\":" + std::to_string(ir_iter) +
+       ",\"max_inner_iterations\":" + std::to_string(gmres_iter) +
+       ",\"tolerance\":" + num(tol) + "}";
+  log_.clear();
+  return j;
 }
 
 int Solver::solve(const double *b, double *x, Report *rep) {

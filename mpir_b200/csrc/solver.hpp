@@ -2,6 +2,8 @@
 // factor, the GMRES basis and the refinement vectors, all on one device.
 #pragma once
 #include <memory>
+#include <string>
+#include <vector>
 #include <stdexcept>
 
 #include "engine.hpp"
@@ -28,6 +30,20 @@ struct Report {
   double  solve_ms         = 0;
 };
 
+// One refinement step and one solve in the solver log (the fields of the
+// reference's VERBOSE log, gmres_ir.hpp:539-632).
+struct IrIter {
+  int64_t iteration;
+  double  residual, d_norm, timestamp_ms, inner_time_ms;
+};
+struct IrEvent {
+  double              initial_residual = 0;
+  std::vector<IrIter> iterations;
+  int                 stop_reason      = 0;
+  int64_t             total_iterations = 0;
+  double              total_time_ms    = 0;
+};
+
 class Solver {
  public:
   Solver(int uf, int uw, int ur, int device);
@@ -51,6 +67,8 @@ class Solver {
   // device vectors.
   int luir(const double *b, double *x, int maxiter, Report *rep);
   int luir_device(const double *d_b, double *d_x, int maxiter, Report *rep);
+  // The log of the solves since the last call, as JSON (GmresLDLIR::DumpLog).
+  std::string dump_log();
 
   void set_stream(cudaStream_t s) { stream_ = s ? s : own_stream_; }
   cudaStream_t stream() const { return stream_; }
@@ -76,6 +94,7 @@ class Solver {
   DeviceBuffer          V_, bs_, bp_, ADp_, x_, r_, t_, d_, hd_, y_, hb_, hx_;
   int64_t               vec_m_ = -1;
   cudaEvent_t           ev0_ = nullptr, ev1_ = nullptr;
+  std::vector<IrEvent>  log_;
 };
 
 double eps_of(int prec);

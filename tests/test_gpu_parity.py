@@ -200,6 +200,52 @@ def test_same_pattern_batch_many_rhs():
         assert len(solver.last_reports) == s.b.shape[0]
 
 
+# ---------------------------------------------------------------- log and driver
+def test_dump_log_schema():
+    """DumpLog: one gmres_ir event per solve with the reference's VERBOSE
+    fields (gmres_ir.hpp:539-632), then the settings; cleared by the dump."""
+    s = kkt.grid3d(grid=8, seed=2)
+    solver = mp.GmresLDLIR(ur="dd")
+    solver.SetTolerance(1e-15)
+    solver.Compute(s.Ap, s.Ai, s.Ax)
+    solver.Solve(s.b)
+    solver.Solve(2 * s.b)
+    log = solver.DumpLog()
+    assert len(log["events"]) == 2
+    assert log["max_outer_iterations"] == 10 and log["tolerance"] == 1e-15
+    ev = log["events"][0]
+    assert ev["name"] == "gmres_ir"
+    assert ev["total_iterations"] == len(ev["iterations"])
+    for it in ev["iterations"]:
+        assert set(it) == {"iteration", "residual", "d_norm", "timestamp_ms", "inner_time_ms"}
+    assert ev["stop_reason"] in ("max_iterations_reached", "converged_small_update",
+                                 "converged_residual_stagnation", "exact_residual")
+    assert solver.DumpLog()["events"] == []
+
+
+def test_example_driver_on_matrix_market_file(tmp_path, capsys):
+    """The example driver (examples/example.cpp) end to end on a Matrix
+    Market file: b = A ones solved to the reference driver's residual level,
+    and the JSON log written beside the matrix."""
+    from mpir_b200 import example
+    from mpir_b200.mmio import write_matrix_market
+    s = kkt.small2d()
+    p = tmp_path / "small2d.mtx"
+    write_matrix_market(p, s.n, s.Ap, s.Ai, s.Ax)
+    assert example.main([str(p), "--log"]) == 0
+    out = capsys.readouterr().out
+    assert out.splitlines()[0] == "symmetric"
+    logs = list(tmp_path.glob("small2d_*.json"))
+    assert len(logs) == 1
+    import json
+    log = json.loads(logs[0].read_text())
+    assert log["matrix"] == "small2d" and log["ilu_k"] == 0
+    assert log["residual_precision"] == "quadruple"
+    assert log["relative_residual"] <= 1e-14
+    assert log["relative_error"] <= 1e-10
+    assert len(log["events"]) == 1
+
+
 # ---------------------------------------------------------------- plain IR
 @pytest.mark.parametrize("name,s", list(small_systems())[:3])
 def test_luir_matches_reference(ref_lib, name, s):
