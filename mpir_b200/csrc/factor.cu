@@ -377,8 +377,10 @@ template <bool TRSM>
 __global__ void __launch_bounds__(kGemmThreads)
     k_step_gemm(const StepDesc *descs, int ndesc, float *panel, float *uarena,
                 const float *linv, const float *Dinv, float *pack) {
-  __shared__ float As[kBK][kBM];
-  __shared__ float Bs[kBK][kBN];
+  // Two slices in shared memory: slice s+1 is loaded into registers while
+  // slice s is multiplied, then stored into the other buffer.
+  __shared__ float As[2][kBK][kBM];
+  __shared__ float Bs[2][kBK][kBN];
   __shared__ float sd[kNB];
   const int        t  = blockIdx.x;
   int              lo = 0, hi = ndesc - 1;
@@ -443,9 +445,11 @@ __global__ void __launch_bounds__(kGemmThreads)
 #pragma unroll
     for (int j = 0; j < 8; j++) acc[i][j] = 0.0f;
   __syncthreads();
-  for (int k0 = 0; k0 < K; k0 += kBK) {
+  constexpr int kLoads = (kBM * kBK) / kGemmThreads;
+  float         ra[kLoads], rb[kLoads];
+  auto          load = [&](int k0) {
 #pragma unroll
-    for (int q = 0; q < (kBM * kBK) / kGemmThreads; q++) {
+    for (int q = 0; q < kLoads; q++) {
       const int idx = tid + q * kGemmThreads;
       const int i = idx % kBM, kk = idx / kBM;
       const int r = m0 + i, k = k0 + kk;
@@ -454,73 +458,95 @@ __global__ void __launch_bounds__(kGemmThreads)
         v = A[r + (int64_t)k * lda];
         if (!TRSM) v *= sd[k];
       }
-      As[kk][i] = v;
-      const int c  = n0 + i;
-      float     bv = 0.0f;
-      if (c < N && k < K) bv = B[c + (int64_t)k * ldb];
-      Bs[kk][i] = bv;
+      ra[q]       = v;
+      const int c = n0 + i;
+      rb[q]       = (c < N && k < K) ? B[c + (int64_t)k * ldb] : 0.0f;
     }
-    __syncthreads();
+  };
+  auto store = [&](int buf) {
+#pragma unroll
+    for (int q = 0; q < kLoads; q++) {
+      const int idx = tid + q * kGemmThreads;
+      As[buf][idx / kBM][idx % kBM] = ra[q];
+      Bs[buf][idx / kBM][idx % kBM] = rb[q];
+    }
+  };
+  load(0);
+  store(0);
+  __syncthreads();
+  int buf = 0;
+  for (int k0 = 0; k0 < K; k0 += kBK) {
+    if (k0 + kBK < K) load(k0 + kBK);  // in flight during this slice
 #pragma unroll
     for (int kk = 0; kk < kBK; kk++) {
       float a[8], b[8];
 #pragma unroll
-      for (int i = 0; i < 8; i++) a[i] = As[kk][tr * 8 + i];
+      for (int i = 0; i < 8; i++) a[i] = As[buf][kk][tr * 8 + i];
 #pragma unroll
-      for (int j = 0; j < 8; j++) b[j] = Bs[kk][tc * 8 + j];
+      for (int j = 0; j < 8; j++) b[j] = Bs[buf][kk][tc * 8 + j];
 #pragma unroll
       for (int i = 0; i < 8; i++)
 #pragma unroll
         for (int j = 0; j < 8; j++) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
     }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int j = 0; j < 8; j++) {
-    const int c = n0 + tc * 8 + j;
-    if (c >= N) continue;
-    const float dv = TRSM ? Dinv[(int64_t)d.col0 + kb + c] : 0.0f;
-#pragma unroll
-    for (int i = 0; i < 8; i++) {
-      const int r = m0 + tr * 8 + i;
-      if (r >= M) continue;
-      if (TRSM) {
-        C[r + (int64_t)c * ldc] = acc[i][j] * dv;
-      } else if (r >= c) {
-        C[r + (int64_t)c * ldc] -= acc[i][j];
-      }
+    if (k0 + kBK < K) {
+      store(buf ^ 1);
+      __syncthreads();
+      buf ^= 1;
     }
   }
-  if (TRSM && pack != nullptr && d.pk >= 0) {
-    // The finished block column again, in the packed layout (PackedFront):
-    // two 4-column K-groups of each of this thread's rows.
-    float *pk = pack + d.pk;
-    float  dvs[8];
+  if (!TRSM) {
 #pragma unroll
     for (int j = 0; j < 8; j++) {
       const int c = n0 + tc * 8 + j;
-      dvs[j]      = c < N ? Dinv[(int64_t)d.col0 + kb + c] : 0.0f;
-    }
+      if (c >= N) continue;
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
-      const int r = m0 + tr * 8 + i;
-      if (r >= M) continue;
-      const int rf = kb + nbk + r;  // row of the front
-      const int p  = rf < w ? rf : rf - w + d.pk_wt;
-      float    *row = pk + static_cast<int64_t>(p >> 7) * d.pk_g * PackedFront::kGroupFloats +
-                   (p & 127) * 4;
-#pragma unroll
-      for (int hh = 0; hh < 2; hh++) {
-        const int c0 = n0 + tc * 8 + hh * 4;
-        if (c0 >= N) continue;
-        float4 v;
-        v.x = acc[i][hh * 4 + 0] * dvs[hh * 4 + 0];
-        v.y = acc[i][hh * 4 + 1] * dvs[hh * 4 + 1];
-        v.z = acc[i][hh * 4 + 2] * dvs[hh * 4 + 2];
-        v.w = acc[i][hh * 4 + 3] * dvs[hh * 4 + 3];
-        *reinterpret_cast<float4 *>(row + static_cast<int64_t>((kb + c0) >> 2) *
-                                              PackedFront::kGroupFloats) = v;
+      for (int i = 0; i < 8; i++) {
+        const int r = m0 + tr * 8 + i;
+        if (r < M && r >= c) C[r + (int64_t)c * ldc] -= acc[i][j];
       }
+    }
+    return;
+  }
+  // TRSM epilogue: the tile times Dinv goes through shared memory, then to
+  // the panel as 128-row column segments (one warp per column) and to the
+  // packed front as whole 2 KB K-groups (PackedFront), both coalesced.
+  extern __shared__ float tile_s[];  // kBM x (kBN + 1)
+  constexpr int           LT = kBN + 1;
+  float                   dvs[8];
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    const int c = n0 + tc * 8 + j;
+    dvs[j]      = c < N ? Dinv[(int64_t)d.col0 + kb + c] : 0.0f;
+  }
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+#pragma unroll
+    for (int j = 0; j < 8; j++) tile_s[(tr * 8 + i) * LT + tc * 8 + j] = acc[i][j] * dvs[j];
+  __syncthreads();
+  const int warp = tid / 32, lane = tid % 32;
+  for (int c = warp; c < N; c += kGemmThreads / 32)
+#pragma unroll
+    for (int q = 0; q < kBM / 32; q++) {
+      const int r = lane + 32 * q;
+      if (m0 + r < M) C[m0 + r + (int64_t)c * ldc] = tile_s[r * LT + c];
+    }
+  if (pack != nullptr && d.pk >= 0) {
+    float *pk = pack + d.pk;
+    for (int e = tid; e < kBM * (kBN / 4); e += kGemmThreads) {
+      const int m = e % kBM, g = e / kBM, c0 = 4 * g;
+      if (c0 >= N || m0 + m >= M) continue;
+      const int rf = kb + nbk + m0 + m;  // row of the front
+      const int p  = rf < w ? rf : rf - w + d.pk_wt;
+      float4    v;
+      v.x = tile_s[m * LT + c0 + 0];
+      v.y = tile_s[m * LT + c0 + 1];
+      v.z = tile_s[m * LT + c0 + 2];
+      v.w = tile_s[m * LT + c0 + 3];
+      *reinterpret_cast<float4 *>(pk +
+                                  static_cast<int64_t>(p >> 7) * d.pk_g * PackedFront::kGroupFloats +
+                                  static_cast<int64_t>((kb + c0) >> 2) * PackedFront::kGroupFloats +
+                                  (p & 127) * 4) = v;
     }
   }
 }
@@ -1141,6 +1167,13 @@ void Numeric::run(const Plan &P, const double *d_Ax, double eps, cudaStream_t s)
   MPIR_CHECK_LAUNCH();
   float        *pan = panel.as<float>(), *ua = uarena.as<float>();
   FactorStatus *st  = status.as<FactorStatus>();
+  static bool   trsm_attr = false;
+  const int     trsm_smem = kBM * (kBN + 1) * sizeof(float);
+  if (!trsm_attr) {
+    MPIR_CUDA(cudaFuncSetAttribute(k_step_gemm<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   trsm_smem));
+    trsm_attr = true;
+  }
   static bool   diag_attr = false;
   const int     diag_smem = kDiagSmemFloats * sizeof(float);
   if (!diag_attr) {
@@ -1196,7 +1229,7 @@ void Numeric::run(const Plan &P, const double *d_Ax, double eps, cudaStream_t s)
       kt.end(s);
       if (stp.trsm_tiles > 0) {
         kt.begin(kKcTrsm, s);
-        launch(k_step_gemm<true>, stp.trsm_tiles, kGemmThreads, 0, s, 
+        launch(k_step_gemm<true>, stp.trsm_tiles, kGemmThreads, trsm_smem, s, 
             dd, stp.count, pan, ua, linv.as<float>(), Dinv.as<float>(), pack.as<float>());
         kt.end(s);
       }
