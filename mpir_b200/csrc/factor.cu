@@ -171,40 +171,44 @@ __global__ void k_extend_add(const EaTask *tasks, int ntasks,
     const int mid = (lo + hi + 1) / 2;
     if (tasks[mid].chunk0 <= t) lo = mid; else hi = mid - 1;
   }
-  const EaTask   tk  = tasks[lo];
-  const int      b0  = (t - tk.chunk0) * kEaChunk;
-  const int      b1  = min(b0 + kEaChunk, tk.rc);
-  const int32_t *rl  = srel + tk.rel;
-  const float   *U   = uarena + tk.child_u;
-  float         *Pp  = panel + tk.parent_panel;
-  const int      rp  = tk.hp - tk.wp;
-  for (int b = b0; b < b1; b++) {
-    const int cb = rl[b];
-    // Column cb of the parent: in its panel (rows from 0) or in its update
-    // matrix (rows from wp).
-    const int off = cb < tk.wp ? 0 : tk.wp;
-    float    *dst = cb < tk.wp ? Pp + (int64_t)cb * tk.hp
-                               : uarena + tk.parent_u + (int64_t)(cb - tk.wp) * rp;
-    const float *Ub = U + (int64_t)b * tk.rc;
-    // Four rows per thread at a time: all loads first (the source and the
-    // destination both may lie in the update arena, so the compiler would
-    // not reorder them itself).
-    for (int a0 = b + threadIdx.x; a0 < tk.rc; a0 += 4 * blockDim.x) {
-      int   ra[4];
-      float v[4];
+  const EaTask   tk = tasks[lo];
+  const int      b0 = (t - tk.chunk0) * kEaChunk;
+  const int      nb = min(kEaChunk, tk.rc - b0);
+  const int32_t *rl = srel + tk.rel;
+  const float   *U  = uarena + tk.child_u;
+  const int      rp = tk.hp - tk.wp;
+  // Column b0 + u of U_C goes to column rl[b0 + u] of the parent: in its
+  // panel (rows from 0) or in its update matrix (rows from wp).
+  __shared__ float *dst_s[kEaChunk];
+  __shared__ int    off_s[kEaChunk];
+  if (threadIdx.x < nb) {
+    const int cb = rl[b0 + threadIdx.x];
+    dst_s[threadIdx.x] = cb < tk.wp ? panel + tk.parent_panel + (int64_t)cb * tk.hp
+                                    : uarena + tk.parent_u + (int64_t)(cb - tk.wp) * rp;
+    off_s[threadIdx.x] = cb < tk.wp ? 0 : tk.wp;
+  }
+  __syncthreads();
+  // Each thread takes one row at a time across all the chunk's columns: the
+  // row map entry is loaded one row ahead, so the values of U_C and of the
+  // parent are loaded together, all before any store (the source and the
+  // destination may both lie in the update arena, so the compiler would not
+  // reorder them itself).
+  int a  = b0 + threadIdx.x;
+  int ra = a < tk.rc ? rl[a] : -1;
+  for (; a < tk.rc; a += blockDim.x) {
+    const int an     = a + blockDim.x;
+    const int ra_nxt = an < tk.rc ? rl[an] : -1;
+    float     v[kEaChunk], o[kEaChunk];
 #pragma unroll
-      for (int u = 0; u < 4; u++) {
-        const int a = a0 + u * blockDim.x;
-        ra[u]       = a < tk.rc ? rl[a] : -1;
-        v[u]        = a < tk.rc ? Ub[a] : 0.0f;
-      }
-      float o[4];
-#pragma unroll
-      for (int u = 0; u < 4; u++) o[u] = ra[u] >= 0 ? dst[ra[u] - off] : 0.0f;
-#pragma unroll
-      for (int u = 0; u < 4; u++)
-        if (ra[u] >= 0) dst[ra[u] - off] = o[u] + v[u];
+    for (int u = 0; u < kEaChunk; u++) {
+      const bool ok = u < nb && a >= b0 + u;
+      v[u]          = ok ? U[a + (int64_t)(b0 + u) * tk.rc] : 0.0f;
+      o[u]          = ok ? dst_s[u][ra - off_s[u]] : 0.0f;
     }
+#pragma unroll
+    for (int u = 0; u < kEaChunk; u++)
+      if (u < nb && a >= b0 + u) dst_s[u][ra - off_s[u]] = o[u] + v[u];
+    ra = ra_nxt;
   }
 }
 
