@@ -49,32 +49,47 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
+// Thread layout of the forward block product: lane l of warp v takes row
+// i = 8 v + l / 4 of the block and its slice q = l % 4 (32 terms);
+// the four slices of i sit in four neighbouring lanes and are added with two
+// shuffles, (s0 + s1) + (s2 + s3), with no CTA barrier.  Vectors the
+// products read are staged with a stride of 33 per 32 entries (pad()), so
+// the four slices of a warp read different banks.
+__device__ __forceinline__ int blk_i() { return (threadIdx.x / 32) * 8 + (threadIdx.x % 32) / 4; }
+__device__ __forceinline__ int blk_q() { return threadIdx.x % 4; }
+__device__ __forceinline__ int pad(int j) { return (j / 32) * 33 + j % 32; }
+__device__ __forceinline__ double quad_sum(double s) {
+  s += __shfl_xor_sync(0xffffffffu, s, 1);
+  s += __shfl_xor_sync(0xffffffffu, s, 2);
+  return s;
+}
+
 // Stage Linv (column-major, leading dimension kNB) for y = Linv z.
 __device__ __forceinline__ void stage_lower(const double *Lv, double *Ls, int nb) {
-  const int tid = threadIdx.x, i = tid % kNB, q = tid / kNB;
+  const int i = blk_i(), q = blk_q();
   for (int jj = 0; jj < kNB / 4; jj++) {
     const int j = q * (kNB / 4) + jj;
     if (j <= i && i < nb) cp_async8(Ls + kNB * j - j * (j - 1) / 2 + (i - j), Lv + i + j * kNB);
   }
 }
 
-// y = Linv z from the staged copy.
-__device__ __forceinline__ double block_lower_apply(const double *Ls, const double *zb, int nb,
-                                                    double (*part)[kNB]) {
-  const int tid = threadIdx.x, i = tid % kNB, q = tid / kNB;
+// y_i = (Linv z)_i from the staged copy, in all four lanes of row i; z is
+// staged with pad().
+__device__ __forceinline__ double block_lower_apply(const double *Ls, const double *zb, int nb) {
+  const int i = blk_i(), q = blk_q();
   cp_async_wait_all();
   double acc = 0.0;
 #pragma unroll 8
   for (int jj = 0; jj < kNB / 4; jj++) {
     const int j = q * (kNB / 4) + jj;
-    if (j <= i && i < nb) acc += Ls[kNB * j - j * (j - 1) / 2 + (i - j)] * zb[j];
+    if (j <= i && i < nb) acc += Ls[kNB * j - j * (j - 1) / 2 + (i - j)] * zb[pad(j)];
   }
-  part[q][i] = acc;
-  __syncthreads();
-  return (part[0][i] + part[1][i]) + (part[2][i] + part[3][i]);
+  return quad_sum(acc);
 }
 
-// Stage the row-major copy Lt (Lt[i * kNB + j] = Linv[i][j]) for x = Linv^T v.
+// Stage the row-major copy Lt (Lt[i * kNB + j] = Linv[i][j]) for x = Linv^T v:
+// thread (q, j) = (tid / 128, tid % 128) copies rows i >= j of slice q (a
+// warp reads 32 consecutive entries of a row).
 __device__ __forceinline__ void stage_upper(const double *Lt, double *Ls, int nb) {
   const int tid = threadIdx.x, j = tid % kNB, q = tid / kNB;
   for (int ii = 0; ii < kNB / 4; ii++) {
@@ -83,7 +98,8 @@ __device__ __forceinline__ void stage_upper(const double *Lt, double *Ls, int nb
   }
 }
 
-// x = Linv^T v from the staged copy: thread (q, j) adds rows i >= j of slice q.
+// x_j = (Linv^T v)_j from the staged copy for thread (q, j): the four slices
+// are added in order through part (one CTA barrier).
 __device__ __forceinline__ double block_upper_apply(const double *Ls, const double *v, int nb,
                                                     double (*part)[kNB]) {
   const int tid = threadIdx.x, j = tid % kNB, q = tid / kNB;
@@ -201,20 +217,22 @@ __device__ __forceinline__ int take_ticket(int32_t *counter) {
 
 // Forward solve of the large fronts of one level: one CTA per 128-row block
 // R of a front.  z_R -= L_{R,b} y_b for the column blocks b left of R, in
-// order, each as soon as y_b is ready: thread (q, i) takes row i and the
-// columns 32q .. 32q+31 of each tile, loads its L values before the wait, and
-// each warp waits for the flag and stages y_b on its own (no CTA barrier per
-// tile); the four quarters are added in order at the end.  A diagonal row
-// block then solves y_R = Linv_R z_R into x and releases flag R; rows at or
+// order, each as soon as y_b is ready: thread (q, i) = (tid / 128,
+// tid % 128) takes row i and the columns 32 q .. 32 q + 31 of each tile (a
+// warp's loads are one 128-byte column segment), loads its L values before
+// the wait, and each warp waits for the flag and stages its slice of y_b on
+// its own (no CTA barrier per tile); the four slices are added in order at
+// the end.  A diagonal row block then solves y_R = Linv_R z_R into x (block
+// product with warp-local slices, see blk_i) and releases flag R; rows at or
 // past w are the front's update vector for its parent.
 __global__ void __launch_bounds__(kSolveThreads, 1)
     k_fwd_fronts(const SolveFront *fr, const int32_t *fmap, const int32_t *frow,
-                 const float *panel,
-                 const double *linv64,
-                 const int64_t *gp, const int64_t *gsrc, double *x, double *zbuf,
-                 int32_t *tickets, int32_t *flags, int32_t *err) {
+                 const float *panel, const double *linv64, const int64_t *gp,
+                 const int64_t *gsrc, double *x, double *zbuf, int32_t *tickets,
+                 int32_t *flags, int32_t *err) {
   extern __shared__ double tri[];  // kTri doubles: the staged Linv_R
-  __shared__ double ys[kNB];
+  __shared__ double ys[4 * 33];
+  __shared__ double ys2[4 * 33];
   __shared__ double yw[kSolveThreads / 32][32];
   __shared__ double part[4][kNB];
   const int         item = take_ticket(tickets);
@@ -223,14 +241,14 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   if (R < F.nb)
     stage_lower(linv64 + F.linv + static_cast<int64_t>(R) * kNB * kNB, tri,
                 min(kNB, F.w - R * kNB));
-  const int         tid = threadIdx.x, rr = tid % kNB, qq = tid / kNB;
-  const int         warp = tid / 32, lane = tid % 32;
-  const int64_t     h = F.h;
-  const int         w = F.w;
-  const int64_t     r = static_cast<int64_t>(R) * kNB + rr;
-  const float      *P  = panel + F.panel;
-  int32_t          *fl = flags + F.flag0;
-  const int         tiles = min(R, F.nb);
+  const int     tid = threadIdx.x, rr = tid % kNB, qq = tid / kNB;
+  const int     warp = tid / 32, lane = tid % 32;
+  const int64_t h = F.h;
+  const int     w = F.w;
+  const int64_t r = static_cast<int64_t>(R) * kNB + rr;
+  const float  *P  = panel + F.panel;
+  int32_t      *fl = flags + F.flag0;
+  const int     tiles = min(R, F.nb);
   // Right-hand side of this row: its entry of x (rows < w), then the
   // children's update vectors in child order.
   double zr = 0.0;
@@ -238,7 +256,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
     zr = r < w ? x[F.col0 + r] : 0.0;
     for (int64_t e = gp[F.gptr + r]; e < gp[F.gptr + r + 1]; e++) zr += zbuf[gsrc[e]];
   }
-  double            acc   = 0.0;
+  double acc = 0.0;
   for (int b = 0; b < tiles; b++) {
     const int c0 = b * kNB + qq * 32;
     float     lv[32];
@@ -259,20 +277,19 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   if (qq == 0 && r < h) z = zr - ((part[0][rr] + part[1][rr]) + (part[2][rr] + part[3][rr]));
   if (R < F.nb) {
     const int nbk = min(kNB, w - R * kNB);
+    if (qq == 0) ys[pad(rr)] = rr < nbk ? z : 0.0;
     __syncthreads();
-    if (tid < kNB) ys[tid] = tid < nbk ? z : 0.0;
-    __syncthreads();
-    const double y = block_lower_apply(tri, ys, nbk, part);
-    if (tid < nbk) x[F.col0 + R * kNB + tid] = y;
+    const double y  = block_lower_apply(tri, ys, nbk);
+    const int    iy = blk_i();
+    if (blk_q() == 0 && iy < nbk) x[F.col0 + R * kNB + iy] = y;
     if ((R + 1) * kNB > w && h > w) {
       // Rows of this block at or past w: their product with the block.
-      __syncthreads();
-      if (tid < kNB) ys[tid] = tid < nbk ? y : 0.0;
+      if (blk_q() == 0) ys2[pad(iy)] = iy < nbk ? y : 0.0;
       __syncthreads();
       double a2 = 0.0;
       if (r >= w && r < h)
         for (int k = qq * 32; k < min(nbk, qq * 32 + 32); k++)
-          a2 += static_cast<double>(P[r + static_cast<int64_t>(R * kNB + k) * h]) * ys[k];
+          a2 += static_cast<double>(P[r + static_cast<int64_t>(R * kNB + k) * h]) * ys2[pad(k)];
       part[qq][rr] = a2;
       __syncthreads();
       if (qq == 0 && r >= w && r < h)
