@@ -131,7 +131,15 @@ struct GemmProb {
   int32_t ntm, ntiles;  // row tiles; tiles of the (lower) tile pattern
   int32_t tile0;   // first CTA of this problem in its GEMM launch
   int32_t rtile0;  // first CTA of this problem in its reduction launch
+  // B converted ahead of the 3xTF32 product (k_convert_b): B D split into
+  // tf32 high and low parts, in the packed layout, at float offsets bc (high)
+  // and bc_lo (low) of the conversion buffer; btiles row tiles of bgroups
+  // K-groups each (row tiles bprow floats apart); cv0 = first CTA of this
+  // problem in its conversion launch.
+  int64_t bc, bc_lo, bprow;
+  int32_t btiles, bgroups, cv0;
 };
+constexpr int kConvGroups = 32;  // K-groups per conversion CTA
 
 // Extend-add task: add the lower triangle of child C's update matrix into
 // its parent's front, CTA-chunked by columns of U_C.

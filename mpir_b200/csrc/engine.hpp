@@ -76,11 +76,11 @@ struct LevelPlan {
   struct Step {
     int32_t begin, count, trsm_tiles, upd_tiles;
     // left-looking update of this block column before its diagonal block
-    int32_t ll_begin, ll_count, ll_tiles, ll_rtiles;
+    int32_t ll_begin, ll_count, ll_tiles, ll_rtiles, ll_convs;
   };
   std::vector<Step> steps;
   // update matrices of the level's large fronts, after their last step
-  int32_t u_begin = 0, u_count = 0, u_tiles = 0, u_rtiles = 0;
+  int32_t u_begin = 0, u_count = 0, u_tiles = 0, u_rtiles = 0, u_convs = 0;
   // Solve: large fronts' gather list = large list; small fronts handled by
   // one warp each; large fronts by the SolveFront launches: fronts
   // [sf_begin, sf_begin + sf_count), forward CTAs, backward chunk CTAs and
@@ -112,6 +112,7 @@ class Plan {
   DeviceBuffer small_list, large_list, steps, ea_tasks, zero_segs, linv_ofs_d, gemm_probs,
       solve_fronts, swarp_list, sblock_list, gp, gsrc, fwd_map, fwd_row, chunk_map, own_map;
   int64_t      ws_elems = 0;  // split-K partial tiles (floats)
+  int64_t      bconv_elems = 0;  // converted B operands of the largest launch (floats)
   std::vector<int32_t> h_small, h_large;
   // Solve lists: fronts solved by one warp, fronts with a SolveFront entry
   // (same order as the SolveFront array).
@@ -142,6 +143,8 @@ class Numeric {
   // Packed fronts for the tensor-core updates: rows (pack) and pivots
   // (packd: D, then sign(D) sqrt|D|, Plan::pd_elems floats each).
   DeviceBuffer pack, packd;
+  // B operands converted ahead of the 3xTF32 updates (GemmProb::bc).
+  DeviceBuffer bconv;
   DeviceBuffer AD, Axs, Kval, Korig, Ax;
   double       eps_uf = 0;
   bool         valid  = false;
@@ -161,9 +164,12 @@ class Numeric {
 // Tensor-core GemmProb updates from the packed fronts (mode 0 bfloat16,
 // 1 3xTF32, 2 float16).  packs = the sign(D) sqrt|D| array.
 void launch_gemm_tc(int mode, const GemmProb *probs, int nprob, int tiles, const float *pack,
-                    const float *packd, const float *packs, float *panel, float *uarena,
-                    float *ws, FactorStatus *st, cudaStream_t s);
+                    const float *packd, const float *packs, const float *bconv, float *panel,
+                    float *uarena, float *ws, FactorStatus *st, cudaStream_t s);
 int  tc_gemm_smem_bytes(int mode);
+// Converts the B operands of a launch's problems for the 3xTF32 product.
+void launch_convert_b(const GemmProb *probs, int nprob, int convs, const float *pack,
+                      const float *packd, float *bconv, cudaStream_t s);
 // Tensor-core GEMM CTAs resident per SM (shared-memory bound).
 int  tc_ctas_per_sm();
 // Streaming multiprocessors of a B200.

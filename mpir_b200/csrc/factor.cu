@@ -800,11 +800,13 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
   std::vector<EaTask>   tasks;
   std::vector<Segment>  segs;
   std::vector<GemmProb> probs;
-  ws_elems = 0;
+  ws_elems    = 0;
+  bconv_elems = 0;
   // Tiles, K splits, launch offsets and workspace of the problems
   // [begin, begin + count) of one launch.  With fewer tiles than about two
   // per SM, K is split (at least 256 per split) and the partials reduced.
-  auto finish_launch = [&](int32_t begin, int32_t count, int32_t &tiles, int32_t &rtiles) {
+  auto finish_launch = [&](int32_t begin, int32_t count, int32_t &tiles, int32_t &rtiles,
+                           int32_t &convs) {
     int64_t total = 0;
     for (int32_t q = begin; q < begin + count; q++) {
       GemmProb &g  = probs[q];
@@ -855,6 +857,22 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
     tiles    = static_cast<int32_t>(t0);
     rtiles   = static_cast<int32_t>(r0);
     ws_elems = std::max(ws_elems, w0);
+    // B converted once per launch for the 3xTF32 product: the problem's B
+    // row tiles, all K-groups its K range reads.
+    int64_t c0 = 0, b0 = 0;
+    for (int32_t q = begin; q < begin + count; q++) {
+      GemmProb &g = probs[q];
+      g.btiles    = (g.N + kBN - 1) / kBN;
+      g.bgroups   = static_cast<int32_t>((g.K + 31) / 32 * 8);
+      g.bprow     = static_cast<int64_t>(g.bgroups) * PackedFront::kGroupFloats;
+      g.bc        = b0;
+      g.bc_lo     = b0 + g.btiles * g.bprow;
+      b0 += 2 * g.btiles * g.bprow;
+      g.cv0 = static_cast<int32_t>(c0);
+      c0 += static_cast<int64_t>(g.btiles) * ((g.bgroups + kConvGroups - 1) / kConvGroups);
+    }
+    convs       = static_cast<int32_t>(c0);
+    bconv_elems = std::max(bconv_elems, b0);
   };
   for (int32_t t = 0; t < S.nlevels; t++) {
     LevelPlan &L = levels[t];
@@ -915,7 +933,7 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
       maxw = std::max(maxw, S.w(h_large[q]));
     for (int64_t kb = 0; kb < maxw; kb += kNB) {
       LevelPlan::Step st{static_cast<int32_t>(descs.size()), 0, 0, 0,
-                         static_cast<int32_t>(probs.size()), 0, 0, 0};
+                         static_cast<int32_t>(probs.size()), 0, 0, 0, 0};
       for (int32_t q = L.large_begin; q < L.large_begin + L.large_count; q++) {
         const int64_t J = h_large[q], w = S.w(J), h = S.h(J);
         if (w <= kb) continue;
@@ -965,7 +983,7 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
         st.count++;
       }
       st.ll_count = static_cast<int32_t>(probs.size()) - st.ll_begin;
-      finish_launch(st.ll_begin, st.ll_count, st.ll_tiles, st.ll_rtiles);
+      finish_launch(st.ll_begin, st.ll_count, st.ll_tiles, st.ll_rtiles, st.ll_convs);
       L.steps.push_back(st);
     }
     // Solve work of the level: narrow, short fronts one warp each, the rest
@@ -1073,7 +1091,7 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
       probs.push_back(g);
     }
     L.u_count = static_cast<int32_t>(probs.size()) - L.u_begin;
-    finish_launch(L.u_begin, L.u_count, L.u_tiles, L.u_rtiles);
+    finish_launch(L.u_begin, L.u_count, L.u_tiles, L.u_rtiles, L.u_convs);
   }
   ndesc = static_cast<int64_t>(descs.size());
   panel_read_bytes = 0;
@@ -1129,6 +1147,7 @@ void Numeric::allocate(const Plan &P) {
   ws.resize(std::max<int64_t>(P.ws_elems, 1) * sizeof(float));
   // Packed fronts: positions that hold no value of L are never written and
   // stay zero from here on.
+  bconv.resize(std::max<int64_t>(P.bconv_elems, 1) * sizeof(float));
   pack.resize(std::max<int64_t>(P.pk_elems, 1) * sizeof(float));
   packd.resize(std::max<int64_t>(2 * P.pd_elems, 1) * sizeof(float));
   MPIR_CUDA(cudaMemset(pack.as<void>(), 0, pack.bytes()));
@@ -1208,16 +1227,20 @@ void Numeric::run(const Plan &P, const double *d_Ax, double eps, cudaStream_t s)
       kt.end(s);
     }
     const GemmProb *gp = P.gemm_probs.as<GemmProb>();
-    auto gemm = [&](int32_t begin, int32_t count, int32_t tiles, int32_t rtiles) {
+    auto gemm = [&](int32_t begin, int32_t count, int32_t tiles, int32_t rtiles,
+                    int32_t convs) {
       if (count <= 0 || tiles <= 0) return;
       kt.begin(kKcUpdate, s);
+      if (update_mode == 1 && convs > 0)
+        launch_convert_b(gp + begin, count, convs, pack.as<float>(), packd.as<float>(),
+                         bconv.as<float>(), s);
       if (update_mode < 0)
         launch(k_gemm_simt, tiles, kGemmThreads, 0, s, gp + begin, count, pan, ua,
                static_cast<const float *>(D.as<float>()), ws.as<float>());
       else
         launch_gemm_tc(update_mode, gp + begin, count, tiles, pack.as<float>(),
-                       packd.as<float>(), packd.as<float>() + P.pd_elems, pan, ua,
-                       ws.as<float>(), st, s);
+                       packd.as<float>(), packd.as<float>() + P.pd_elems, bconv.as<float>(),
+                       pan, ua, ws.as<float>(), st, s);
       if (rtiles > 0)
         launch(k_split_reduce, rtiles, 256, 0, s, gp + begin, count, pan, ua,
                static_cast<const float *>(ws.as<float>()));
@@ -1225,7 +1248,7 @@ void Numeric::run(const Plan &P, const double *d_Ax, double eps, cudaStream_t s)
     };
     for (const auto &stp : L.steps) {
       const StepDesc *dd = P.steps.as<StepDesc>() + stp.begin;
-      gemm(stp.ll_begin, stp.ll_count, stp.ll_tiles, stp.ll_rtiles);
+      gemm(stp.ll_begin, stp.ll_count, stp.ll_tiles, stp.ll_rtiles, stp.ll_convs);
       kt.begin(kKcDiag, s);
       launch(k_diag_block, stp.count, kDiagThreads, diag_smem, s, dd, pan, linv.as<float>(),
              D.as<float>(), Dinv.as<float>(), packd.as<float>(),
@@ -1238,7 +1261,7 @@ void Numeric::run(const Plan &P, const double *d_Ax, double eps, cudaStream_t s)
         kt.end(s);
       }
     }
-    gemm(L.u_begin, L.u_count, L.u_tiles, L.u_rtiles);
+    gemm(L.u_begin, L.u_count, L.u_tiles, L.u_rtiles, L.u_convs);
     MPIR_CHECK_LAUNCH();
   }
   // Float64 inverses of the diagonal blocks for the triangular solves.

@@ -171,35 +171,43 @@ __device__ __forceinline__ uint32_t pack16(float a, float b) {
   return MODE == 2 ? pack_f16(a, b) : pack_bf16(a, b);
 }
 
-// Round packed row m of one stage in place (see the file comment).
-template <int MODE>
+// tf32 high and low parts of four values (round to nearest both times).
+__device__ __forceinline__ void split4(const float (&v)[4], uint4 &hi, uint4 &lo) {
+  uint32_t *hp = &hi.x, *lp = &lo.x;
+#pragma unroll
+  for (int e = 0; e < 4; e++) {
+    const uint32_t h = to_tf32(v[e]);
+    hp[e]            = h;
+    lp[e]            = to_tf32(v[e] - __uint_as_float(h));
+  }
+}
+
+// Round packed row m of one stage in place (see the file comment).  PRE: B
+// arrived already split (k_convert_b), so only A is converted.
+template <int MODE, bool PRE>
 __device__ __forceinline__ void convert_row(uint8_t *stage, int m) {
   using C         = Cfg<MODE>;
   const float *dv = reinterpret_cast<const float *>(stage + C::kD);
   if (MODE == 1) {
 #pragma unroll
     for (int g = 0; g < C::kKG; g++) {
-      float4 *pa = reinterpret_cast<float4 *>(stage + C::kA + g * kGroup + m * 16);
-      float4 *pb = reinterpret_cast<float4 *>(stage + C::kB + g * kGroup + m * 16);
-      const float4 a = *pa, b = *pb;
-      const float4 d = *reinterpret_cast<const float4 *>(dv + 4 * g);
+      float4      *pa    = reinterpret_cast<float4 *>(stage + C::kA + g * kGroup + m * 16);
+      const float4 a     = *pa;
       const float  av[4] = {a.x, a.y, a.z, a.w};
-      const float  bv[4] = {b.x * d.x, b.y * d.y, b.z * d.z, b.w * d.w};
-      uint4        ah, al, bh, bl;
-      uint32_t    *ahp = &ah.x, *alp = &al.x, *bhp = &bh.x, *blp = &bl.x;
-#pragma unroll
-      for (int e = 0; e < 4; e++) {
-        const uint32_t xh = to_tf32(av[e]);
-        ahp[e]            = xh;
-        alp[e]            = to_tf32(av[e] - __uint_as_float(xh));
-        const uint32_t yh = to_tf32(bv[e]);
-        bhp[e]            = yh;
-        blp[e]            = to_tf32(bv[e] - __uint_as_float(yh));
-      }
-      *reinterpret_cast<uint4 *>(pa)                                         = ah;
-      *reinterpret_cast<uint4 *>(pb)                                         = bh;
+      uint4        ah, al;
+      split4(av, ah, al);
+      *reinterpret_cast<uint4 *>(pa)                                    = ah;
       *reinterpret_cast<uint4 *>(stage + C::kAlo + g * kGroup + m * 16) = al;
-      *reinterpret_cast<uint4 *>(stage + C::kBlo + g * kGroup + m * 16) = bl;
+      if (!PRE) {
+        float4      *pb    = reinterpret_cast<float4 *>(stage + C::kB + g * kGroup + m * 16);
+        const float4 b     = *pb;
+        const float4 d     = *reinterpret_cast<const float4 *>(dv + 4 * g);
+        const float  bv[4] = {b.x * d.x, b.y * d.y, b.z * d.z, b.w * d.w};
+        uint4        bh, bl;
+        split4(bv, bh, bl);
+        *reinterpret_cast<uint4 *>(pb)                                    = bh;
+        *reinterpret_cast<uint4 *>(stage + C::kBlo + g * kGroup + m * 16) = bl;
+      }
     }
   } else {
     // 32 columns of row m: read all (8 float32 K-groups), then write 4
@@ -293,10 +301,13 @@ constexpr int kMaxProbSmem = 2048;  // problems whose first units go to shared m
 template <int MODE>
 __global__ void __launch_bounds__(tc::kThreads, tc::kStages <= 3 ? 2 : 1)
     k_gemm_tc(const GemmProb *probs, int nprob, int units, const float *pack,
-              const float *packd, const float *packs, float *panel, float *uarena, float *ws,
-              FactorStatus *st) {
+              const float *packd, const float *packs, const float *bconv, float *panel,
+              float *uarena, float *ws, FactorStatus *st) {
   using namespace tc;
   using C = Cfg<MODE>;
+  // 3xTF32 with B converted ahead (k_convert_b): the producer copies B's
+  // high and low parts and the converters round A only.
+  const bool pre = MODE == 1 && bconv != nullptr;
   extern __shared__ __align__(1024) uint8_t smem[];
   // full[kStages], conv[kStages], empty[kStages], acc_full, acc_free, drain
   __shared__ __align__(8) uint64_t bars[3 * kStages + 3];
@@ -348,6 +359,10 @@ __global__ void __launch_bounds__(tc::kThreads, tc::kStages <= 3 ? 2 : 1)
         const float *Bg = pack + U.pb->pb + static_cast<int64_t>(U.j) * U.pb->prow +
                           static_cast<int64_t>(U.k_lo / 4) * PackedFront::kGroupFloats;
         const float *Dg = (C::kHalf ? packs : packd) + U.pb->pd + U.k_lo;
+        const int64_t bo = static_cast<int64_t>(U.j) * U.pb->bprow +
+                           static_cast<int64_t>(U.k_lo / 4) * PackedFront::kGroupFloats;
+        const float *Bh = pre ? bconv + U.pb->bc + bo : nullptr;
+        const float *Bl = pre ? bconv + U.pb->bc_lo + bo : nullptr;
         for (int c = 0; c < U.nch; c++, g++) {
           const int s = static_cast<int>(g % kStages);
           const int round = static_cast<int>(g / kStages);
@@ -356,14 +371,18 @@ __global__ void __launch_bounds__(tc::kThreads, tc::kStages <= 3 ? 2 : 1)
             break;
           }
           const uint32_t base = smem_u32(smem + s * C::kStage);
-          arrive_expect_tx(full0 + 8 * s, C::kTx);
-          bulk_load(base + C::kA,
-                    Ag + static_cast<int64_t>(c) * C::kKG * PackedFront::kGroupFloats, C::kRaw,
-                    full0 + 8 * s);
-          bulk_load(base + C::kB,
-                    Bg + static_cast<int64_t>(c) * C::kKG * PackedFront::kGroupFloats, C::kRaw,
-                    full0 + 8 * s);
-          bulk_load(base + C::kD, Dg + c * C::kKC, C::kKC * 4, full0 + 8 * s);
+          const int64_t  ko   = static_cast<int64_t>(c) * C::kKG * PackedFront::kGroupFloats;
+          if (pre) {
+            arrive_expect_tx(full0 + 8 * s, 3 * C::kRaw);
+            bulk_load(base + C::kA, Ag + ko, C::kRaw, full0 + 8 * s);
+            bulk_load(base + C::kB, Bh + ko, C::kRaw, full0 + 8 * s);
+            bulk_load(base + C::kBlo, Bl + ko, C::kRaw, full0 + 8 * s);
+          } else {
+            arrive_expect_tx(full0 + 8 * s, C::kTx);
+            bulk_load(base + C::kA, Ag + ko, C::kRaw, full0 + 8 * s);
+            bulk_load(base + C::kB, Bg + ko, C::kRaw, full0 + 8 * s);
+            bulk_load(base + C::kD, Dg + c * C::kKC, C::kKC * 4, full0 + 8 * s);
+          }
         }
       }
       // No copy may still target shared memory at exit: the last stage issued
@@ -445,7 +464,10 @@ __global__ void __launch_bounds__(tc::kThreads, tc::kStages <= 3 ? 2 : 1)
           ok = false;
           break;
         }
-        convert_row<MODE>(smem + s * C::kStage, m);
+        if (pre)
+          convert_row<MODE, true>(smem + s * C::kStage, m);
+        else
+          convert_row<MODE, false>(smem + s * C::kStage, m);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         arrive(conv0 + 8 * s);
       }
@@ -532,10 +554,53 @@ int tc_gemm_smem_bytes(int mode) {
   return static_cast<int>(tc::kStages * stage + kMaxProbSmem * sizeof(int));
 }
 
+// B of each problem of a launch, scaled by the pivots and split into tf32
+// high and low parts once (the 3xTF32 product would otherwise redo this in
+// every CTA that shares B): CTA t converts kConvGroups K-groups of one row
+// tile, thread (g, m) one packed row of one K-group, with the same
+// arithmetic as the in-kernel conversion.
+__global__ void __launch_bounds__(256)
+    k_convert_b(const GemmProb *probs, int nprob, const float *pack, const float *packd,
+                float *bconv) {
+  using namespace tc;
+  const int t  = blockIdx.x;
+  int       lo = 0, hi = nprob - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    if (probs[mid].cv0 <= t) lo = mid; else hi = mid - 1;
+  }
+  const GemmProb &pb     = probs[lo];
+  const int       chunks = (pb.bgroups + kConvGroups - 1) / kConvGroups;
+  const int       local  = t - pb.cv0;
+  const int       tile   = local / chunks;
+  const int       g0     = (local % chunks) * kConvGroups;
+  const int       g1     = min(g0 + kConvGroups, pb.bgroups);
+  const int       m      = threadIdx.x % 128;
+  for (int g = g0 + threadIdx.x / 128; g < g1; g += 2) {
+    const float4 b = *reinterpret_cast<const float4 *>(
+        pack + pb.pb + static_cast<int64_t>(tile) * pb.prow +
+        static_cast<int64_t>(g) * PackedFront::kGroupFloats + m * 4);
+    const float4 d     = *reinterpret_cast<const float4 *>(packd + pb.pd + 4 * g);
+    const float  bv[4] = {b.x * d.x, b.y * d.y, b.z * d.z, b.w * d.w};
+    uint4        bh, bl;
+    split4(bv, bh, bl);
+    const int64_t o = static_cast<int64_t>(tile) * pb.bprow +
+                      static_cast<int64_t>(g) * PackedFront::kGroupFloats + m * 4;
+    *reinterpret_cast<uint4 *>(bconv + pb.bc + o)    = bh;
+    *reinterpret_cast<uint4 *>(bconv + pb.bc_lo + o) = bl;
+  }
+}
+
+void launch_convert_b(const GemmProb *probs, int nprob, int convs, const float *pack,
+                      const float *packd, float *bconv, cudaStream_t s) {
+  if (convs > 0) launch(k_convert_b, convs, 256, 0, s, probs, nprob, pack, packd, bconv);
+}
+
 template <int MODE>
 static void launch_mode(const GemmProb *probs, int nprob, int units, const float *pack,
-                        const float *packd, const float *packs, float *panel, float *uarena,
-                        float *ws, FactorStatus *st, cudaStream_t s) {
+                        const float *packd, const float *packs, const float *bconv,
+                        float *panel, float *uarena, float *ws, FactorStatus *st,
+                        cudaStream_t s) {
   static bool attr = false;
   const int   smem = tc_gemm_smem_bytes(MODE);
   if (!attr) {
@@ -545,19 +610,19 @@ static void launch_mode(const GemmProb *probs, int nprob, int units, const float
   }
   const int grid = std::min(units, kSMs * tc_ctas_per_sm());
   launch(k_gemm_tc<MODE>, grid, tc::kThreads, smem, s, probs, nprob, units, pack, packd, packs,
-         panel, uarena, ws, st);
+         MODE == 1 ? bconv : nullptr, panel, uarena, ws, st);
 }
 
 void launch_gemm_tc(int mode, const GemmProb *probs, int nprob, int units, const float *pack,
-                    const float *packd, const float *packs, float *panel, float *uarena,
-                    float *ws, FactorStatus *st, cudaStream_t s) {
+                    const float *packd, const float *packs, const float *bconv, float *panel,
+                    float *uarena, float *ws, FactorStatus *st, cudaStream_t s) {
   if (units <= 0) return;
   if (mode == 0)
-    launch_mode<0>(probs, nprob, units, pack, packd, packs, panel, uarena, ws, st, s);
+    launch_mode<0>(probs, nprob, units, pack, packd, packs, bconv, panel, uarena, ws, st, s);
   else if (mode == 1)
-    launch_mode<1>(probs, nprob, units, pack, packd, packs, panel, uarena, ws, st, s);
+    launch_mode<1>(probs, nprob, units, pack, packd, packs, bconv, panel, uarena, ws, st, s);
   else
-    launch_mode<2>(probs, nprob, units, pack, packd, packs, panel, uarena, ws, st, s);
+    launch_mode<2>(probs, nprob, units, pack, packd, packs, bconv, panel, uarena, ws, st, s);
 }
 
 }  // namespace mpir
