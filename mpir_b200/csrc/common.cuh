@@ -153,11 +153,6 @@ struct EaTask {
   int32_t chunk0;      // first column chunk of this task within the launch
 };
 
-// Zero-fill segment (float offset into the update arena, length).
-struct Segment {
-  int64_t ofs, len;
-  int64_t chunk0;  // first chunk of this segment within the launch
-};
 
 // Output row of local packed row m of a problem, -1 inside its gap.
 __host__ __device__ __forceinline__ int gemm_out_row(const GemmProb &pb, int m) {
@@ -176,7 +171,6 @@ constexpr int kSmallThreads = 256;
 constexpr int kDiagThreads  = 512;
 constexpr int kGemmThreads  = 256;
 constexpr int kEaChunk      = 8;     // U_C columns per extend-add CTA
-constexpr int64_t kZeroChunk = 16384;  // floats per zero-fill CTA
 constexpr int kSolveRows = 128;        // rows per forward-solve CTA
 constexpr int kSolveChunk = 128;       // rows per backward-solve CTA
 constexpr int kSolveThreads = 512;     // 4 column quarters x 128 rows

@@ -67,8 +67,6 @@ DeviceBuffer upload(const std::vector<T> &v, cudaStream_t s) {
 struct LevelPlan {
   int32_t small_begin = 0, small_count = 0;  // into small list
   int32_t large_begin = 0, large_count = 0;  // into large list
-  int32_t zero_begin = 0, zero_count = 0;
-  int64_t zero_chunks = 0;
   struct Round {
     int32_t begin, count, chunks;
   };
@@ -109,7 +107,7 @@ class Plan {
   DeviceBuffer amap, arow, acol, diag_pos, Kp, Kj, Ksrc;
   DeviceBuffer sfirst, srowptr, srows, srel, slofs, uofs, zofs, child_ptr,
       child_list, perm;
-  DeviceBuffer small_list, large_list, steps, ea_tasks, zero_segs, linv_ofs_d, gemm_probs,
+  DeviceBuffer small_list, large_list, steps, ea_tasks, linv_ofs_d, gemm_probs,
       solve_fronts, swarp_list, sblock_list, gp, gsrc, fwd_map, fwd_row, chunk_map, own_map;
   int64_t      ws_elems = 0;  // split-K partial tiles (floats)
   int64_t      bconv_elems = 0;  // converted B operands of the largest launch (floats)

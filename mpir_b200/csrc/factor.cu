@@ -147,24 +147,14 @@ __global__ void __launch_bounds__(kSmallThreads)
 
 // ---------------------------------------------------------------------------
 // Zero the update matrices of the level's large fronts.
-__global__ void k_zero_segments(const Segment *segs, int nseg, float *base) {
-  const int64_t t  = blockIdx.x;
-  int           lo = 0, hi = nseg - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) / 2;
-    if (segs[mid].chunk0 <= t) lo = mid; else hi = mid - 1;
-  }
-  const Segment sg  = segs[lo];
-  const int64_t beg = (t - sg.chunk0) * kZeroChunk;
-  const int64_t end = min(beg + kZeroChunk, sg.len);
-  float        *p   = base + sg.ofs;
-  for (int64_t i = beg + threadIdx.x; i < end; i += blockDim.x) p[i] = 0.0f;
-}
 
 // Extend-add of children's update matrices into large parents.
+// phase 1: only the columns that go to the parent's panel (before the parent
+// is factored); phase 2: only those that go to its update matrix (after the
+// product that defines it).
 __global__ void k_extend_add(const EaTask *tasks, int ntasks,
                              const int32_t *srel, float *panel,
-                             float *uarena) {
+                             float *uarena, int phase) {
   const int t  = blockIdx.x;
   int       lo = 0, hi = ntasks - 1;
   while (lo < hi) {
@@ -181,13 +171,18 @@ __global__ void k_extend_add(const EaTask *tasks, int ntasks,
   // panel (rows from 0) or in its update matrix (rows from wp).
   __shared__ float *dst_s[kEaChunk];
   __shared__ int    off_s[kEaChunk];
-  if (threadIdx.x < nb) {
-    const int cb = rl[b0 + threadIdx.x];
-    dst_s[threadIdx.x] = cb < tk.wp ? panel + tk.parent_panel + (int64_t)cb * tk.hp
-                                    : uarena + tk.parent_u + (int64_t)(cb - tk.wp) * rp;
-    off_s[threadIdx.x] = cb < tk.wp ? 0 : tk.wp;
+  __shared__ int    act_s[kEaChunk];
+  if (threadIdx.x < kEaChunk) {
+    const int u  = threadIdx.x;
+    const int cb = u < nb ? rl[b0 + u] : 0;
+    dst_s[u]     = cb < tk.wp ? panel + tk.parent_panel + (int64_t)cb * tk.hp
+                              : uarena + tk.parent_u + (int64_t)(cb - tk.wp) * rp;
+    off_s[u]     = cb < tk.wp ? 0 : tk.wp;
+    act_s[u]     = u < nb && (phase == 1 ? cb < tk.wp : cb >= tk.wp);
   }
-  __syncthreads();
+  // The row map is increasing, so a chunk's columns all belong to one phase
+  // except at the panel / update-matrix boundary: leave if none is active.
+  if (!__syncthreads_or(threadIdx.x < kEaChunk && act_s[threadIdx.x])) return;
   // Each thread takes one row at a time across all the chunk's columns: the
   // row map entry is loaded one row ahead, so the values of U_C and of the
   // parent are loaded together, all before any store (the source and the
@@ -201,13 +196,13 @@ __global__ void k_extend_add(const EaTask *tasks, int ntasks,
     float     v[kEaChunk], o[kEaChunk];
 #pragma unroll
     for (int u = 0; u < kEaChunk; u++) {
-      const bool ok = u < nb && a >= b0 + u;
+      const bool ok = act_s[u] && a >= b0 + u;
       v[u]          = ok ? U[a + (int64_t)(b0 + u) * tk.rc] : 0.0f;
       o[u]          = ok ? dst_s[u][ra - off_s[u]] : 0.0f;
     }
 #pragma unroll
     for (int u = 0; u < kEaChunk; u++)
-      if (u < nb && a >= b0 + u) dst_s[u][ra - off_s[u]] = o[u] + v[u];
+      if (act_s[u] && a >= b0 + u) dst_s[u][ra - off_s[u]] = o[u] + v[u];
     ra = ra_nxt;
   }
 }
@@ -646,7 +641,8 @@ __global__ void __launch_bounds__(kGemmThreads)
 #pragma unroll
     for (int i = 0; i < 8; i++) {
       const int r = m0 + tr * 8 + i < M ? gemm_out_row(pb, m0 + tr * 8 + i) : -1;
-      if (r >= 0 && (!pb.lower || r >= c)) C[r + (int64_t)c * pb.ldc] -= acc[i][j];
+      if (r >= 0 && (!pb.lower || r >= c))
+        C[r + (int64_t)c * pb.ldc] = (pb.c_in_u ? 0.0f : C[r + (int64_t)c * pb.ldc]) - acc[i][j];
     }
   }
 }
@@ -698,7 +694,7 @@ __global__ void __launch_bounds__(256)
         const int r = m < pb.M ? gemm_out_row(pb, m) : -1;
         at[4 * u + v] = (r < 0 || c >= pb.N || (pb.lower && r < c)) ? -1
                                                                        : r + (int64_t)c * pb.ldc;
-        cv[4 * u + v] = at[4 * u + v] >= 0 ? C[at[4 * u + v]] : 0.0f;
+        cv[4 * u + v] = (!pb.c_in_u && at[4 * u + v] >= 0) ? C[at[4 * u + v]] : 0.0f;
       }
     }
 #pragma unroll
@@ -798,7 +794,6 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
   h_large.clear();
   std::vector<StepDesc> descs;
   std::vector<EaTask>   tasks;
-  std::vector<Segment>  segs;
   std::vector<GemmProb> probs;
   ws_elems    = 0;
   bconv_elems = 0;
@@ -884,17 +879,6 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
     }
     L.small_count = static_cast<int32_t>(h_small.size()) - L.small_begin;
     L.large_count = static_cast<int32_t>(h_large.size()) - L.large_begin;
-    // Zero-fill of the large fronts' update matrices.
-    L.zero_begin  = static_cast<int32_t>(segs.size());
-    int64_t chunk = 0;
-    for (int32_t q = L.large_begin; q < L.large_begin + L.large_count; q++) {
-      const int64_t J = h_large[q], r = S.h(J) - S.w(J);
-      if (r <= 0) continue;
-      segs.push_back(Segment{S.uofs[J], r * r, chunk});
-      chunk += (r * r + kZeroChunk - 1) / kZeroChunk;
-    }
-    L.zero_count  = static_cast<int32_t>(segs.size()) - L.zero_begin;
-    L.zero_chunks = chunk;
     // Extend-add rounds for the large fronts (round q = q-th child).
     int64_t maxkids = 0;
     for (int32_t q = L.large_begin; q < L.large_begin + L.large_count; q++) {
@@ -1121,7 +1105,6 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
   large_list = upload(h_large, s);
   steps      = upload(descs, s);
   ea_tasks   = upload(tasks, s);
-  zero_segs  = upload(segs, s);
   gemm_probs = upload(probs, s);
   linv_ofs_d = upload(linv_ofs, s);
   solve_fronts = upload(sfronts, s);
@@ -1205,18 +1188,17 @@ void Numeric::run(const Plan &P, const double *d_Ax, double eps, cudaStream_t s)
     diag_attr = true;
   }
   for (const LevelPlan &L : P.levels) {
-    if (L.zero_count > 0) {
-      kt.begin(kKcZero, s);
-      launch(k_zero_segments, static_cast<unsigned>(L.zero_chunks), 256, 0, s, 
-          P.zero_segs.as<Segment>() + L.zero_begin, L.zero_count, ua);
-      kt.end(s);
-    }
-    for (const auto &R : L.ea_rounds) {
-      kt.begin(kKcExtendAdd, s);
-      launch(k_extend_add, R.chunks, 256, 0, s, P.ea_tasks.as<EaTask>() + R.begin,
-                                            R.count, P.srel.as<int32_t>(), pan, ua);
-      kt.end(s);
-    }
+    // Children's update matrices into the fronts' panels (the update
+    // matrices' own columns follow after the product that defines them).
+    auto extend_add = [&](int phase) {
+      for (const auto &R : L.ea_rounds) {
+        kt.begin(kKcExtendAdd, s);
+        launch(k_extend_add, R.chunks, 256, 0, s, P.ea_tasks.as<EaTask>() + R.begin, R.count,
+               P.srel.as<int32_t>(), pan, ua, phase);
+        kt.end(s);
+      }
+    };
+    extend_add(1);
     if (L.small_count > 0) {
       kt.begin(kKcSmallFront, s);
       launch(k_small_fronts<kSmallFront>, L.small_count, kSmallThreads, 0, s, 
@@ -1262,6 +1244,7 @@ void Numeric::run(const Plan &P, const double *d_Ax, double eps, cudaStream_t s)
       }
     }
     gemm(L.u_begin, L.u_count, L.u_tiles, L.u_rtiles, L.u_convs);
+    extend_add(2);
     MPIR_CHECK_LAUNCH();
   }
   // Float64 inverses of the diagonal blocks for the triangular solves.

@@ -489,7 +489,7 @@ __global__ void __launch_bounds__(tc::kThreads, tc::kStages <= 3 ? 2 : 1)
                                     (static_cast<int64_t>(U.tile) * pb.splits + U.sp) *
                                         (kTileM * kTileN)
                                  : nullptr;
-      const int       N = pb.N, ldc = pb.ldc, lower = pb.lower;
+      const int       N = pb.N, ldc = pb.ldc, lower = pb.lower, c_in_u = pb.c_in_u;
 #pragma unroll
       for (int cb = 0; cb < kTileN / 32; cb++) {
         uint32_t       r[32];
@@ -522,7 +522,10 @@ __global__ void __launch_bounds__(tc::kThreads, tc::kStages <= 3 ? 2 : 1)
 #pragma unroll
             for (int q = 0; q < 16; q++) {
               const int col = n0 + cb * 32 + 16 * hh + q;
-              cv[q] = (col < N && (!lower || row >= col)) ? Cout[row + (int64_t)col * ldc] : 0.0f;
+              // an update matrix is defined by this product (stored, not updated)
+              cv[q] = (!c_in_u && col < N && (!lower || row >= col))
+                          ? Cout[row + (int64_t)col * ldc]
+                          : 0.0f;
             }
 #pragma unroll
             for (int q = 0; q < 16; q++) {
