@@ -209,158 +209,250 @@ __global__ void k_extend_add(const EaTask *tasks, int ntasks,
 
 // ---------------------------------------------------------------------------
 // Diagonal block of one step: LDL^T of the nbk x nbk block (nbk <= 128) and
-// the inverse X = L^{-1} of its unit-lower factor, blocked by 32 columns, in
-// shared memory (row-major copies of the block and of X):
-//   panel p (columns 32p .. 32p+31): thread (i, c) = (tid % 128, tid / 128)
-//     holds row i of the panel's columns 32p + c + 4t (t < 8) in registers;
-//     pivot k: the holders of column k publish it (double-buffered, one
-//     barrier per pivot) and each thread applies
-//     F[i][j] -= (F[i][k] / d_k) F[j][k] to its columns k < j <= i;
-//   after the panel: its multipliers L = F / d and its unscaled columns G go
-//     to shared memory, and the columns right of the panel take the rank-32
-//     update F[i][j] -= sum_k L[i][k] G[j][k] (no barrier inside);
-//   X: the four 32 x 32 diagonal blocks by forward substitution (one warp
-//     each, lane = column), then the blocks below them in three rounds,
-//     X_ab = -X_aa sum_{b <= c < a} L_ac X_cb.
-constexpr int kDiagLD = kNB + 1, kDiagLG = 33;
-constexpr int kDiagSmemFloats = 2 * kNB * kDiagLD + kNB * kDiagLG + 3 * 32 * kDiagLG;
+// the inverse X = L^{-1} of its unit-lower factor, right-looking by panels of
+// 32 columns in shared memory (row-major copies of the block and of X; the
+// block is padded with a unit diagonal up to a multiple of 32).  Panel p:
+//   A. warp 0 factors the 32 x 32 diagonal block: lane = row, the pivot
+//      column is broadcast by shuffles, F[i][j] -= (F[i][k] / d_k) F[j][k]
+//      (the reciprocal on this chain is the fast approximate one; D^{-1}
+//      itself is the correctly rounded 1 / d_k), then inverts its unit-lower
+//      factor by forward substitution (lane = column).  Meanwhile warps on
+//      the other three schedulers form T_pb = sum_{b <= c < p} L_pc X_cb for
+//      the blocks b < p of X's row block p;
+//   B. the rows below take their unscaled panel entries G = F X_pp^T
+//      (G = L D) and L = G D^{-1}, both kept transposed, while the warps
+//      without rows below finish X_pb = -X_pp T_pb;
+//   C. L goes into the block, and the columns right of the panel take the
+//      rank-32 update F[i][j] -= sum_k L[i][k] G[j][k] in 4 x 4 tiles.
+// One block-wide barrier per phase; nothing of X is left for after the loop.
+constexpr int kDiagLD = kNB + 1;  // Fs, Xs row stride (conflict-free columns)
+constexpr int kDiagLG = 36;       // Xd row stride (16-byte rows)
+constexpr int kDiagLT = 33;       // Ts row stride
+constexpr int kDiagSmemFloats =
+    2 * kNB * kDiagLD + 2 * 32 * kNB + 32 * kDiagLG + 3 * 32 * kDiagLT;
+
+// Phase A of panel p for warp 0: the diagonal block at (c0, c0).  Kept out
+// of line: inlined into the kernel, whose other phases hold many registers,
+// its chain of shuffles is scheduled about 1.5x slower.
+__device__ __noinline__ void diag_panel(float *Fs, float *Xs, float *Xd, float *dinv_s,
+                                           int c0, int n, const StepDesc &d, float *D,
+                                           float *Dinv, float *packd, float *packs,
+                                           FactorStatus *st, int &npos) {
+  constexpr int LD = kDiagLD, LG = kDiagLG;
+  const int     lane = threadIdx.x % 32, r = c0 + lane;
+  float         a[32];
+#pragma unroll
+  for (int j = 0; j < 32; j++) a[j] = Fs[r * LD + c0 + j];
+  float piv = 1.0f;
+#pragma unroll
+  for (int k = 0; k < 32; k++) {
+    const float dk = __shfl_sync(0xffffffffu, a[k], k);
+    const float dv = __fdividef(1.0f, dk);
+    const float l  = a[k] * dv;  // L[r][k]
+#pragma unroll
+    for (int j = 0; j < 32; j++) {
+      if (j > k) {
+        const float fjk = __shfl_sync(0xffffffffu, a[k], j);  // F[c0 + j][k]
+        if (j <= lane) a[j] -= l * fjk;
+      }
+    }
+    if (lane > k) a[k] = l;
+    if (lane == k) piv = dk;
+  }
+  const float pinv = 1.0f / piv;
+#pragma unroll
+  for (int j = 0; j < 32; j++) Fs[r * LD + c0 + j] = a[j];
+  dinv_s[r] = pinv;
+  if (r < n) {
+    const int64_t cidx = (int64_t)d.col0 + d.kb + r;
+    D[cidx]            = piv;
+    Dinv[cidx]         = pinv;
+    if (packd != nullptr && d.pd >= 0) {
+      packd[d.pd + d.kb + r] = piv;
+      packs[d.pd + d.kb + r] = copysignf(sqrtf(fabsf(piv)), piv);
+    }
+    note_pivot(st, static_cast<int32_t>(cidx), piv, &npos);
+  }
+  __syncwarp();
+  // X of the diagonal block (lane = column)
+  float x[32];
+#pragma unroll
+  for (int ii = 0; ii < 32; ii++) {
+    float acc = 0.0f;
+#pragma unroll
+    for (int kk = 0; kk < ii; kk++) acc += Fs[(c0 + ii) * LD + c0 + kk] * x[kk];
+    x[ii] = ii == lane ? 1.0f : (ii > lane ? -acc : 0.0f);
+  }
+#pragma unroll
+  for (int ii = 0; ii < 32; ii++) {
+    Xs[(c0 + ii) * LD + c0 + lane] = x[ii];
+    Xd[ii * LG + lane]             = x[ii];
+  }
+}
 
 __global__ void __launch_bounds__(kDiagThreads)
     k_diag_block(const StepDesc *descs, float *panel, float *linv, float *D, float *Dinv,
                  float *packd, float *packs, FactorStatus *st) {
   static_assert(kDiagThreads == 4 * kNB, "diag kernel thread mapping");
-  constexpr int LD = kDiagLD, LG = kDiagLG;
-  extern __shared__ float sm[];
-  float          *Fs = sm;                // the block, row-major
-  float          *Xs = Fs + kNB * LD;     // X, row-major
-  float          *Gs = Xs + kNB * LD;     // unscaled columns of the current panel
-  float          *Ts = Gs + kNB * LG;     // 3 scratch 32 x 32 blocks
-  __shared__ float col[2][kNB];
+  constexpr int LD = kDiagLD, LG = kDiagLG, LT = kDiagLT;
+  extern __shared__ __align__(16) float sm[];
+  float          *Fs = sm;             // the block, row-major
+  float          *Xs = Fs + kNB * LD;  // X, row-major
+  float          *Gt = Xs + kNB * LD;  // G^T of the current panel (rows below it)
+  float          *Lt = Gt + 32 * kNB;  // L^T of the current panel (rows below it)
+  float          *Xd = Lt + 32 * kNB;  // X of the current panel's diagonal block
+  float          *Ts = Xd + 32 * LG;   // T_pb, b < p
   __shared__ float dinv_s[kNB];
-  const StepDesc   d   = descs[blockIdx.x];
-  const int        n   = d.nbk;
-  const int64_t    h   = d.h;
+  const StepDesc   d    = descs[blockIdx.x];
+  const int        n    = d.nbk;
+  const int        nblk = (n + 31) / 32, n32 = 32 * nblk;
+  const int64_t    h    = d.h;
   const int        tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
-  const int        ri  = tid % kNB, c = tid / kNB;
-  float           *P   = panel + d.panel + d.kb + (int64_t)d.kb * h;
-  for (int idx = tid; idx < kNB * kNB; idx += kDiagThreads) {
-    const int i = idx % kNB, j = idx / kNB;
-    Fs[i * LD + j] = (i >= j && i < n && j < n) ? P[i + (int64_t)j * h] : 0.0f;
-    Xs[i * LD + j] = 0.0f;
+  const int        ri = tid % kNB, c = tid / kNB;
+  float           *P  = panel + d.panel + d.kb + (int64_t)d.kb * h;
+  {
+    // Thread (ri, c): row ri, columns c + 4m; all loads in flight before the
+    // first store.
+    float v[32];
+#pragma unroll
+    for (int m = 0; m < 32; m++) {
+      const int j = c + 4 * m;
+      v[m] = (ri >= j && ri < n) ? P[ri + (int64_t)j * h] : (ri == j ? 1.0f : 0.0f);
+    }
+#pragma unroll
+    for (int m = 0; m < 32; m++) Fs[ri * LD + c + 4 * m] = v[m];
   }
   __syncthreads();
   int npos = 0;
-  for (int c0 = 0; c0 < n; c0 += 32) {
-    float r[8];
+  for (int p = 0;; p++) {
+    const int c0 = 32 * p;
+    // A.
+    if (warp == 0) {
+      diag_panel(Fs, Xs, Xd, dinv_s, c0, n, d, D, Dinv, packd, packs, st, npos);
+    } else if (warp % 4 != 0) {
+      // T_pb (thread: rows 4 tr .. 4 tr + 3, columns 2 tc, 2 tc + 1 of block
+      // b); these warps share no scheduler with warp 0.
+      const int item = 32 * ((warp / 4) * 3 + warp % 4 - 1) + lane;
+      if (item < 128 * p) {
+        const int    b = item / 128, q = item % 128, tc = q % 16, tr = q / 16;
+        const float *Fr = Fs + (c0 + 4 * tr) * LD;
+        const float *Xc = Xs + 32 * b + 2 * tc;
+        float        acc[4][2] = {};
+#pragma unroll 4
+        for (int k = 32 * b; k < c0; k++) {
+          const float x0 = Xc[k * LD], x1 = Xc[k * LD + 1];
 #pragma unroll
-    for (int t = 0; t < 8; t++) r[t] = Fs[ri * LD + c0 + c + 4 * t];
-#pragma unroll
-    for (int kk = 0; kk < 32; kk++) {
-      const int k = c0 + kk;
-      if (k >= n) break;
-      const int b = kk & 1;
-      if (c == (kk & 3)) col[b][ri] = r[kk >> 2];
-      __syncthreads();
-      const float dk = col[b][k];
-      const float dv = 1.0f / dk;
-      if (ri > k && ri < n) {
-        const float s = col[b][ri] * dv;  // L[i][k]
-#pragma unroll
-        for (int t = 0; t < 8; t++) {
-          const int jj = c + 4 * t;
-          if (jj > kk && c0 + jj <= ri) r[t] -= s * col[b][c0 + jj];
+          for (int rr = 0; rr < 4; rr++) {
+            const float f = Fr[rr * LD + k];
+            acc[rr][0] += f * x0;
+            acc[rr][1] += f * x1;
+          }
         }
-      }
-      if (tid == 0) {
-        const int64_t cidx = (int64_t)d.col0 + d.kb + k;
-        dinv_s[k]          = dv;
-        D[cidx]            = dk;
-        Dinv[cidx]         = dv;
-        if (packd != nullptr && d.pd >= 0) {
-          packd[d.pd + d.kb + k] = dk;
-          packs[d.pd + d.kb + k] = copysignf(sqrtf(fabsf(dk)), dk);
+#pragma unroll
+        for (int rr = 0; rr < 4; rr++) {
+          Ts[b * 32 * LT + (4 * tr + rr) * LT + 2 * tc]     = acc[rr][0];
+          Ts[b * 32 * LT + (4 * tr + rr) * LT + 2 * tc + 1] = acc[rr][1];
         }
-        note_pivot(st, static_cast<int32_t>(cidx), dk, &npos);
       }
     }
     __syncthreads();
-    // The panel back: multipliers below the diagonal, pivots on it; the
-    // unscaled values for the trailing update.
+    // B.
+    const bool below = c0 + 32 < n32;
+    if (ri >= c0 + 32 && ri < n32) {
+      // G = F X_pp^T (thread: row ri, columns c + 4t)
+      float f[32];
 #pragma unroll
-    for (int t = 0; t < 8; t++) {
-      const int jj = c + 4 * t, j = c0 + jj;
-      if (j < n) {
-        Gs[ri * LG + jj] = r[t];
-        Fs[ri * LD + j]  = ri > j ? r[t] * dinv_s[j] : r[t];
+      for (int k = 0; k < 32; k++) f[k] = Fs[ri * LD + c0 + k];
+#pragma unroll
+      for (int t = 0; t < 8; t++) {
+        const int     jj  = c + 4 * t;
+        const float4 *xr  = reinterpret_cast<const float4 *>(Xd + jj * LG);
+        float         acc = 0.0f;
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+          const float4 xv = xr[q];
+          acc += f[4 * q] * xv.x;
+          acc += f[4 * q + 1] * xv.y;
+          acc += f[4 * q + 2] * xv.z;
+          acc += f[4 * q + 3] * xv.w;
+        }
+        Gt[jj * kNB + ri] = acc;
+        Lt[jj * kNB + ri] = acc * dinv_s[c0 + jj];
+      }
+    } else if (ri < c0 + 32 && p > 0) {
+      // X_pb = -X_pp T_pb (lane = column) on the warps without rows below.
+      const int u = (warp / 4) * (p + 1) + warp % 4, nu = 4 * (p + 1);
+      for (int e = u; e < 32 * p; e += nu) {
+        const int     b = e / 32, rr = e % 32;
+        const float4 *xr = reinterpret_cast<const float4 *>(Xd + rr * LG);
+        const float  *tb = Ts + b * 32 * LT + lane;
+        float         acc[4] = {};
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+          if (4 * q <= rr) {  // row rr of X_pp is zero right of rr
+            const float4 xv = xr[q];
+            acc[0] += xv.x * tb[(4 * q) * LT];
+            acc[1] += xv.y * tb[(4 * q + 1) * LT];
+            acc[2] += xv.z * tb[(4 * q + 2) * LT];
+            acc[3] += xv.w * tb[(4 * q + 3) * LT];
+          }
+        }
+        Xs[(c0 + rr) * LD + 32 * b + lane] = -((acc[0] + acc[1]) + (acc[2] + acc[3]));
+      }
+    }
+    if (!below) break;
+    __syncthreads();
+    // C. (the panel's L into the block; the update by 4 x 4 tiles of the
+    // lower triangle, row-major over the tiles)
+    if (ri >= c0 + 32 && ri < n32) {
+#pragma unroll
+      for (int t = 0; t < 8; t++) Fs[ri * LD + c0 + c + 4 * t] = Lt[(c + 4 * t) * kNB + ri];
+    }
+    {
+      const int mt = (n32 - c0 - 32) / 4, ntiles = mt * (mt + 1) / 2;
+      if (tid < ntiles) {
+        int ti = static_cast<int>((sqrtf(8.0f * tid + 1.0f) - 1.0f) * 0.5f);
+        if ((ti + 1) * (ti + 2) / 2 <= tid) ti++;
+        if (ti * (ti + 1) / 2 > tid) ti--;
+        const int tj = tid - ti * (ti + 1) / 2;
+        const int i0 = c0 + 32 + 4 * ti, j0 = c0 + 32 + 4 * tj;
+        float     acc[4][4] = {};
+#pragma unroll 8
+        for (int k = 0; k < 32; k++) {
+          const float4 lv = *reinterpret_cast<const float4 *>(Lt + k * kNB + i0);
+          const float4 gv = *reinterpret_cast<const float4 *>(Gt + k * kNB + j0);
+          const float  la[4] = {lv.x, lv.y, lv.z, lv.w}, ga[4] = {gv.x, gv.y, gv.z, gv.w};
+#pragma unroll
+          for (int r = 0; r < 4; r++)
+#pragma unroll
+            for (int s = 0; s < 4; s++) acc[r][s] += la[r] * ga[s];
+        }
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+#pragma unroll
+          for (int s = 0; s < 4; s++)
+            if (j0 + s <= i0 + r) Fs[(i0 + r) * LD + j0 + s] -= acc[r][s];
       }
     }
     __syncthreads();
-    if (c0 + 32 < n) {
-      if (ri >= c0 + 32 && ri < n) {
-        float lrow[32];
-#pragma unroll
-        for (int kk = 0; kk < 32; kk++) lrow[kk] = Fs[ri * LD + c0 + kk];
-        for (int j = c0 + 32 + c; j <= ri; j += 4) {
-          float acc = 0.0f;
-#pragma unroll
-          for (int kk = 0; kk < 32; kk++) acc += lrow[kk] * Gs[j * LG + kk];
-          Fs[ri * LD + j] -= acc;
-        }
-      }
-      __syncthreads();
-    }
   }
-  if (tid == 0) atomicAdd(&st->npos, npos);
-  // X: diagonal 32 x 32 blocks, one warp each (lane = column).
-  if (warp < 4 && 32 * warp < n) {
-    const int p0 = 32 * warp, j = p0 + lane;
-    float     xc[32];
-#pragma unroll
-    for (int ii = 0; ii < 32; ii++) {
-      const int i   = p0 + ii;
-      float     acc = 0.0f;
-#pragma unroll
-      for (int kk = 0; kk < ii; kk++) acc += Fs[i * LD + p0 + kk] * xc[kk];
-      xc[ii] = ii == lane ? 1.0f : (ii > lane ? -acc : 0.0f);
-    }
-#pragma unroll
-    for (int ii = 0; ii < 32; ii++) Xs[(p0 + ii) * LD + j] = xc[ii];
+  if (warp == 0) {
+    npos = __reduce_add_sync(0xffffffffu, npos);
+    if (lane == 0 && npos > 0) atomicAdd(&st->npos, npos);
   }
   __syncthreads();
-  // X below the diagonal blocks, by block distance dd.
-  const int nblk = (n + 31) / 32;
-  for (int dd = 1; dd < nblk; dd++) {
-    const int npair = nblk - dd;  // pairs (a, b) = (b + dd, b)
-    // T_e = sum_{b <= cb < a} L_{a,cb} X_{cb,b}
-    for (int e = tid; e < npair * 1024; e += kDiagThreads) {
-      const int pr = e / 1024, rr = (e % 1024) / 32, cc = e % 32;
-      const int bb = pr, aa = pr + dd;
-      float     acc = 0.0f;
-      for (int k = 32 * bb; k < 32 * aa; k++)
-        acc += Fs[(32 * aa + rr) * LD + k] * Xs[k * LD + 32 * bb + cc];
-      Ts[pr * 32 * LG + rr * LG + cc] = acc;
-    }
-    __syncthreads();
-    // X_ab = -X_aa T
-    for (int e = tid; e < npair * 1024; e += kDiagThreads) {
-      const int pr = e / 1024, rr = (e % 1024) / 32, cc = e % 32;
-      const int bb = pr, aa = pr + dd;
-      float     acc = 0.0f;
-#pragma unroll 8
-      for (int kk = 0; kk < 32; kk++)
-        acc += Xs[(32 * aa + rr) * LD + 32 * aa + kk] * Ts[pr * 32 * LG + kk * LG + cc];
-      Xs[(32 * aa + rr) * LD + 32 * bb + cc] = -acc;
-    }
-    __syncthreads();
-  }
-  for (int idx = tid; idx < kNB * kNB; idx += kDiagThreads) {
-    const int i = idx % kNB, j = idx / kNB;
-    if (i >= j && i < n && j < n) P[i + (int64_t)j * h] = Fs[i * LD + j];
+  // The factor back into the panel (lower triangle) and X (blocks above the
+  // diagonal blocks are zero).
+#pragma unroll 4
+  for (int m = 0; m < 32; m++) {
+    const int j = c + 4 * m;
+    if (ri >= j && ri < n) P[ri + (int64_t)j * h] = Fs[ri * LD + j];
   }
   float *Lv = linv + d.linv;
-  for (int idx = tid; idx < kNB * kNB; idx += kDiagThreads) {
-    const int i = idx % kNB, j = idx / kNB;
-    Lv[i + j * kNB] = (i < n && j < n) ? Xs[i * LD + j] : 0.0f;
+#pragma unroll 4
+  for (int m = 0; m < 32; m++) {
+    const int j = c + 4 * m;
+    Lv[ri + j * kNB] = (ri < n && j < n && ri / 32 >= j / 32) ? Xs[ri * LD + j] : 0.0f;
   }
 }
 
