@@ -78,7 +78,7 @@ struct SolveFront {
                    // gp[gptr + i] .. gp[gptr + i + 1], in child order
   int32_t h, w, nb;
   int32_t col0;    // permuted index of the front's first column
-  int32_t flag0;   // first of the front's nb ready flags
+  int32_t n;       // order of the whole system (stride of the ready copies)
   int32_t chunk0, chunks;  // backward chunk CTAs
   int32_t own0;    // first backward column-block CTA
 };

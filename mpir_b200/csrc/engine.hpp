@@ -99,9 +99,9 @@ class Plan {
   int64_t                nnz_full   = 0;
   int64_t                ndesc      = 0;  // step descriptors in total
   int64_t                spart_elems = 0; // backward chunk partials (doubles)
-  // Solve synchronisation words: 2 tickets per level, then the forward and
-  // the backward ready flags (nflags each); reset before every solve.
-  int64_t                nflags = 0, sync_elems = 0;
+  // Solve synchronisation words (2 tickets per level) and whether any front
+  // takes the ticketed block kernels; reset before every solve.
+  int64_t                nblock_fronts = 0, sync_elems = 0;
   double                 update_flops = 0, trsm_flops = 0, panel_read_bytes = 0;
   // Pattern arrays on the device.
   DeviceBuffer amap, arow, acol, diag_pos, Kp, Kj, Ksrc;

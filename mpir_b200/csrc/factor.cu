@@ -860,7 +860,7 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
   linv_ofs.assign(ns, -1);
   linv_elems   = 0;
   spart_elems  = 0;
-  nflags       = 0;
+  nblock_fronts = 0;
   h_swarp.clear();
   h_sblock.clear();
   std::vector<int64_t> gp_h, gsrc_h;
@@ -1104,8 +1104,8 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
       f.w      = static_cast<int32_t>(w);
       f.nb     = static_cast<int32_t>((w + kNB - 1) / kNB);
       f.col0   = static_cast<int32_t>(S.sfirst[J]);
-      f.flag0  = static_cast<int32_t>(nflags);
-      nflags += f.nb;
+      f.n      = static_cast<int32_t>(S.n);
+      nblock_fronts++;
       L.fwd_items += static_cast<int32_t>((h + kNB - 1) / kNB);
       f.chunks = static_cast<int32_t>((h - w + kNB - 1) / kNB);
       f.chunk0 = L.bwd_chunk_items;
@@ -1208,7 +1208,7 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
   fwd_row      = upload(fwd_row_h, s);
   chunk_map    = upload(chunk_map_h, s);
   own_map      = upload(own_map_h, s);
-  sync_elems   = 2 * static_cast<int64_t>(levels.size()) + 2 * nflags;
+  sync_elems   = 2 * static_cast<int64_t>(levels.size());
   MPIR_CUDA(cudaStreamSynchronize(s));
 }
 

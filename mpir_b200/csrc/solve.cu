@@ -76,15 +76,24 @@ __device__ __forceinline__ void stage_lower(const double *Lv, double *Ls, int nb
 // y_i = (Linv z)_i from the staged copy, in all four lanes of row i; z is
 // staged with pad().
 __device__ __forceinline__ double block_lower_apply(const double *Ls, const double *zb, int nb) {
-  const int i = blk_i(), q = blk_q();
+  const int     i = blk_i(), q = blk_q(), j0 = q * (kNB / 4);
+  const double *z = zb + 33 * q;  // pad(j0 + jj) = 33 q + jj
   cp_async_wait_all();
-  double acc = 0.0;
-#pragma unroll 8
-  for (int jj = 0; jj < kNB / 4; jj++) {
-    const int j = q * (kNB / 4) + jj;
-    if (j <= i && i < nb) acc += Ls[kNB * j - j * (j - 1) / 2 + (i - j)] * zb[pad(j)];
+  double a0 = 0.0, a1 = 0.0;
+  if (i < nb && i >= j0) {
+    // Column j starts at kNB j - j (j - 1) / 2: the offset of (i, j) grows
+    // by kNB - j - 1 from column j to column j + 1.
+    int off = kNB * j0 - j0 * (j0 - 1) / 2 + (i - j0);
+#pragma unroll
+    for (int jj = 0; jj < kNB / 4; jj += 2) {
+      const int j = j0 + jj;
+      if (j <= i) a0 += Ls[off] * z[jj];
+      off += kNB - j - 1;
+      if (j + 1 <= i) a1 += Ls[off] * z[jj + 1];
+      off += kNB - j - 2;
+    }
   }
-  return quad_sum(acc);
+  return quad_sum(a0 + a1);
 }
 
 // Stage the row-major copy Lt (Lt[i * kNB + j] = Linv[i][j]) for x = Linv^T v:
@@ -102,15 +111,21 @@ __device__ __forceinline__ void stage_upper(const double *Lt, double *Ls, int nb
 // are added in order through part (one CTA barrier).
 __device__ __forceinline__ double block_upper_apply(const double *Ls, const double *v, int nb,
                                                     double (*part)[kNB]) {
-  const int tid = threadIdx.x, j = tid % kNB, q = tid / kNB;
+  const int tid = threadIdx.x, j = tid % kNB, q = tid / kNB, i0 = q * (kNB / 4);
   cp_async_wait_all();
-  double acc = 0.0;
-#pragma unroll 8
-  for (int ii = 0; ii < kNB / 4; ii++) {
-    const int i = q * (kNB / 4) + ii;
-    if (i >= j && i < nb) acc += Ls[i * (i + 1) / 2 + j] * v[i];
+  double a0 = 0.0, a1 = 0.0;
+  // Row i starts at i (i + 1) / 2: the offset of (i, j) grows by i + 1 from
+  // row i to row i + 1.
+  int off = i0 * (i0 + 1) / 2 + j;
+#pragma unroll
+  for (int ii = 0; ii < kNB / 4; ii += 2) {
+    const int i = i0 + ii;
+    if (i >= j && i < nb) a0 += Ls[off] * v[i];
+    off += i + 1;
+    if (i + 1 >= j && i + 1 < nb) a1 += Ls[off] * v[i + 1];
+    off += i + 2;
   }
-  part[q][j] = acc;
+  part[q][j] = a0 + a1;
   __syncthreads();
   return (part[0][j] + part[1][j]) + (part[2][j] + part[3][j]);
 }
@@ -184,26 +199,43 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta)
 }
 
 
-// Ready flags between the CTAs of one solve launch (release / acquire at GPU
-// scope).  A wait gives up after a few seconds, sets the sticky error word
-// and returns false; once that word is set every other wait returns false at
-// once, so one failure ends the launch quickly.
-__device__ __forceinline__ int32_t ld_acquire(const int32_t *p) {
-  int32_t v;
-  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+// Block results go from the CTA that computes them to the CTAs that wait on
+// them through the ready buffer: each entry holds the pending marker (a
+// signalling NaN, which no arithmetic produces) until its value is stored,
+// and a waiting lane polls its own entry at GPU scope, so the value is its
+// own ready signal (no flag, no fence, no second load).  The producer stores
+// kReadyCopies copies; the warps of the ~150 CTAs that wait for the same
+// block poll different copies.  A wait gives up after a few seconds, sets
+// the sticky error word and returns 0; it looks at that word every 64 polls,
+// so one failure ends the launch quickly.
+constexpr unsigned long long kPending = 0x7ff0deadbeef0001ull;
+constexpr int kReadyCopies = 8;
+
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const double *p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
 }
-__device__ __forceinline__ void st_release(int32_t *p, int32_t v) {
-  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+__device__ __forceinline__ void st_relaxed_f64(double *p, double v) {
+  asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(__double_as_longlong(v))
+               : "memory");
 }
-__device__ __forceinline__ bool wait_flag(const int32_t *p, int32_t *err) {
+__device__ __forceinline__ double wait_value(const double *p, int32_t *err) {
   for (long it = 0; it < (1L << 22); it++) {
-    if (ld_acquire(p) != 0) return true;
-    if (*reinterpret_cast<volatile int32_t *>(err) != 0) return false;
-    if (it >= 64) __nanosleep(32);
+    const unsigned long long v = ld_relaxed_u64(p);
+    if (v != kPending) return __longlong_as_double(static_cast<long long>(v));
+    if ((it & 63) == 63) {
+      if (*reinterpret_cast<volatile int32_t *>(err) != 0) return 0.0;
+      __nanosleep(32);
+    }
   }
   atomicExch(err, 1);
-  return false;
+  return 0.0;
+}
+
+__global__ void k_mark_pending(int64_t n, double *ready) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) reinterpret_cast<unsigned long long *>(ready)[i] = kPending;
 }
 
 // CTA-wide ticket: the order in which CTAs of a launch take their work.
@@ -220,16 +252,16 @@ __device__ __forceinline__ int take_ticket(int32_t *counter) {
 // order, each as soon as y_b is ready: thread (q, i) = (tid / 128,
 // tid % 128) takes row i and the columns 32 q .. 32 q + 31 of each tile (a
 // warp's loads are one 128-byte column segment), loads its L values before
-// the wait, and each warp waits for the flag and stages its slice of y_b on
-// its own (no CTA barrier per tile); the four slices are added in order at
-// the end.  A diagonal row block then solves y_R = Linv_R z_R into x (block
-// product with warp-local slices, see blk_i) and releases flag R; rows at or
-// past w are the front's update vector for its parent.
+// the wait, and each lane waits for its own entry of y_b in the ready buffer
+// (no CTA barrier per tile); the four slices are added in order at the end.
+// A diagonal row block then solves y_R = Linv_R z_R into x and the ready
+// buffer (block product with warp-local slices, see blk_i); rows at or past
+// w are the front's update vector for its parent.
 __global__ void __launch_bounds__(kSolveThreads, 1)
     k_fwd_fronts(const SolveFront *fr, const int32_t *fmap, const int32_t *frow,
                  const float *panel, const double *linv64, const int64_t *gp,
                  const int64_t *gsrc, double *x, double *zbuf, int32_t *tickets,
-                 int32_t *flags, int32_t *err) {
+                 double *ready, int32_t *err) {
   extern __shared__ double tri[];  // kTri doubles: the staged Linv_R
   __shared__ double ys[4 * 33];
   __shared__ double ys2[4 * 33];
@@ -247,7 +279,8 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   const int     w = F.w;
   const int64_t r = static_cast<int64_t>(R) * kNB + rr;
   const float  *P  = panel + F.panel;
-  int32_t      *fl = flags + F.flag0;
+  const int64_t n  = F.n;
+  const double *yr = ready + ((item * 16 + threadIdx.x / 32) % kReadyCopies) * n + F.col0;
   const int     tiles = min(R, F.nb);
   // Right-hand side of this row: its entry of x (rows < w), then the
   // children's update vectors in child order.
@@ -263,9 +296,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
 #pragma unroll
     for (int k = 0; k < 32; k++)
       lv[k] = (r < h && c0 + k < w) ? __ldg(P + r + static_cast<int64_t>(c0 + k) * h) : 0.0f;
-    if (lane == 0) wait_flag(fl + b, err);
-    __syncwarp();
-    yw[warp][lane] = c0 + lane < w ? __ldcg(x + F.col0 + c0 + lane) : 0.0;
+    yw[warp][lane] = c0 + lane < w ? wait_value(yr + c0 + lane, err) : 0.0;
     __syncwarp();
 #pragma unroll
     for (int k = 0; k < 32; k++) acc += static_cast<double>(lv[k]) * yw[warp][k];
@@ -281,7 +312,12 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
     __syncthreads();
     const double y  = block_lower_apply(tri, ys, nbk);
     const int    iy = blk_i();
-    if (blk_q() == 0 && iy < nbk) x[F.col0 + R * kNB + iy] = y;
+    if (blk_q() == 0 && iy < nbk) {
+      const int64_t j = F.col0 + R * kNB + iy;
+#pragma unroll
+      for (int c = 0; c < kReadyCopies; c++) st_relaxed_f64(ready + c * n + j, y);
+      x[j] = y;
+    }
     if ((R + 1) * kNB > w && h > w) {
       // Rows of this block at or past w: their product with the block.
       if (blk_q() == 0) ys2[pad(iy)] = iy < nbk ? y : 0.0;
@@ -295,10 +331,6 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
       if (qq == 0 && r >= w && r < h)
         z -= (part[0][rr] + part[1][rr]) + (part[2][rr] + part[3][rr]);
     }
-    // The CTA's writes of y happen before thread 0's release store (bar.sync,
-    // then the release, which is cumulative).
-    __syncthreads();
-    if (tid == 0) st_release(fl + R, 1);
   }
   if (qq == 0 && r >= w && r < h) zbuf[F.zofs + r] = z;
 }
@@ -404,14 +436,14 @@ __global__ void __launch_bounds__(kSolveThreads)
 // Backward solve, column blocks of the large fronts of one level: one CTA
 // per column block b (last first).  t = (sum of the chunk partials, in chunk
 // order) + (sum over the row blocks R > b of the diagonal part, last first,
-// each as soon as x_R is ready); then x_b = Linv_b^T (z_b - t) into x and the
-// front vector, and flag b is released.  In a tile, warp v takes the
-// block's columns 8v .. 8v+7 and the lanes the rows.
+// each as soon as x_R is in the ready buffer); then x_b = Linv_b^T (z_b - t)
+// into x and the ready buffer.  In a tile, warp v takes the block's columns
+// 8v .. 8v+7 and the lanes the rows.
 __global__ void __launch_bounds__(kSolveThreads, 1)
     k_bwd_fronts(const SolveFront *fr, const int32_t *fmap, const float *panel,
                  const double *linv64t,
                  double *x, const double *part, int32_t *tickets,
-                 int32_t *flags, int32_t *err) {
+                 double *ready, int32_t *err) {
   extern __shared__ double tri[];  // kTri doubles: the staged Linv_b^T
   __shared__ double v[kNB];
   __shared__ double ts[kNB];
@@ -426,7 +458,8 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   const int         w = F.w;
   const int         nbk = min(kNB, w - b * kNB);
   const float      *P   = panel + F.panel;
-  int32_t          *fl  = flags + F.flag0;
+  const int64_t     n   = F.n;
+  const double     *xr  = ready + ((item * 16 + threadIdx.x / 32) % kReadyCopies) * n + F.col0;
   {
     // Chunk partials of column k (no wait needed): thread (q, k) adds chunks
     // q, q + 4, ...; the four sums are added in order below.
@@ -455,12 +488,10 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
                            : 0.0f;
       }
     }
-    if (lane == 0) wait_flag(fl + R, err);
-    __syncwarp();
 #pragma unroll
     for (int i = 0; i < 4; i++) {
       const int    rr = lane + 32 * i;
-      const double zv = rr < rows ? __ldcg(x + F.col0 + rb + rr) : 0.0;
+      const double zv = rr < rows ? wait_value(xr + rb + rr, err) : 0.0;
 #pragma unroll
       for (int j = 0; j < 8; j++) acc[j] += static_cast<double>(lv[j][i]) * zv;
     }
@@ -479,9 +510,12 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   __syncthreads();
   // Lt[i * kNB + j] = Linv[i][j]
   const double xb = block_upper_apply(tri, v, nbk, red);
-  if (tid < nbk) x[F.col0 + b * kNB + tid] = xb;
-  __syncthreads();
-  if (tid == 0) st_release(fl + b, 1);
+  if (tid < nbk) {
+    const int64_t j = F.col0 + b * kNB + tid;
+#pragma unroll
+    for (int c = 0; c < kReadyCopies; c++) st_relaxed_f64(ready + c * n + j, xb);
+    x[j] = xb;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -490,6 +524,7 @@ void SolveWorkspace::allocate(const Plan &P) {
   zbuf.resize(std::max<int64_t>(P.S.z_elems, 1) * sizeof(double));
   part.resize(std::max<int64_t>(P.spart_elems, 1) * sizeof(double));
   sync.resize(std::max<int64_t>(P.sync_elems, 1) * sizeof(int32_t));
+  ready.resize(std::max<int64_t>(kReadyCopies * P.S.n, 1) * sizeof(double));
   err.resize(sizeof(int32_t));
   MPIR_CUDA(cudaMemset(err.as<void>(), 0, sizeof(int32_t)));
   xbuf.resize(std::max<int64_t>(P.S.n, 1) * sizeof(double));
@@ -535,14 +570,17 @@ void ldlt_solve(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
   const double *lv  = F.linv64.as<double>();
   double      *zbuf = ws.zbuf.as<double>();
   const int    nl   = static_cast<int>(P.levels.size());
-  // Tickets (2 per level), then the forward and backward ready flags.
-  int32_t          *sync = ws.sync.as<int32_t>();
-  int32_t          *ffl  = sync + 2 * nl;
-  int32_t          *bfl  = ffl + P.nflags;
-  int32_t          *err  = ws.err.as<int32_t>();
-  const SolveFront *sf   = P.solve_fronts.as<SolveFront>();
-  if (P.nflags > 0)
-    MPIR_CUDA(cudaMemsetAsync(sync, 0, P.sync_elems * sizeof(int32_t), s));
+  // Tickets (2 per level); the ready buffer is marked pending before each
+  // direction.
+  int32_t          *sync  = ws.sync.as<int32_t>();
+  double           *ready = ws.ready.as<double>();
+  int32_t          *err   = ws.err.as<int32_t>();
+  const SolveFront *sf    = P.solve_fronts.as<SolveFront>();
+  const bool        block = P.nblock_fronts > 0;
+  const int64_t     nready = kReadyCopies * S.n;
+  const unsigned    nmark  = static_cast<unsigned>((nready + 255) / 256);
+  if (block) MPIR_CUDA(cudaMemsetAsync(sync, 0, P.sync_elems * sizeof(int32_t), s));
+  if (block && (phases & kForward)) launch(k_mark_pending, nmark, 256, 0, s, nready, ready);
   static bool attr = false;
   if (!attr) {
     MPIR_CUDA(cudaFuncSetAttribute(k_fwd_fronts, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -564,7 +602,7 @@ void ldlt_solve(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
       launch(k_fwd_fronts, L.fwd_items, kSolveThreads, kTri * sizeof(double), s, sf + L.sf_begin,
              P.fwd_map.as<int32_t>() + L.fwd_map0, P.fwd_row.as<int32_t>() + L.fwd_map0, pan,
              lv, P.gp.as<int64_t>(),
-             P.gsrc.as<int64_t>(), x, zbuf, sync + 2 * t, ffl, err);
+             P.gsrc.as<int64_t>(), x, zbuf, sync + 2 * t, ready, err);
     }
   }
   if (phases & kDiagonal)
@@ -574,6 +612,7 @@ void ldlt_solve(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
   if (!(phases & kBackward)) return;
   MPIR_CHECK_LAUNCH();
   kt.begin(kKcSolveBwd, s);
+  if (block) launch(k_mark_pending, nmark, 256, 0, s, nready, ready);
   for (int t = nl - 1; t >= 0; t--) {
     const LevelPlan &L = P.levels[t];
     if (L.sw_count > 0)
@@ -589,7 +628,7 @@ void ldlt_solve(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
       launch(k_bwd_fronts, L.bwd_owner_items, kSolveThreads, kTri * sizeof(double), s,
              sf + L.sf_begin, P.own_map.as<int32_t>() + L.own_map0, pan,
              F.linv64t.as<double>(), x,
-             static_cast<const double *>(ws.part.as<double>()), sync + 2 * t + 1, bfl, err);
+             static_cast<const double *>(ws.part.as<double>()), sync + 2 * t + 1, ready, err);
     }
   }
   kt.end(s);

@@ -9,8 +9,10 @@ namespace mpir {
 struct SolveWorkspace {
   DeviceBuffer zbuf;      // front vectors, zofs layout (doubles)
   DeviceBuffer part;      // backward chunk partial sums (doubles)
-  DeviceBuffer sync;      // tickets and ready flags (Plan::sync_elems int32)
-  DeviceBuffer err;       // int32, set to 1 when a ready-flag wait gave up
+  DeviceBuffer sync;      // tickets (Plan::sync_elems int32)
+  DeviceBuffer ready;     // block results for the CTAs that wait on them (n
+                          // doubles, the pending marker until written)
+  DeviceBuffer err;       // int32, set to 1 when a bounded wait gave up
   DeviceBuffer xbuf;      // fixed vector the captured solve works on
   cudaGraphExec_t graph = nullptr;  // captured L D L^T solve (all phases)
   int64_t graph_launches = 0;       // kernels one replay runs
