@@ -146,6 +146,12 @@ class Numeric {
   DeviceBuffer AD, Axs, Kval, Korig, Ax;
   double       eps_uf = 0;
   bool         valid  = false;
+  // Captured factorization (run_graph) and what it was captured for.
+  cudaGraphExec_t graph          = nullptr;
+  const double   *graph_ax       = nullptr;
+  double          graph_eps      = 0;
+  int             graph_mode     = -2;
+  int64_t         graph_launches = 0;
   // Trailing-update engine: -1 float32 SIMT, 0 bfloat16 tensor cores,
   // 1 3xTF32 tensor cores, 2 float16 tensor cores.
   int          update_mode = -1;
@@ -153,6 +159,13 @@ class Numeric {
   void allocate(const Plan &P);
   // Scale the caller's values (device, caller order), assemble and factor.
   void run(const Plan &P, const double *d_Ax, double eps_uf, cudaStream_t s);
+  // The same, replayed from a CUDA graph captured on capture_stream at the
+  // first call (and again when d_Ax, eps_uf or the update engine change); the
+  // plain launches when the per-class kernel timer is on.
+  void run_graph(const Plan &P, const double *d_Ax, double eps_uf, cudaStream_t s,
+                 cudaStream_t capture_stream);
+  void release_graph();
+  ~Numeric() { release_graph(); }
   // Reads the status; returns #positive D, -1 on a zero pivot or -5 when a
   // bounded device wait ran out.
   int64_t result(cudaStream_t s, int32_t *zero_col = nullptr,

@@ -1213,6 +1213,7 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
 }
 
 void Numeric::allocate(const Plan &P) {
+  release_graph();
   const Symbolic &S = P.S;
   panel.resize(std::max<int64_t>(S.panel_elems, 1) * sizeof(float));
   uarena.resize(std::max<int64_t>(S.uarena_elems, 1) * sizeof(float));
@@ -1242,14 +1243,57 @@ static unsigned grid_for(int64_t n, int threads) {
   return static_cast<unsigned>((n + threads - 1) / threads);
 }
 
+__global__ void k_status_reset(FactorStatus *st) {
+  if (threadIdx.x == 0) *st = FactorStatus{INT_MAX, 0, 0, 0};
+}
+
+void Numeric::release_graph() {
+  if (graph) cudaGraphExecDestroy(graph);
+  graph = nullptr;
+}
+
+void Numeric::run_graph(const Plan &P, const double *d_Ax, double eps, cudaStream_t s,
+                        cudaStream_t capture_stream) {
+  if (kernel_timer().enabled || P.S.n == 0) {  // per-class timing needs the plain launches
+    run(P, d_Ax, eps, s);
+    return;
+  }
+  if (!graph || graph_ax != d_Ax || graph_eps != eps || graph_mode != update_mode) {
+    release_graph();
+    cudaGraph_t g = nullptr;
+    MPIR_CUDA(cudaStreamSynchronize(capture_stream));
+    MPIR_CUDA(cudaStreamBeginCapture(capture_stream, cudaStreamCaptureModeThreadLocal));
+    const int64_t before = launch_counter();
+    try {
+      run(P, d_Ax, eps, capture_stream);
+    } catch (...) {
+      cudaStreamEndCapture(capture_stream, &g);
+      if (g) cudaGraphDestroy(g);
+      launch_counter() = before;
+      throw;
+    }
+    MPIR_CUDA(cudaStreamEndCapture(capture_stream, &g));
+    graph_launches   = launch_counter() - before;
+    launch_counter() = before;
+    const cudaError_t e = cudaGraphInstantiate(&graph, g, 0);
+    cudaGraphDestroy(g);
+    MPIR_CUDA(e);
+    graph_ax   = d_Ax;
+    graph_eps  = eps;
+    graph_mode = update_mode;
+  }
+  eps_uf = eps;
+  MPIR_CUDA(cudaGraphLaunch(graph, s));
+  launch_counter() += graph_launches;
+  valid = true;
+}
+
 void Numeric::run(const Plan &P, const double *d_Ax, double eps, cudaStream_t s) {
   const Symbolic &S  = P.S;
   KernelTimer    &kt = kernel_timer();
   eps_uf             = eps;
   valid              = false;
-  FactorStatus init{INT_MAX, 0, 0, 0};
-  MPIR_CUDA(cudaMemcpyAsync(status.as<void>(), &init, sizeof init,
-                            cudaMemcpyHostToDevice, s));
+  launch(k_status_reset, 1, 32, 0, s, status.as<FactorStatus>());
   MPIR_CUDA(cudaMemsetAsync(panel.as<void>(), 0, S.panel_elems * sizeof(float), s));
   if (S.n == 0) return;
   kt.begin(kKcScatter, s);

@@ -112,7 +112,7 @@ int Solver::factor_device(const double *d_Ax) {
   if (!plan_) throw std::logic_error("factor before analyze");
   MPIR_CUDA(cudaSetDevice(device));
   MPIR_CUDA(cudaEventRecord(ev0_, stream_));
-  num_.run(*plan_, d_Ax, eps_of(uf), stream_);
+  num_.run_graph(*plan_, d_Ax, eps_of(uf), stream_, own_stream_);
   MPIR_CUDA(cudaEventRecord(ev1_, stream_));
   int32_t zc  = 0;
   bool    bad = false;
