@@ -290,17 +290,28 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
     for (int64_t e = gp[F.gptr + r]; e < gp[F.gptr + r + 1]; e++) zr += zbuf[gsrc[e]];
   }
   double acc = 0.0;
-  for (int b = 0; b < tiles; b++) {
+  // The next tile's L values are loaded while the current one waits for y_b
+  // and is applied: two tiles in flight, so a CTA that starts late (when an
+  // earlier one leaves its SM) catches up on the tiles already available at
+  // about twice the rate of one tile at a time.
+  float lv[32], lvn[32];
+  auto  load_tile = [&](float (&dst)[32], int b) {
     const int c0 = b * kNB + qq * 32;
-    float     lv[32];
 #pragma unroll
     for (int k = 0; k < 32; k++)
-      lv[k] = (r < h && c0 + k < w) ? __ldg(P + r + static_cast<int64_t>(c0 + k) * h) : 0.0f;
+      dst[k] = (r < h && c0 + k < w) ? __ldg(P + r + static_cast<int64_t>(c0 + k) * h) : 0.0f;
+  };
+  if (tiles > 0) load_tile(lv, 0);
+  for (int b = 0; b < tiles; b++) {
+    const int c0 = b * kNB + qq * 32;
+    if (b + 1 < tiles) load_tile(lvn, b + 1);
     yw[warp][lane] = c0 + lane < w ? wait_value(yr + c0 + lane, err) : 0.0;
     __syncwarp();
 #pragma unroll
     for (int k = 0; k < 32; k++) acc += static_cast<double>(lv[k]) * yw[warp][k];
     __syncwarp();
+#pragma unroll
+    for (int k = 0; k < 32; k++) lv[k] = lvn[k];
   }
   part[qq][rr] = acc;
   __syncthreads();
@@ -473,21 +484,30 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   double acc[8];
 #pragma unroll
   for (int j = 0; j < 8; j++) acc[j] = 0.0;
-  for (int R = F.nb - 1; R > b; R--) {
+  // Tile R (the warp's columns 8 warp + j, rows lane + 32 i of row block R);
+  // the next tile (R - 1) is loaded while the current one waits for x_R and
+  // is applied, as in the forward solve.
+  float lv[8][4], lvn[8][4];
+  auto  load_tile = [&](float (&dst)[8][4], int R) {
     const int64_t rb   = static_cast<int64_t>(R) * kNB;
     const int     rows = min(kNB, w - R * kNB);
-    float lv[8][4];
 #pragma unroll
     for (int j = 0; j < 8; j++) {
       const int c = warp * 8 + j;
 #pragma unroll
       for (int i = 0; i < 4; i++) {
         const int rr = lane + 32 * i;
-        lv[j][i]     = (c < nbk && rr < rows)
+        dst[j][i]    = (c < nbk && rr < rows)
                            ? __ldg(P + rb + rr + static_cast<int64_t>(b * kNB + c) * h)
                            : 0.0f;
       }
     }
+  };
+  if (F.nb - 1 > b) load_tile(lv, F.nb - 1);
+  for (int R = F.nb - 1; R > b; R--) {
+    const int64_t rb   = static_cast<int64_t>(R) * kNB;
+    const int     rows = min(kNB, w - R * kNB);
+    if (R - 1 > b) load_tile(lvn, R - 1);
 #pragma unroll
     for (int i = 0; i < 4; i++) {
       const int    rr = lane + 32 * i;
@@ -495,6 +515,10 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
 #pragma unroll
       for (int j = 0; j < 8; j++) acc[j] += static_cast<double>(lv[j][i]) * zv;
     }
+#pragma unroll
+    for (int j = 0; j < 8; j++)
+#pragma unroll
+      for (int i = 0; i < 4; i++) lv[j][i] = lvn[j][i];
   }
 #pragma unroll
   for (int j = 0; j < 8; j++) {
