@@ -739,13 +739,18 @@ __global__ void __launch_bounds__(kGemmThreads)
   }
 }
 
-// C -= sum of the split partials of one tile, added in split order.  Thread
-// t takes 4 consecutive rows of a column (one float4 of each partial) and
-// four such groups at once, so 16 loads per split are in flight.
+// C -= sum of the split partials of one tile, added in split order.  A tile
+// is reduced by kReduceSlices CTAs, one float4 group (4 consecutive rows of a
+// column) per thread: the late left-looking steps of a large front have a
+// few tiles and many splits, so one CTA per tile would sum long chains
+// alone.  The partials are loaded four splits at a time and added in order.
+constexpr int kReduceSlices = 16;
+
 __global__ void __launch_bounds__(256)
     k_split_reduce(const GemmProb *probs, int nprob, float *panel, float *uarena,
                    const float *ws) {
-  const int t  = blockIdx.x;
+  static_assert(kBM * kBN / 4 == kReduceSlices * 256, "one float4 group per thread");
+  const int t = blockIdx.x / kReduceSlices, slice = blockIdx.x % kReduceSlices;
   int       lo = 0, hi = nprob - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) / 2;
@@ -754,49 +759,47 @@ __global__ void __launch_bounds__(256)
   const GemmProb pb = probs[lo];
   int            sp, tile, m0, n0;
   locate_tile(pb, (t - pb.rtile0) * pb.splits, sp, tile, m0, n0);
-  float       *C = (pb.c_in_u ? uarena : panel) + pb.c_ofs;
-  const float *W = ws + pb.ws_ofs + static_cast<int64_t>(tile) * pb.splits * (kBM * kBN);
-  constexpr int kGroups = kBM * kBN / 4;  // float4 groups of a tile
-#pragma unroll 1
-  for (int g0 = threadIdx.x; g0 < kGroups; g0 += 4 * 256) {
-    float4 acc[4];
+  float         *C  = (pb.c_in_u ? uarena : panel) + pb.c_ofs;
+  const int      g  = slice * 256 + threadIdx.x;
+  const float4  *W  = reinterpret_cast<const float4 *>(
+                         ws + pb.ws_ofs + static_cast<int64_t>(tile) * pb.splits * (kBM * kBN)) + g;
+  constexpr int  kT = kBM * kBN / 4;  // float4 groups of a tile
+  float4         acc = make_float4(0.f, 0.f, 0.f, 0.f);
+  int            q   = 0;
+  for (; q + 4 <= pb.splits; q += 4) {
+    float4 v[4];
 #pragma unroll
-    for (int u = 0; u < 4; u++) acc[u] = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (int q = 0; q < pb.splits; q++) {
-      const float4 *Wq = reinterpret_cast<const float4 *>(W + static_cast<int64_t>(q) * (kBM * kBN));
-#pragma unroll
-      for (int u = 0; u < 4; u++) {
-        const float4 v = __ldcs(Wq + g0 + u * 256);
-        acc[u].x += v.x;
-        acc[u].y += v.y;
-        acc[u].z += v.z;
-        acc[u].w += v.w;
-      }
-    }
-    // All loads of C first, then the stores (one memory latency, not 16).
-    int64_t at[16];
-    float   cv[16];
+    for (int u = 0; u < 4; u++) v[u] = __ldcs(W + static_cast<int64_t>(q + u) * kT);
 #pragma unroll
     for (int u = 0; u < 4; u++) {
-      const int e = 4 * (g0 + u * 256);
-      const int c = n0 + e / kBM;
-#pragma unroll
-      for (int v = 0; v < 4; v++) {
-        const int m = m0 + e % kBM + v;
-        const int r = m < pb.M ? gemm_out_row(pb, m) : -1;
-        at[4 * u + v] = (r < 0 || c >= pb.N || (pb.lower && r < c)) ? -1
-                                                                       : r + (int64_t)c * pb.ldc;
-        cv[4 * u + v] = (!pb.c_in_u && at[4 * u + v] >= 0) ? C[at[4 * u + v]] : 0.0f;
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < 4; u++) {
-      const float a[4] = {acc[u].x, acc[u].y, acc[u].z, acc[u].w};
-#pragma unroll
-      for (int v = 0; v < 4; v++)
-        if (at[4 * u + v] >= 0) C[at[4 * u + v]] = cv[4 * u + v] - a[v];
+      acc.x += v[u].x;
+      acc.y += v[u].y;
+      acc.z += v[u].z;
+      acc.w += v[u].w;
     }
   }
+  for (; q < pb.splits; q++) {
+    const float4 v = __ldcs(W + static_cast<int64_t>(q) * kT);
+    acc.x += v.x;
+    acc.y += v.y;
+    acc.z += v.z;
+    acc.w += v.w;
+  }
+  const int   e = 4 * g;
+  const int   c = n0 + e / kBM;
+  int64_t     at[4];
+  float       cv[4];
+  const float a[4] = {acc.x, acc.y, acc.z, acc.w};
+#pragma unroll
+  for (int v = 0; v < 4; v++) {
+    const int m = m0 + e % kBM + v;
+    const int r = m < pb.M ? gemm_out_row(pb, m) : -1;
+    at[v] = (r < 0 || c >= pb.N || (pb.lower && r < c)) ? -1 : r + (int64_t)c * pb.ldc;
+    cv[v] = (!pb.c_in_u && at[v] >= 0) ? C[at[v]] : 0.0f;
+  }
+#pragma unroll
+  for (int v = 0; v < 4; v++)
+    if (at[v] >= 0) C[at[v]] = cv[v] - a[v];
 }
 
 // Inverses, in float64, of the unit-lower diagonal blocks of the large
@@ -1360,7 +1363,7 @@ void Numeric::run(const Plan &P, const double *d_Ax, double eps, cudaStream_t s)
                        packd.as<float>(), packd.as<float>() + P.pd_elems, bconv.as<float>(),
                        pan, ua, ws.as<float>(), st, s);
       if (rtiles > 0)
-        launch(k_split_reduce, rtiles, 256, 0, s, gp + begin, count, pan, ua,
+        launch(k_split_reduce, rtiles * kReduceSlices, 256, 0, s, gp + begin, count, pan, ua,
                static_cast<const float *>(ws.as<float>()));
       kt.end(s);
     };
