@@ -139,7 +139,7 @@ struct GemmProb {
   int64_t bc, bc_lo, bprow;
   int32_t btiles, bgroups, cv0;
 };
-constexpr int kConvGroups = 32;  // K-groups per conversion CTA
+constexpr int kConvGroups = 8;   // K-groups per conversion CTA (4 per thread)
 
 // Extend-add task: add the lower triangle of child C's update matrix into
 // its parent's front, CTA-chunked by columns of U_C.

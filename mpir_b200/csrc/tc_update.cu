@@ -579,13 +579,27 @@ __global__ void __launch_bounds__(256)
   const int       g0     = (local % chunks) * kConvGroups;
   const int       g1     = min(g0 + kConvGroups, pb.bgroups);
   const int       m      = threadIdx.x % 128;
-  for (int g = g0 + threadIdx.x / 128; g < g1; g += 2) {
-    const float4 b = *reinterpret_cast<const float4 *>(
-        pack + pb.pb + static_cast<int64_t>(tile) * pb.prow +
-        static_cast<int64_t>(g) * PackedFront::kGroupFloats + m * 4);
-    const float4 d     = *reinterpret_cast<const float4 *>(packd + pb.pd + 4 * g);
-    const float  bv[4] = {b.x * d.x, b.y * d.y, b.z * d.z, b.w * d.w};
-    uint4        bh, bl;
+  // All loads of the thread's K-groups first, then the stores (the
+  // conversion buffer and the packed fronts are separate arrays, but the
+  // compiler cannot tell).
+  constexpr int kPer = kConvGroups / 2;
+  float4        b[kPer], d[kPer];
+#pragma unroll
+  for (int u = 0; u < kPer; u++) {
+    const int g = g0 + threadIdx.x / 128 + 2 * u;
+    if (g < g1) {
+      b[u] = *reinterpret_cast<const float4 *>(
+          pack + pb.pb + static_cast<int64_t>(tile) * pb.prow +
+          static_cast<int64_t>(g) * PackedFront::kGroupFloats + m * 4);
+      d[u] = *reinterpret_cast<const float4 *>(packd + pb.pd + 4 * g);
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < kPer; u++) {
+    const int g = g0 + threadIdx.x / 128 + 2 * u;
+    if (g >= g1) continue;
+    const float bv[4] = {b[u].x * d[u].x, b[u].y * d[u].y, b[u].z * d[u].z, b[u].w * d[u].w};
+    uint4       bh, bl;
     split4(bv, bh, bl);
     const int64_t o = static_cast<int64_t>(tile) * pb.bprow +
                       static_cast<int64_t>(g) * PackedFront::kGroupFloats + m * 4;
