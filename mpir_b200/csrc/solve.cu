@@ -468,6 +468,8 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   const int64_t     h = F.h;
   const int         w = F.w;
   const int         nbk = min(kNB, w - b * kNB);
+  // This block's right-hand side, read now (not on the chain at the end).
+  if (tid < nbk) v[tid] = x[F.col0 + b * kNB + tid];
   const float      *P   = panel + F.panel;
   const int64_t     n   = F.n;
   const double     *xr  = ready + ((item * 16 + threadIdx.x / 32) % kReadyCopies) * n + F.col0;
@@ -529,8 +531,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   }
   __syncthreads();
   if (tid < nbk)
-    v[tid] = x[F.col0 + b * kNB + tid] -
-             (((red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid])) + ts[tid]);
+    v[tid] = v[tid] - (((red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid])) + ts[tid]);
   __syncthreads();
   // Lt[i * kNB + j] = Linv[i][j]
   const double xb = block_upper_apply(tri, v, nbk, red);
