@@ -244,19 +244,22 @@ __global__ void __launch_bounds__(kRedThreads)
     }
   }
   if (!last_block(count)) return;
-  if (threadIdx.x == 0) {
-    if (mode == 0) {
-      double t = 0.0;
-      for (unsigned b = 0; b < gridDim.x; b++) t += __ldcg(part + b);
-      *out = t;
-    } else {
-      double s = 0.0, q = 1.0;
-      for (unsigned b = 0; b < gridDim.x; b++)
-        ssq_merge(s, q, __ldcg(part + 2 * b), __ldcg(part + 2 * b + 1));
-      *out = s * sqrt(q);
-    }
-    *count = 0;
+  // The last block adds the blocks' partials: thread j takes partials j,
+  // j + blockDim.x, ... in that order, then the fixed tree of the block
+  // reductions (the loads are independent, so none waits for another).
+  if (mode == 0) {
+    double t = 0.0;
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) t += __ldcg(part + b);
+    t = block_sum(t, sh);
+    if (threadIdx.x == 0) *out = t;
+  } else {
+    double s = 0.0, q = 1.0;
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+      ssq_merge(s, q, __ldcg(part + 2 * b), __ldcg(part + 2 * b + 1));
+    block_ssq(s, q, sh);
+    if (threadIdx.x == 0) *out = s * sqrt(q);
   }
+  if (threadIdx.x == 0) *count = 0;
 }
 
 // y = a * x (a read from the host argument).
