@@ -260,7 +260,7 @@ int mpir_analyze_host(int64_t n, const int64_t *Ap, const int64_t *Ai,
 /* ---- Kernel timing (benchmark support) ----------------------------------- */
 /* Classes: 0 small fronts, 1 diagonal blocks, 2 panel solve, 3 trailing
  * update, 4 extend-add, 5 zero fill, 6 scatter, 7 forward solve, 8 backward
- * solve, 9 SpMV, 10 vector. */
+ * solve, 9 SpMV, 10 vector, 11 split-K reduction of the updates. */
 int mpir_kernel_timer_enable(int on);
 /* Kernel launches this library has issued in this process. */
 int64_t mpir_launch_count(void);

@@ -423,7 +423,8 @@ def analyze_host(Ap, Ai, Ax=None, ordering=ORDER_AUTO, pattern=False):
 
 
 KERNEL_CLASSES = ["small_front", "diag_block", "panel_solve", "trailing_update", "extend_add",
-                  "zero_fill", "scatter", "solve_forward", "solve_backward", "spmv", "vector"]
+                  "zero_fill", "scatter", "solve_forward", "solve_backward", "spmv", "vector",
+                  "split_reduce"]
 
 
 def launch_count() -> int:

@@ -171,6 +171,9 @@ constexpr int kSmallThreads = 256;
 constexpr int kDiagThreads  = 512;
 constexpr int kGemmThreads  = 256;
 constexpr int kEaChunk      = 8;     // U_C columns per extend-add CTA
+// A parent whose children's update matrices hold at most kEaSeqWork entries
+// in all is extended by one CTA (its children in order) instead of rounds.
+constexpr int64_t kEaSeqWork = int64_t{1} << 16;
 constexpr int kSolveRows = 128;        // rows per forward-solve CTA
 constexpr int kSolveChunk = 128;       // rows per backward-solve CTA
 constexpr int kSolveThreads = 512;     // 4 column quarters x 128 rows

@@ -71,6 +71,9 @@ struct LevelPlan {
     int32_t begin, count, chunks;
   };
   std::vector<Round> ea_rounds;
+  // Parents extended by one CTA each: [ea_seq_begin, + ea_seq_count) of the
+  // plan's ea_seq (task begin, task end) pairs.
+  int32_t ea_seq_begin = 0, ea_seq_count = 0;
   struct Step {
     int32_t begin, count, trsm_tiles, upd_tiles;
     // left-looking update of this block column before its diagonal block
@@ -107,6 +110,7 @@ class Plan {
   DeviceBuffer amap, arow, acol, diag_pos, Kp, Kj, Ksrc;
   DeviceBuffer sfirst, srowptr, srows, srel, slofs, uofs, zofs, child_ptr,
       child_list, perm;
+  DeviceBuffer ea_seq;  // int32 pairs, see LevelPlan::ea_seq_begin
   DeviceBuffer small_list, large_list, steps, ea_tasks, linv_ofs_d, gemm_probs,
       solve_fronts, swarp_list, sblock_list, gp, gsrc, fwd_map, fwd_row, chunk_map, own_map;
   int64_t      ws_elems = 0;  // split-K partial tiles (floats)
@@ -209,6 +213,7 @@ enum KernelClass : int {
   kKcSolveBwd,
   kKcSpmv,
   kKcVec,
+  kKcReduce,
   kKcCount
 };
 KernelTimer &kernel_timer();

@@ -207,6 +207,51 @@ __global__ void k_extend_add(const EaTask *tasks, int ntasks,
   }
 }
 
+// Extend-add for parents with only small children: CTA p takes parent p's
+// tasks (children) in order, a barrier between them (siblings may add to the
+// same entries; the order is the rounds' order, child order).  Within a
+// task warp v takes the 8-column chunks v, v + 8, ..., its lanes the rows.
+__global__ void __launch_bounds__(256)
+    k_extend_add_seq(const int32_t *seq, const EaTask *tasks, const int32_t *srel,
+                     float *panel, float *uarena, int phase) {
+  const int t0 = seq[2 * blockIdx.x], t1 = seq[2 * blockIdx.x + 1];
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  for (int ti = t0; ti < t1; ti++) {
+    const EaTask   tk = tasks[ti];
+    const int32_t *rl = srel + tk.rel;
+    const float   *U  = uarena + tk.child_u;
+    const int      rp = tk.hp - tk.wp;
+    for (int b0 = warp * kEaChunk; b0 < tk.rc; b0 += 8 * kEaChunk) {
+      const int nb = min(kEaChunk, tk.rc - b0);
+      float    *dst[kEaChunk];
+      int       off[kEaChunk];
+      bool      act[kEaChunk];
+#pragma unroll
+      for (int u = 0; u < kEaChunk; u++) {
+        const int cb = u < nb ? rl[b0 + u] : 0;
+        dst[u]       = cb < tk.wp ? panel + tk.parent_panel + (int64_t)cb * tk.hp
+                                  : uarena + tk.parent_u + (int64_t)(cb - tk.wp) * rp;
+        off[u]       = cb < tk.wp ? 0 : tk.wp;
+        act[u]       = u < nb && (phase == 1 ? cb < tk.wp : cb >= tk.wp);
+      }
+      for (int a = b0 + lane; a < tk.rc; a += 32) {
+        const int ra = rl[a];
+        float     v[kEaChunk], o[kEaChunk];
+#pragma unroll
+        for (int u = 0; u < kEaChunk; u++) {
+          const bool ok = act[u] && a >= b0 + u;
+          v[u]          = ok ? U[a + (int64_t)(b0 + u) * tk.rc] : 0.0f;
+          o[u]          = ok ? dst[u][ra - off[u]] : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < kEaChunk; u++)
+          if (act[u] && a >= b0 + u) dst[u][ra - off[u]] = o[u] + v[u];
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Diagonal block of one step: LDL^T of the nbk x nbk block (nbk <= 128) and
 // the inverse X = L^{-1} of its unit-lower factor, right-looking by panels of
@@ -889,6 +934,7 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
   h_large.clear();
   std::vector<StepDesc> descs;
   std::vector<EaTask>   tasks;
+  std::vector<int32_t>  seq_h;
   std::vector<GemmProb> probs;
   ws_elems    = 0;
   bconv_elems = 0;
@@ -974,30 +1020,53 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
     }
     L.small_count = static_cast<int32_t>(h_small.size()) - L.small_begin;
     L.large_count = static_cast<int32_t>(h_large.size()) - L.large_begin;
-    // Extend-add rounds for the large fronts (round q = q-th child).
+    // Extend-add: parents with only small children get one CTA each (their
+    // children in order); the others go by rounds (round q = q-th child).
+    auto ea_task = [&](int64_t P, int64_t C) {
+      EaTask tk;
+      tk.child_u      = S.uofs[C];
+      tk.parent_panel = S.slofs[P];
+      tk.parent_u     = S.uofs[P];
+      tk.rel          = S.srowptr[C] + S.w(C);
+      tk.rc           = static_cast<int32_t>(S.h(C) - S.w(C));
+      tk.hp           = static_cast<int32_t>(S.h(P));
+      tk.wp           = static_cast<int32_t>(S.w(P));
+      tk.chunk0       = 0;
+      return tk;
+    };
+    std::vector<char> seq_parent(L.large_count, 0);
+    L.ea_seq_begin = static_cast<int32_t>(seq_h.size() / 2);
+    for (int32_t q = L.large_begin; q < L.large_begin + L.large_count; q++) {
+      const int64_t P    = h_large[q];
+      int64_t       work = 0;
+      for (int64_t c = S.child_ptr[P]; c < S.child_ptr[P + 1]; c++) {
+        const int64_t rc = S.h(S.child_list[c]) - S.w(S.child_list[c]);
+        work += rc * (rc + 1) / 2;
+      }
+      if (S.child_ptr[P + 1] - S.child_ptr[P] < 2 || work > kEaSeqWork) continue;
+      seq_parent[q - L.large_begin] = 1;
+      seq_h.push_back(static_cast<int32_t>(tasks.size()));
+      for (int64_t c = S.child_ptr[P]; c < S.child_ptr[P + 1]; c++)
+        tasks.push_back(ea_task(P, S.child_list[c]));
+      seq_h.push_back(static_cast<int32_t>(tasks.size()));
+    }
+    L.ea_seq_count = static_cast<int32_t>(seq_h.size() / 2) - L.ea_seq_begin;
     int64_t maxkids = 0;
     for (int32_t q = L.large_begin; q < L.large_begin + L.large_count; q++) {
       const int64_t J = h_large[q];
-      maxkids = std::max(maxkids, S.child_ptr[J + 1] - S.child_ptr[J]);
+      if (!seq_parent[q - L.large_begin])
+        maxkids = std::max(maxkids, S.child_ptr[J + 1] - S.child_ptr[J]);
     }
     for (int64_t round = 0; round < maxkids; round++) {
       LevelPlan::Round R{static_cast<int32_t>(tasks.size()), 0, 0};
       int32_t          ch = 0;
       for (int32_t q = L.large_begin; q < L.large_begin + L.large_count; q++) {
         const int64_t P = h_large[q];
+        if (seq_parent[q - L.large_begin]) continue;
         if (S.child_ptr[P] + round >= S.child_ptr[P + 1]) continue;
-        const int64_t C  = S.child_list[S.child_ptr[P] + round];
-        const int64_t rc = S.h(C) - S.w(C);
-        EaTask        tk;
-        tk.child_u      = S.uofs[C];
-        tk.parent_panel = S.slofs[P];
-        tk.parent_u     = S.uofs[P];
-        tk.rel          = S.srowptr[C] + S.w(C);
-        tk.rc           = static_cast<int32_t>(rc);
-        tk.hp           = static_cast<int32_t>(S.h(P));
-        tk.wp           = static_cast<int32_t>(S.w(P));
-        tk.chunk0       = ch;
-        ch += static_cast<int32_t>((rc + kEaChunk - 1) / kEaChunk);
+        EaTask tk = ea_task(P, S.child_list[S.child_ptr[P] + round]);
+        tk.chunk0 = ch;
+        ch += (tk.rc + kEaChunk - 1) / kEaChunk;
         tasks.push_back(tk);
       }
       R.count  = static_cast<int32_t>(tasks.size()) - R.begin;
@@ -1200,6 +1269,7 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
   large_list = upload(h_large, s);
   steps      = upload(descs, s);
   ea_tasks   = upload(tasks, s);
+  ea_seq     = upload(seq_h, s);
   gemm_probs = upload(probs, s);
   linv_ofs_d = upload(linv_ofs, s);
   solve_fronts = upload(sfronts, s);
@@ -1330,6 +1400,14 @@ void Numeric::run(const Plan &P, const double *d_Ax, double eps, cudaStream_t s)
     // Children's update matrices into the fronts' panels (the update
     // matrices' own columns follow after the product that defines them).
     auto extend_add = [&](int phase) {
+      if (L.ea_seq_count > 0) {
+        kt.begin(kKcExtendAdd, s);
+        launch(k_extend_add_seq, L.ea_seq_count, 256, 0, s,
+               P.ea_seq.as<int32_t>() + 2 * L.ea_seq_begin,
+               static_cast<const EaTask *>(P.ea_tasks.as<EaTask>()), P.srel.as<int32_t>(), pan,
+               ua, phase);
+        kt.end(s);
+      }
       for (const auto &R : L.ea_rounds) {
         kt.begin(kKcExtendAdd, s);
         launch(k_extend_add, R.chunks, 256, 0, s, P.ea_tasks.as<EaTask>() + R.begin, R.count,
@@ -1362,10 +1440,13 @@ void Numeric::run(const Plan &P, const double *d_Ax, double eps, cudaStream_t s)
         launch_gemm_tc(update_mode, gp + begin, count, tiles, pack.as<float>(),
                        packd.as<float>(), packd.as<float>() + P.pd_elems, bconv.as<float>(),
                        pan, ua, ws.as<float>(), st, s);
-      if (rtiles > 0)
-        launch(k_split_reduce, rtiles * kReduceSlices, 256, 0, s, gp + begin, count, pan, ua,
-               static_cast<const float *>(ws.as<float>()));
       kt.end(s);
+      if (rtiles > 0) {
+        kt.begin(kKcReduce, s);
+        launch(k_split_reduce, rtiles * kReduceSlices, 256, 0, s, gp + begin, count,
+               pan, ua, static_cast<const float *>(ws.as<float>()));
+        kt.end(s);
+      }
     };
     for (const auto &stp : L.steps) {
       const StepDesc *dd = P.steps.as<StepDesc>() + stp.begin;
