@@ -233,6 +233,13 @@ __device__ __forceinline__ double wait_value(const double *p, int32_t *err) {
   return 0.0;
 }
 
+// The value at p from a load issued ahead (raw) when that load already saw
+// it, else the wait for it.
+__device__ __forceinline__ double take_value(unsigned long long raw, const double *p,
+                                             int32_t *err) {
+  return raw != kPending ? __longlong_as_double(static_cast<long long>(raw)) : wait_value(p, err);
+}
+
 __global__ void k_mark_pending(int64_t n, double *ready) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) reinterpret_cast<unsigned long long *>(ready)[i] = kPending;
@@ -301,17 +308,31 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
     for (int k = 0; k < 32; k++)
       dst[k] = (r < h && c0 + k < w) ? __ldg(P + r + static_cast<int64_t>(c0 + k) * h) : 0.0f;
   };
-  if (tiles > 0) load_tile(lv, 0);
+  // The lane's entry of y_b is loaded ahead with the tile's L values too;
+  // only an entry that was still pending then is waited for.
+  auto load_y = [&](int b) {
+    const int c0 = b * kNB + qq * 32;
+    return c0 + lane < w ? ld_relaxed_u64(yr + c0 + lane) : 0ull;
+  };
+  unsigned long long yv = 0ull, yvn = 0ull;
+  if (tiles > 0) {
+    load_tile(lv, 0);
+    yv = load_y(0);
+  }
   for (int b = 0; b < tiles; b++) {
     const int c0 = b * kNB + qq * 32;
-    if (b + 1 < tiles) load_tile(lvn, b + 1);
-    yw[warp][lane] = c0 + lane < w ? wait_value(yr + c0 + lane, err) : 0.0;
+    if (b + 1 < tiles) {
+      load_tile(lvn, b + 1);
+      yvn = load_y(b + 1);
+    }
+    yw[warp][lane] = c0 + lane < w ? take_value(yv, yr + c0 + lane, err) : 0.0;
     __syncwarp();
 #pragma unroll
     for (int k = 0; k < 32; k++) acc += static_cast<double>(lv[k]) * yw[warp][k];
     __syncwarp();
 #pragma unroll
     for (int k = 0; k < 32; k++) lv[k] = lvn[k];
+    yv = yvn;
   }
   part[qq][rr] = acc;
   __syncthreads();
