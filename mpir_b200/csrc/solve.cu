@@ -274,9 +274,19 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   __shared__ double ys2[4 * 33];
   __shared__ double yw[kSolveThreads / 32][32];
   __shared__ double part[4][kNB];
-  const int         item = take_ticket(tickets);
-  const SolveFront  F    = fr[fmap[item]];
-  const int         R    = frow[item];
+  // The front's descriptor sits in shared memory: the code after the tile
+  // loop (on the chain of diagonal blocks) reads its fields again, and from
+  // global memory that took a round trip past an L1 the tiles had flushed.
+  __shared__ SolveFront sF;
+  __shared__ int        sR;
+  const int             item = take_ticket(tickets);
+  if (threadIdx.x == 0) {
+    sF = fr[fmap[item]];
+    sR = frow[item];
+  }
+  __syncthreads();
+  const SolveFront &F = sF;
+  const int         R = sR;
   if (R < F.nb)
     stage_lower(linv64 + F.linv + static_cast<int64_t>(R) * kNB * kNB, tri,
                 min(kNB, F.w - R * kNB));
@@ -480,9 +490,13 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   __shared__ double v[kNB];
   __shared__ double ts[kNB];
   __shared__ double red[4][kNB];
-  const int         item = take_ticket(tickets);
-  const SolveFront  F    = fr[fmap[item]];
-  const int         b    = F.nb - 1 - (item - F.own0);
+  // The front's descriptor sits in shared memory (see k_fwd_fronts).
+  __shared__ SolveFront sF;
+  const int             item = take_ticket(tickets);
+  if (threadIdx.x == 0) sF = fr[fmap[item]];
+  __syncthreads();
+  const SolveFront &F = sF;
+  const int         b = F.nb - 1 - (item - F.own0);
   stage_upper(linv64t + F.linv + static_cast<int64_t>(b) * kNB * kNB, tri,
               min(kNB, F.w - b * kNB));
   const int         tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
