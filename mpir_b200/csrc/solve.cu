@@ -233,6 +233,35 @@ __device__ __forceinline__ double wait_value(const double *p, int32_t *err) {
   return 0.0;
 }
 
+// Waits for this lane's entries p[lane + 32 i] (i < 4) of a block result, the
+// entries at or past lim reading as 0; each round polls all four at once.
+__device__ __forceinline__ void wait_block4(const double *p, int lim, double (&v)[4],
+                                            int32_t *err) {
+  const int lane = threadIdx.x % 32;
+  unsigned  need = 0;
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    v[i] = 0.0;
+    if (lane + 32 * i < lim) need |= 1u << i;
+  }
+  for (long it = 0; need != 0 && it < (1L << 22); it++) {
+    unsigned long long raw[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) raw[i] = (need >> i & 1u) ? ld_relaxed_u64(p + lane + 32 * i) : 0ull;
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+      if ((need >> i & 1u) && raw[i] != kPending) {
+        v[i] = __longlong_as_double(static_cast<long long>(raw[i]));
+        need &= ~(1u << i);
+      }
+    if ((it & 63) == 63) {
+      if (*reinterpret_cast<volatile int32_t *>(err) != 0) return;
+      __nanosleep(32);
+    }
+  }
+  if (need != 0) atomicExch(err, 1);
+}
+
 // The value at p from a load issued ahead (raw) when that load already saw
 // it, else the wait for it.
 __device__ __forceinline__ double take_value(unsigned long long raw, const double *p,
@@ -301,10 +330,14 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   const int     tiles = min(R, F.nb);
   // Right-hand side of this row: its entry of x (rows < w), then the
   // children's update vectors in child order.
-  double zr = 0.0;
-  if (qq == 0 && r < h) {
-    zr = r < w ? x[F.col0 + r] : 0.0;
-    for (int64_t e = gp[F.gptr + r]; e < gp[F.gptr + r + 1]; e++) zr += zbuf[gsrc[e]];
+  __shared__ double zs[kNB];
+  if (qq == 0) {
+    double zr = 0.0;
+    if (r < h) {
+      zr = r < w ? x[F.col0 + r] : 0.0;
+      for (int64_t e = gp[F.gptr + r]; e < gp[F.gptr + r + 1]; e++) zr += zbuf[gsrc[e]];
+    }
+    zs[rr] = zr;
   }
   double acc = 0.0;
   // The next tile's L values are loaded while the current one waits for y_b
@@ -325,20 +358,38 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
     return c0 + lane < w ? ld_relaxed_u64(yr + c0 + lane) : 0ull;
   };
   unsigned long long yv = 0ull, yvn = 0ull;
+  cp_async_wait_all();
   if (tiles > 0) {
     load_tile(lv, 0);
     yv = load_y(0);
   }
+  // The last tile's block result is the one just before this block on the
+  // chain: the first warp of each column quarter waits for the quarter's 32
+  // entries and shares them with the quarter's other three warps through a
+  // named barrier (each warp waiting for its own copy saw them up to 2 us
+  // apart, and the CTA could only go on with the last).
+  __shared__ double ylast[kNB];
   for (int b = 0; b < tiles; b++) {
-    const int c0 = b * kNB + qq * 32;
+    const int  c0   = b * kNB + qq * 32;
+    const bool last = b + 1 == tiles;
     if (b + 1 < tiles) {
       load_tile(lvn, b + 1);
-      yvn = load_y(b + 1);
+      if (b + 2 < tiles) yvn = load_y(b + 1);
     }
-    yw[warp][lane] = c0 + lane < w ? take_value(yv, yr + c0 + lane, err) : 0.0;
-    __syncwarp();
+    const double *ysrc = yw[warp];
+    if (!last) {
+      yw[warp][lane] = c0 + lane < w ? take_value(yv, yr + c0 + lane, err) : 0.0;
+      __syncwarp();
+    } else {
+      if (warp % 4 == 0)
+        ylast[qq * 32 + lane] =
+            c0 + lane < w ? wait_value(ready + ((item + qq) % kReadyCopies) * n + F.col0 + c0 + lane, err)
+                          : 0.0;
+      asm volatile("bar.sync %0, %1;" ::"r"(1 + qq), "r"(kNB) : "memory");
+      ysrc = ylast + qq * 32;
+    }
 #pragma unroll
-    for (int k = 0; k < 32; k++) acc += static_cast<double>(lv[k]) * yw[warp][k];
+    for (int k = 0; k < 32; k++) acc += static_cast<double>(lv[k]) * ysrc[k];
     __syncwarp();
 #pragma unroll
     for (int k = 0; k < 32; k++) lv[k] = lvn[k];
@@ -347,7 +398,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   part[qq][rr] = acc;
   __syncthreads();
   double z = 0.0;
-  if (qq == 0 && r < h) z = zr - ((part[0][rr] + part[1][rr]) + (part[2][rr] + part[3][rr]));
+  if (qq == 0 && r < h) z = zs[rr] - ((part[0][rr] + part[1][rr]) + (part[2][rr] + part[3][rr]));
   if (R < F.nb) {
     const int nbk = min(kNB, w - R * kNB);
     if (qq == 0) ys[pad(rr)] = rr < nbk ? z : 0.0;
@@ -540,17 +591,36 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
       }
     }
   };
+  // The last tile (R = b + 1) is the block just before this one on the
+  // chain: one warp waits for all of x_R and shares it (as in the forward).
+  __shared__ double xlast[kNB];
   if (F.nb - 1 > b) load_tile(lv, F.nb - 1);
   for (int R = F.nb - 1; R > b; R--) {
     const int64_t rb   = static_cast<int64_t>(R) * kNB;
     const int     rows = min(kNB, w - R * kNB);
     if (R - 1 > b) load_tile(lvn, R - 1);
+    if (R - 1 > b) {
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
-      const int    rr = lane + 32 * i;
-      const double zv = rr < rows ? wait_value(xr + rb + rr, err) : 0.0;
+      for (int i = 0; i < 4; i++) {
+        const int    rr = lane + 32 * i;
+        const double zv = rr < rows ? wait_value(xr + rb + rr, err) : 0.0;
 #pragma unroll
-      for (int j = 0; j < 8; j++) acc[j] += static_cast<double>(lv[j][i]) * zv;
+        for (int j = 0; j < 8; j++) acc[j] += static_cast<double>(lv[j][i]) * zv;
+      }
+    } else {
+      if (warp == 0) {
+        double xv[4];
+        wait_block4(ready + (item % kReadyCopies) * n + F.col0 + rb, rows, xv, err);
+#pragma unroll
+        for (int i = 0; i < 4; i++) xlast[lane + 32 * i] = xv[i];
+      }
+      __syncthreads();
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const double zv = xlast[lane + 32 * i];
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc[j] += static_cast<double>(lv[j][i]) * zv;
+      }
     }
 #pragma unroll
     for (int j = 0; j < 8; j++)
