@@ -30,18 +30,19 @@ constexpr int kSmallH      = kWarpSolveH;
 
 // ---------------------------------------------------------------------------
 // Products with the float64 inverse of one diagonal block (128 x 128), 512
-// threads: thread (q, i) takes row (or column) i and the 32 terms of slice q;
-// slices are summed in order.  Each thread first copies the inverse entries
-// it will use into shared memory with cp.async (asynchronous, no registers
-// held): a CTA does this when it starts, so the product at the end of its
-// wait chain reads shared memory only.  Forward layout: the lower triangle by
-// columns (column j from row j at 128 j - j (j - 1) / 2); backward layout: the
-// lower triangle by rows (row i at i (i + 1) / 2); both keep a warp's 32
-// accesses on consecutive addresses.
+// threads.  Each thread first copies the inverse entries it will use into
+// shared memory with cp.async (asynchronous, no registers held): a CTA does
+// this when it starts, so the product at the end of its wait chain reads
+// shared memory only, and each thread reads only what it copied itself.
 constexpr int kTri = kNB * (kNB + 1) / 2;
 
 __device__ __forceinline__ void cp_async8(double *dst, const double *src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(
+                   static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+               "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async16(double *dst, const double *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
                    static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
                "l"(src) : "memory");
 }
@@ -50,11 +51,9 @@ __device__ __forceinline__ void cp_async_wait_all() {
 }
 
 // Thread layout of the forward block product: lane l of warp v takes row
-// i = 8 v + l / 4 of the block and its slice q = l % 4 (32 terms);
-// the four slices of i sit in four neighbouring lanes and are added with two
-// shuffles, (s0 + s1) + (s2 + s3), with no CTA barrier.  Vectors the
-// products read are staged with a stride of 33 per 32 entries (pad()), so
-// the four slices of a warp read different banks.
+// i = 8 v + l / 4 of the block and its slice q = l % 4; the four slices of i
+// sit in four neighbouring lanes and are added with two shuffles,
+// (s0 + s1) + (s2 + s3), with no CTA barrier.
 __device__ __forceinline__ int blk_i() { return (threadIdx.x / 32) * 8 + (threadIdx.x % 32) / 4; }
 __device__ __forceinline__ int blk_q() { return threadIdx.x % 4; }
 __device__ __forceinline__ int pad(int j) { return (j / 32) * 33 + j % 32; }
@@ -64,34 +63,41 @@ __device__ __forceinline__ double quad_sum(double s) {
   return s;
 }
 
-// Stage Linv (column-major, leading dimension kNB) for y = Linv z.
-__device__ __forceinline__ void stage_lower(const double *Lv, double *Ls, int nb) {
-  const int i = blk_i(), q = blk_q();
-  for (int jj = 0; jj < kNB / 4; jj++) {
-    const int j = q * (kNB / 4) + jj;
-    if (j <= i && i < nb) cp_async8(Ls + kNB * j - j * (j - 1) / 2 + (i - j), Lv + i + j * kNB);
-  }
+// Forward copy of Linv, by rows in 64-byte segments: row i = 8 a + r holds
+// its first 8 (a + 1) entries (those right of the diagonal are zero), and a
+// row of an odd group a one segment of padding more, so the 8 rows a warp
+// reads start alternately in the two halves of the banks (a warp's 16-byte
+// loads then take the minimum of four shared-memory wavefronts).
+constexpr int kFwdTri = 64 * (16 * 17 / 2 + 8);
+__device__ __forceinline__ int fwd_row_start(int i) {
+  const int a = i / 8, r = i % 8;
+  return 64 * (a * (a + 1) / 2 + a / 2) + r * 8 * (a + 1 + (a & 1));
 }
 
-// y_i = (Linv z)_i from the staged copy, in all four lanes of row i; z is
-// staged with pad().
-__device__ __forceinline__ double block_lower_apply(const double *Ls, const double *zb, int nb) {
-  const int     i = blk_i(), q = blk_q(), j0 = q * (kNB / 4);
-  const double *z = zb + 33 * q;  // pad(j0 + jj) = 33 q + jj
+// Thread (i, q) copies the pairs j = 8 m + 2 q, 8 m + 2 q + 1 (m <= i / 8) of
+// row i from the row-major inverse Lt (Lt[i * kNB + j] = Linv[i][j]).
+__device__ __forceinline__ void stage_lower(const double *Lt, double *Ls) {
+  const int     i = blk_i(), q = blk_q(), a = i / 8;
+  double       *d = Ls + fwd_row_start(i) + 2 * q;
+  const double *s = Lt + i * kNB + 2 * q;
+  for (int m = 0; m <= a; m++) cp_async16(d + 8 * m, s + 8 * m);
+}
+
+// y_i = (Linv z)_i from the staged copy, in all four lanes of row i; z holds
+// 128 entries (16-byte aligned).  Warp v (rows 8 v .. 8 v + 7) takes the
+// segments m <= v: 4 (v + 1) loads of Linv and of z per warp in all.
+__device__ __forceinline__ double block_lower_apply(const double *Ls, const double *z) {
+  const int     i = blk_i(), q = blk_q(), a = i / 8;
+  const double *row = Ls + fwd_row_start(i) + 2 * q;
+  const double *zq  = z + 2 * q;
   cp_async_wait_all();
   double a0 = 0.0, a1 = 0.0;
-  if (i < nb && i >= j0) {
-    // Column j starts at kNB j - j (j - 1) / 2: the offset of (i, j) grows
-    // by kNB - j - 1 from column j to column j + 1.
-    int off = kNB * j0 - j0 * (j0 - 1) / 2 + (i - j0);
-#pragma unroll
-    for (int jj = 0; jj < kNB / 4; jj += 2) {
-      const int j = j0 + jj;
-      if (j <= i) a0 += Ls[off] * z[jj];
-      off += kNB - j - 1;
-      if (j + 1 <= i) a1 += Ls[off] * z[jj + 1];
-      off += kNB - j - 2;
-    }
+#pragma unroll 4
+  for (int m = 0; m <= a; m++) {
+    const double2 l = *reinterpret_cast<const double2 *>(row + 8 * m);
+    const double2 v = *reinterpret_cast<const double2 *>(zq + 8 * m);
+    a0 += l.x * v.x;
+    a1 += l.y * v.y;
   }
   return quad_sum(a0 + a1);
 }
@@ -295,11 +301,11 @@ __device__ __forceinline__ int take_ticket(int32_t *counter) {
 // w are the front's update vector for its parent.
 __global__ void __launch_bounds__(kSolveThreads, 1)
     k_fwd_fronts(const SolveFront *fr, const int32_t *fmap, const int32_t *frow,
-                 const float *panel, const double *linv64, const int64_t *gp,
+                 const float *panel, const double *linv64t, const int64_t *gp,
                  const int64_t *gsrc, double *x, double *zbuf, int32_t *tickets,
                  double *ready, int32_t *err) {
-  extern __shared__ double tri[];  // kTri doubles: the staged Linv_R
-  __shared__ double ys[4 * 33];
+  extern __shared__ __align__(16) double tri[];  // kFwdTri doubles: the staged Linv_R
+  __shared__ __align__(16) double ys[kNB];
   __shared__ double ys2[4 * 33];
   __shared__ double yw[kSolveThreads / 32][32];
   __shared__ double part[4][kNB];
@@ -317,8 +323,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   const SolveFront &F = sF;
   const int         R = sR;
   if (R < F.nb)
-    stage_lower(linv64 + F.linv + static_cast<int64_t>(R) * kNB * kNB, tri,
-                min(kNB, F.w - R * kNB));
+    stage_lower(linv64t + F.linv + static_cast<int64_t>(R) * kNB * kNB, tri);
   const int     tid = threadIdx.x, rr = tid % kNB, qq = tid / kNB;
   const int     warp = tid / 32, lane = tid % 32;
   const int64_t h = F.h;
@@ -401,9 +406,9 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   if (qq == 0 && r < h) z = zs[rr] - ((part[0][rr] + part[1][rr]) + (part[2][rr] + part[3][rr]));
   if (R < F.nb) {
     const int nbk = min(kNB, w - R * kNB);
-    if (qq == 0) ys[pad(rr)] = rr < nbk ? z : 0.0;
+    if (qq == 0) ys[rr] = rr < nbk ? z : 0.0;
     __syncthreads();
-    const double y  = block_lower_apply(tri, ys, nbk);
+    const double y  = block_lower_apply(tri, ys);
     const int    iy = blk_i();
     if (blk_q() == 0 && iy < nbk) {
       const int64_t j = F.col0 + R * kNB + iy;
@@ -697,7 +702,7 @@ void ldlt_solve(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
   KernelTimer    &kt = kernel_timer();
   if (S.n == 0) return;
   const float *pan  = F.panel.as<float>();
-  const double *lv  = F.linv64.as<double>();
+  const double *lvt = F.linv64t.as<double>();
   double      *zbuf = ws.zbuf.as<double>();
   const int    nl   = static_cast<int>(P.levels.size());
   // Tickets (2 per level); the ready buffer is marked pending before each
@@ -714,7 +719,7 @@ void ldlt_solve(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
   static bool attr = false;
   if (!attr) {
     MPIR_CUDA(cudaFuncSetAttribute(k_fwd_fronts, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   static_cast<int>(kTri * sizeof(double))));
+                                   static_cast<int>(kFwdTri * sizeof(double))));
     MPIR_CUDA(cudaFuncSetAttribute(k_bwd_fronts, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(kTri * sizeof(double))));
     attr = true;
@@ -729,9 +734,9 @@ void ldlt_solve(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
              P.child_list.as<int32_t>(), P.srel.as<int32_t>(), P.zofs.as<int64_t>(), pan, x,
              zbuf);
     if (L.sf_count > 0) {
-      launch(k_fwd_fronts, L.fwd_items, kSolveThreads, kTri * sizeof(double), s, sf + L.sf_begin,
-             P.fwd_map.as<int32_t>() + L.fwd_map0, P.fwd_row.as<int32_t>() + L.fwd_map0, pan,
-             lv, P.gp.as<int64_t>(),
+      launch(k_fwd_fronts, L.fwd_items, kSolveThreads, kFwdTri * sizeof(double), s,
+             sf + L.sf_begin, P.fwd_map.as<int32_t>() + L.fwd_map0,
+             P.fwd_row.as<int32_t>() + L.fwd_map0, pan, lvt, P.gp.as<int64_t>(),
              P.gsrc.as<int64_t>(), x, zbuf, sync + 2 * t, ready, err);
     }
   }
