@@ -374,31 +374,34 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   // named barrier (each warp waiting for its own copy saw them up to 2 us
   // apart, and the CTA could only go on with the last).
   __shared__ double ylast[kNB];
-  for (int b = 0; b < tiles; b++) {
-    const int  c0   = b * kNB + qq * 32;
-    const bool last = b + 1 == tiles;
-    if (b + 1 < tiles) {
-      load_tile(lvn, b + 1);
-      if (b + 2 < tiles) yvn = load_y(b + 1);
-    }
-    const double *ysrc = yw[warp];
-    if (!last) {
-      yw[warp][lane] = c0 + lane < w ? take_value(yv, yr + c0 + lane, err) : 0.0;
-      __syncwarp();
-    } else {
-      if (warp % 4 == 0)
-        ylast[qq * 32 + lane] =
-            c0 + lane < w ? wait_value(ready + ((item + qq) % kReadyCopies) * n + F.col0 + c0 + lane, err)
-                          : 0.0;
-      asm volatile("bar.sync %0, %1;" ::"r"(1 + qq), "r"(kNB) : "memory");
-      ysrc = ylast + qq * 32;
-    }
+  for (int b = 0; b + 1 < tiles; b++) {
+    const int c0 = b * kNB + qq * 32;
+    load_tile(lvn, b + 1);
+    if (b + 2 < tiles) yvn = load_y(b + 1);
+    yw[warp][lane] = c0 + lane < w ? take_value(yv, yr + c0 + lane, err) : 0.0;
+    __syncwarp();
 #pragma unroll
-    for (int k = 0; k < 32; k++) acc += static_cast<double>(lv[k]) * ysrc[k];
+    for (int k = 0; k < 32; k++) acc += static_cast<double>(lv[k]) * yw[warp][k];
     __syncwarp();
 #pragma unroll
     for (int k = 0; k < 32; k++) lv[k] = lvn[k];
     yv = yvn;
+  }
+  if (tiles > 0) {
+    // The last tile: its L values are widened before the wait (float to
+    // double conversions run at a quarter of the FMA rate; done after the
+    // wait, by all 16 warps, they took about 0.5 us of the chain).
+    const int c0 = (tiles - 1) * kNB + qq * 32;
+    double    ld[32];
+#pragma unroll
+    for (int k = 0; k < 32; k++) ld[k] = static_cast<double>(lv[k]);
+    if (warp % 4 == 0)
+      ylast[qq * 32 + lane] =
+          c0 + lane < w ? wait_value(ready + ((item + qq) % kReadyCopies) * n + F.col0 + c0 + lane, err)
+                        : 0.0;
+    asm volatile("bar.sync %0, %1;" ::"r"(1 + qq), "r"(kNB) : "memory");
+#pragma unroll
+    for (int k = 0; k < 32; k++) acc += ld[k] * ylast[qq * 32 + k];
   }
   part[qq][rr] = acc;
   __syncthreads();
@@ -600,44 +603,69 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   // chain: one warp waits for all of x_R and shares it (as in the forward).
   __shared__ double xlast[kNB];
   if (F.nb - 1 > b) load_tile(lv, F.nb - 1);
-  for (int R = F.nb - 1; R > b; R--) {
+  for (int R = F.nb - 1; R > b + 1; R--) {
     const int64_t rb   = static_cast<int64_t>(R) * kNB;
     const int     rows = min(kNB, w - R * kNB);
-    if (R - 1 > b) load_tile(lvn, R - 1);
-    if (R - 1 > b) {
+    load_tile(lvn, R - 1);
 #pragma unroll
-      for (int i = 0; i < 4; i++) {
-        const int    rr = lane + 32 * i;
-        const double zv = rr < rows ? wait_value(xr + rb + rr, err) : 0.0;
+    for (int i = 0; i < 4; i++) {
+      const int    rr = lane + 32 * i;
+      const double zv = rr < rows ? wait_value(xr + rb + rr, err) : 0.0;
 #pragma unroll
-        for (int j = 0; j < 8; j++) acc[j] += static_cast<double>(lv[j][i]) * zv;
-      }
-    } else {
-      if (warp == 0) {
-        double xv[4];
-        wait_block4(ready + (item % kReadyCopies) * n + F.col0 + rb, rows, xv, err);
-#pragma unroll
-        for (int i = 0; i < 4; i++) xlast[lane + 32 * i] = xv[i];
-      }
-      __syncthreads();
-#pragma unroll
-      for (int i = 0; i < 4; i++) {
-        const double zv = xlast[lane + 32 * i];
-#pragma unroll
-        for (int j = 0; j < 8; j++) acc[j] += static_cast<double>(lv[j][i]) * zv;
-      }
+      for (int j = 0; j < 8; j++) acc[j] += static_cast<double>(lv[j][i]) * zv;
     }
 #pragma unroll
     for (int j = 0; j < 8; j++)
 #pragma unroll
       for (int i = 0; i < 4; i++) lv[j][i] = lvn[j][i];
   }
+  if (F.nb - 1 > b) {
+    // The last tile (R = b + 1): its L values are widened before the wait,
+    // as in the forward solve.
+    const int64_t rb   = static_cast<int64_t>(b + 1) * kNB;
+    const int     rows = min(kNB, w - (b + 1) * kNB);
+    double        ld[8][4];
 #pragma unroll
-  for (int j = 0; j < 8; j++) {
-    double s = acc[j];
+    for (int j = 0; j < 8; j++)
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) ts[warp * 8 + j] = s;
+      for (int i = 0; i < 4; i++) ld[j][i] = static_cast<double>(lv[j][i]);
+    if (warp == 0) {
+      double xv[4];
+      wait_block4(ready + (item % kReadyCopies) * n + F.col0 + rb, rows, xv, err);
+#pragma unroll
+      for (int i = 0; i < 4; i++) xlast[lane + 32 * i] = xv[i];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const double zv = xlast[lane + 32 * i];
+#pragma unroll
+      for (int j = 0; j < 8; j++) acc[j] += ld[j][i] * zv;
+    }
+  }
+  // Sums of the warp's 8 columns over its 32 lanes: the usual butterfly
+  // (partners lane ^ 16, ^ 8, ^ 4, ^ 2, ^ 1), but at each of the first three
+  // levels a lane keeps half of its columns and sends the other half, so it
+  // takes 4 + 2 + 1 + 1 + 1 shuffles instead of 8 x 5 (the same additions in
+  // the same order).  Lane l ends with column (l >> 2) & 7.
+  {
+    const unsigned full = 0xffffffffu;
+    double         s4[4], s2[2];
+    const bool     b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const double keep = b4 ? acc[u + 4] : acc[u], send = b4 ? acc[u] : acc[u + 4];
+      s4[u] = keep + __shfl_xor_sync(full, send, 16);
+    }
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      const double keep = b3 ? s4[u + 2] : s4[u], send = b3 ? s4[u] : s4[u + 2];
+      s2[u] = keep + __shfl_xor_sync(full, send, 8);
+    }
+    double s = (b2 ? s2[1] : s2[0]) + __shfl_xor_sync(full, b2 ? s2[0] : s2[1], 4);
+    s += __shfl_xor_sync(full, s, 2);
+    s += __shfl_xor_sync(full, s, 1);
+    if ((lane & 3) == 0) ts[warp * 8 + ((lane >> 2) & 7)] = s;
   }
   __syncthreads();
   if (tid < nbk)
