@@ -83,6 +83,15 @@ struct SolveFront {
   int32_t own0;    // first backward column-block CTA
 };
 
+// One work item of the ticketed solve launches: a copy of its front's
+// descriptor and its row block (forward) or column block (backward), so a CTA
+// reads one record after taking its ticket.
+struct SolveItem {
+  SolveFront f;
+  int32_t    r;
+  int32_t    pad;
+};
+
 // Packed copy of a large front's L for the tensor-core updates.  Rows are
 // renumbered so that the off-diagonal rows start on a 128-row boundary:
 // packed row p = r for r < w, p = Wt + (r - w) for r >= w, Wt = w rounded up

@@ -89,7 +89,8 @@ struct LevelPlan {
   int32_t sf_begin = 0, sf_count = 0;
   int32_t sw_begin = 0, sw_count = 0;  // warp-solved fronts (swarp list)
   int32_t fwd_items = 0, bwd_chunk_items = 0, bwd_owner_items = 0;
-  // Offsets of the level's item -> front maps (front index within the level).
+  // Offsets of the level's work items (Plan::fwd_item, own_item) and of its
+  // chunk -> front map (front index within the level).
   int64_t fwd_map0 = 0, chunk_map0 = 0, own_map0 = 0;
 };
 
@@ -112,7 +113,7 @@ class Plan {
       child_list, perm;
   DeviceBuffer ea_seq;  // int32 pairs, see LevelPlan::ea_seq_begin
   DeviceBuffer small_list, large_list, steps, ea_tasks, linv_ofs_d, gemm_probs,
-      solve_fronts, swarp_list, sblock_list, gp, gsrc, fwd_map, fwd_row, chunk_map, own_map;
+      solve_fronts, swarp_list, sblock_list, gp, gsrc, fwd_item, chunk_map, own_item;
   int64_t      ws_elems = 0;  // split-K partial tiles (floats)
   int64_t      bconv_elems = 0;  // converted B operands of the largest launch (floats)
   std::vector<int32_t> h_small, h_large;

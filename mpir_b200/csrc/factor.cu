@@ -912,7 +912,8 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
   h_swarp.clear();
   h_sblock.clear();
   std::vector<int64_t> gp_h, gsrc_h;
-  std::vector<int32_t> fwd_map_h, fwd_row_h, chunk_map_h, own_map_h;
+  std::vector<int32_t>   chunk_map_h;
+  std::vector<SolveItem> fwd_item_h, own_item_h;
   std::vector<SolveFront> sfronts;
   update_flops = 0;
   trsm_flops   = 0;
@@ -1190,29 +1191,25 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
     }
     L.sf_count  = static_cast<int32_t>(sfronts.size()) - L.sf_begin;
     // Item -> front maps of the level's solve launches.
-    L.fwd_map0   = static_cast<int64_t>(fwd_map_h.size());
+    L.fwd_map0   = static_cast<int64_t>(fwd_item_h.size());
     L.chunk_map0 = static_cast<int64_t>(chunk_map_h.size());
-    L.own_map0   = static_cast<int64_t>(own_map_h.size());
+    L.own_map0   = static_cast<int64_t>(own_item_h.size());
     // Forward: every front's diagonal row blocks first (their chains start
     // together), then the off-diagonal row blocks, which wait on them.
     for (int32_t q = 0; q < L.sf_count; q++) {
       const SolveFront &f = sfronts[L.sf_begin + q];
-      for (int32_t i = 0; i < f.nb; i++) {
-        fwd_map_h.push_back(q);
-        fwd_row_h.push_back(i);
-      }
+      for (int32_t i = 0; i < f.nb; i++) fwd_item_h.push_back(SolveItem{f, i, 0});
     }
     for (int32_t q = 0; q < L.sf_count; q++) {
       const SolveFront &f = sfronts[L.sf_begin + q];
-      for (int32_t i = f.nb; i < (f.h + kNB - 1) / kNB; i++) {
-        fwd_map_h.push_back(q);
-        fwd_row_h.push_back(i);
-      }
+      for (int32_t i = f.nb; i < (f.h + kNB - 1) / kNB; i++)
+        fwd_item_h.push_back(SolveItem{f, i, 0});
     }
+    // Backward: each front's column blocks, last first.
     for (int32_t q = 0; q < L.sf_count; q++) {
       const SolveFront &f = sfronts[L.sf_begin + q];
       for (int32_t i = 0; i < f.chunks; i++) chunk_map_h.push_back(q);
-      for (int32_t i = 0; i < f.nb; i++) own_map_h.push_back(q);
+      for (int32_t i = 0; i < f.nb; i++) own_item_h.push_back(SolveItem{f, f.nb - 1 - i, 0});
     }
     L.sw_count  = static_cast<int32_t>(h_swarp.size()) - L.sw_begin;
     spart_elems = std::max(spart_elems, spart);
@@ -1277,10 +1274,9 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
   sblock_list  = upload(h_sblock, s);
   gp           = upload(gp_h, s);
   gsrc         = upload(gsrc_h, s);
-  fwd_map      = upload(fwd_map_h, s);
-  fwd_row      = upload(fwd_row_h, s);
+  fwd_item     = upload(fwd_item_h, s);
   chunk_map    = upload(chunk_map_h, s);
-  own_map      = upload(own_map_h, s);
+  own_item     = upload(own_item_h, s);
   sync_elems   = 2 * static_cast<int64_t>(levels.size());
   MPIR_CUDA(cudaStreamSynchronize(s));
 }

@@ -280,13 +280,6 @@ __global__ void k_mark_pending(int64_t n, double *ready) {
   if (i < n) reinterpret_cast<unsigned long long *>(ready)[i] = kPending;
 }
 
-// CTA-wide ticket: the order in which CTAs of a launch take their work.
-__device__ __forceinline__ int take_ticket(int32_t *counter) {
-  __shared__ int s_ticket;
-  if (threadIdx.x == 0) s_ticket = atomicAdd(counter, 1);
-  __syncthreads();
-  return s_ticket;
-}
 
 
 // Forward solve of the large fronts of one level: one CTA per 128-row block
@@ -300,8 +293,7 @@ __device__ __forceinline__ int take_ticket(int32_t *counter) {
 // buffer (block product with warp-local slices, see blk_i); rows at or past
 // w are the front's update vector for its parent.
 __global__ void __launch_bounds__(kSolveThreads, 1)
-    k_fwd_fronts(const SolveFront *fr, const int32_t *fmap, const int32_t *frow,
-                 const float *panel, const double *linv64t, const int64_t *gp,
+    k_fwd_fronts(const SolveItem *items, const float *panel, const double *linv64t, const int64_t *gp,
                  const int64_t *gsrc, double *x, double *zbuf, int32_t *tickets,
                  double *ready, int32_t *err) {
   extern __shared__ __align__(16) double tri[];  // kFwdTri doubles: the staged Linv_R
@@ -309,19 +301,23 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   __shared__ double ys2[4 * 33];
   __shared__ double yw[kSolveThreads / 32][32];
   __shared__ double part[4][kNB];
-  // The front's descriptor sits in shared memory: the code after the tile
-  // loop (on the chain of diagonal blocks) reads its fields again, and from
-  // global memory that took a round trip past an L1 the tiles had flushed.
+  // Thread 0 takes the CTA's ticket (the order in which CTAs take their work,
+  // so every block a CTA waits for belongs to an earlier ticket) and copies
+  // the item's record into shared memory: the code after the tile loop (on
+  // the chain of diagonal blocks) reads the descriptor again, and from global
+  // memory that took a round trip past an L1 the tiles had flushed.
   __shared__ SolveFront sF;
-  __shared__ int        sR;
-  const int             item = take_ticket(tickets);
+  __shared__ int        sR, sItem;
   if (threadIdx.x == 0) {
-    sF = fr[fmap[item]];
-    sR = frow[item];
+    const int it = atomicAdd(tickets, 1);
+    sItem        = it;
+    sF           = items[it].f;
+    sR           = items[it].r;
   }
   __syncthreads();
-  const SolveFront &F = sF;
-  const int         R = sR;
+  const int         item = sItem;
+  const SolveFront &F    = sF;
+  const int         R    = sR;
   if (R < F.nb)
     stage_lower(linv64t + F.linv + static_cast<int64_t>(R) * kNB * kNB, tri);
   const int     tid = threadIdx.x, rr = tid % kNB, qq = tid / kNB;
@@ -541,7 +537,7 @@ __global__ void __launch_bounds__(kSolveThreads)
 // into x and the ready buffer.  In a tile, warp v takes the block's columns
 // 8v .. 8v+7 and the lanes the rows.
 __global__ void __launch_bounds__(kSolveThreads, 1)
-    k_bwd_fronts(const SolveFront *fr, const int32_t *fmap, const float *panel,
+    k_bwd_fronts(const SolveItem *items, const float *panel,
                  const double *linv64t,
                  double *x, const double *part, int32_t *tickets,
                  double *ready, int32_t *err) {
@@ -549,13 +545,19 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   __shared__ double v[kNB];
   __shared__ double ts[kNB];
   __shared__ double red[4][kNB];
-  // The front's descriptor sits in shared memory (see k_fwd_fronts).
+  // Ticket and item record as in k_fwd_fronts.
   __shared__ SolveFront sF;
-  const int             item = take_ticket(tickets);
-  if (threadIdx.x == 0) sF = fr[fmap[item]];
+  __shared__ int        sB, sItem;
+  if (threadIdx.x == 0) {
+    const int it = atomicAdd(tickets, 1);
+    sItem        = it;
+    sF           = items[it].f;
+    sB           = items[it].r;
+  }
   __syncthreads();
-  const SolveFront &F = sF;
-  const int         b = F.nb - 1 - (item - F.own0);
+  const int         item = sItem;
+  const SolveFront &F    = sF;
+  const int         b    = sB;
   stage_upper(linv64t + F.linv + static_cast<int64_t>(b) * kNB * kNB, tri,
               min(kNB, F.w - b * kNB));
   const int         tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
@@ -763,8 +765,7 @@ void ldlt_solve(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
              zbuf);
     if (L.sf_count > 0) {
       launch(k_fwd_fronts, L.fwd_items, kSolveThreads, kFwdTri * sizeof(double), s,
-             sf + L.sf_begin, P.fwd_map.as<int32_t>() + L.fwd_map0,
-             P.fwd_row.as<int32_t>() + L.fwd_map0, pan, lvt, P.gp.as<int64_t>(),
+             P.fwd_item.as<SolveItem>() + L.fwd_map0, pan, lvt, P.gp.as<int64_t>(),
              P.gsrc.as<int64_t>(), x, zbuf, sync + 2 * t, ready, err);
     }
   }
@@ -789,7 +790,7 @@ void ldlt_solve(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
                static_cast<const double *>(x),
                ws.part.as<double>());
       launch(k_bwd_fronts, L.bwd_owner_items, kSolveThreads, kTri * sizeof(double), s,
-             sf + L.sf_begin, P.own_map.as<int32_t>() + L.own_map0, pan,
+             P.own_item.as<SolveItem>() + L.own_map0, pan,
              F.linv64t.as<double>(), x,
              static_cast<const double *>(ws.part.as<double>()), sync + 2 * t + 1, ready, err);
     }
