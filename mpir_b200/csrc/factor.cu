@@ -869,11 +869,15 @@ __global__ void __launch_bounds__(kDiagThreads)
     X[i * LD + j] = i == j ? 1.0 : 0.0;
   }
   __syncthreads();
+  // Step k subtracts L[i][k] X[k][j] from X[i][j] for all i > k, j <= k:
+  // thread (i, g) = (tid % kNB, tid / kNB) takes row i and the columns
+  // j = g, g + 4, ... (every entry gets its terms in increasing k).
+  static_assert(kDiagThreads == 4 * kNB, "invert thread mapping");
+  const int ri = tid % kNB, g = tid / kNB;
   for (int k = 0; k < n; k++) {
-    const int m = n - k - 1;
-    for (int idx = tid; idx < m * (k + 1); idx += bd) {
-      const int i = k + 1 + idx % m, j = idx / m;
-      X[i * LD + j] -= static_cast<double>(F[i * LD + k]) * X[k * LD + j];
+    if (ri > k && ri < n) {
+      const double f = static_cast<double>(F[ri * LD + k]);
+      for (int j = g; j <= k; j += 4) X[ri * LD + j] -= f * X[k * LD + j];
     }
     __syncthreads();
   }
