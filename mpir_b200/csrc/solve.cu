@@ -215,7 +215,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta)
 // the sticky error word and returns 0; it looks at that word every 64 polls,
 // so one failure ends the launch quickly.
 constexpr unsigned long long kPending = 0x7ff0deadbeef0001ull;
-constexpr int kReadyCopies = 8;
+constexpr int kReadyCopies = 16;
 
 __device__ __forceinline__ unsigned long long ld_relaxed_u64(const double *p) {
   unsigned long long v;
