@@ -196,12 +196,42 @@ int mpir_solver_dump_log(mpir_solver s, char *buf, int64_t cap, int64_t *len);
 
 /* nrhs right-hand sides with the current factor: B and X hold nrhs
  * contiguous vectors of length n (column-major n x nrhs, host memory); one
- * GMRES-IR solve per column, each exactly as mpir_solver_solve; reps (NULL,
- * or nrhs reports) receives each solve's report.  Stops at the first error.
- * The reference solves one right-hand side per GmresLDLIR::Solve call
- * (gmres_ir.hpp:534); this entry point is that loop. */
+ * GMRES-IR solve per column; reps (NULL, or nrhs reports) receives each
+ * solve's report.  Stops at the first error.  The reference solves one
+ * right-hand side per GmresLDLIR::Solve call (gmres_ir.hpp:534); this entry
+ * point runs those solves in groups of up to 16 through
+ * mpir_solver_solve_batch (a group of one through mpir_solver_solve). */
 int mpir_solver_solve_many(mpir_solver s, int64_t nrhs, const double *B,
                            double *X, mpir_report *reps);
+
+/* 1 <= nrhs <= 16 GMRES-IR solves with the current factor in lockstep: each
+ * right-hand side follows GmresLDLIR::Solve (gmres_ir.hpp:534-634) with its
+ * own Krylov basis, iteration counts and stop tests, while every
+ * preconditioner application (QDLDL_solve, qdldl.hpp:417-432, applied once
+ * per vector by the reference) is one several-vector triangular solve that
+ * reads the factor once for all of them.  Results agree with one-at-a-time
+ * mpir_solver_solve calls to rounding (each at backward error <= 1e-14 where
+ * the single solve reaches it).  B and X column-major n x nrhs in the
+ * caller's order, host (_batch) or device (_batch_device) memory; reps:
+ * NULL or nrhs reports (solve_ms is the whole batch's time). */
+int mpir_solver_solve_batch(mpir_solver s, int nrhs, const double *B,
+                            double *X, mpir_report *reps);
+int mpir_solver_solve_batch_device(mpir_solver s, int nrhs, const double *d_B,
+                                   double *d_X, mpir_report *reps);
+
+/* X <- (L D L^T)^{-1} X for 1 <= nrhs <= 16 vectors (n x nrhs column-major,
+ * host memory) in the solver's internal order: the permuted, diagonally
+ * scaled matrix the factor belongs to (mpir_solver_symbolic's perm).  The
+ * preconditioner application of QDLDL_solve (qdldl.hpp:417-432); one vector
+ * runs the single-vector kernels, several the several-vector kernels. */
+int mpir_solver_apply_factor(mpir_solver s, int nrhs, double *X);
+
+/* Failure-test controls of the bounded device waits of the triangular
+ * solves: each wait gives up after 2^poll_log2 polls (0 restores the default
+ * of about a second), and the forward work item withhold_item (-1: none)
+ * never publishes its block result, so the waits on it run out and the
+ * solve returns MPIR_ERR_TIMEOUT.  For tests of the timeout path only. */
+int mpir_solver_set_wait_controls(mpir_solver s, int poll_log2, int withhold_item);
 
 /* Plain iterative refinement with the LDL^T factor, LUIR_QDLDL
  * (qdldl-luir/luir.hpp:33-241) with float64 residual, working and solution

@@ -100,6 +100,12 @@ def lib():
         "mpir_solver_solve_device": (i32, [vp, vp, vp, vp]),
         "mpir_solver_set_stream": (i32, [vp, vp]),
         "mpir_solver_solve_many": (i32, [vp, i64, vp, vp, vp]),
+        "mpir_solver_solve_batch": (i32, [vp, i32, vp, vp, vp]),
+        "mpir_solver_solve_batch_device": (i32, [vp, i32, vp, vp, vp]),
+        "mpir_solver_apply_factor": (i32, [vp, i32, vp]),
+        "mpir_solver_set_wait_controls": (i32, [vp, i32, i32]),
+        "mpir_qdldl_lsolve": (i32, [i64, vp, vp, vp, i32, vp, i32, i32]),
+        "mpir_qdldl_ltsolve": (i32, [i64, vp, vp, vp, i32, vp, i32, i32]),
         "mpir_solver_dump_log": (i32, [vp, vp, i64, vp]),
         "mpir_solver_luir": (i32, [vp, vp, vp, i32, vp]),
         "mpir_solver_luir_device": (i32, [vp, vp, vp, i32, vp]),
@@ -199,6 +205,26 @@ def QDLDL_solve(n, Lp, Li, Lx, Dinv, x, fact_prec="f32", device=0):
     _check(lib().mpir_qdldl_solve(n, _p(_i64(Lp)), _p(_i64(Li)), _p(Lx), _p(Dinv), prec,
                                   _p(x), xp, device))
     return x
+
+
+def _lsolve_common(fn, n, Lp, Li, Lx, x, fact_prec, device):
+    prec = _PREC[fact_prec]
+    xp = F64 if x.dtype == np.float64 else F32
+    if not x.flags["C_CONTIGUOUS"]:
+        raise ValueError("x must be contiguous")
+    Lx = np.ascontiguousarray(Lx)
+    _check(fn(n, _p(_i64(Lp)), _p(_i64(Li)), _p(Lx), prec, _p(x), xp, device))
+    return x
+
+
+def QDLDL_Lsolve(n, Lp, Li, Lx, x, fact_prec="f32", device=0):
+    """QDLDL_Lsolve (qdldl.hpp:362-372) on the GPU: x <- (L + I)^{-1} x in place."""
+    return _lsolve_common(lib().mpir_qdldl_lsolve, n, Lp, Li, Lx, x, fact_prec, device)
+
+
+def QDLDL_Ltsolve(n, Lp, Li, Lx, x, fact_prec="f32", device=0):
+    """QDLDL_Ltsolve (qdldl.hpp:389-400) on the GPU: x <- (L + I)^{-T} x in place."""
+    return _lsolve_common(lib().mpir_qdldl_ltsolve, n, Lp, Li, Lx, x, fact_prec, device)
 
 
 def LUIR_QDLDL(n, Ap, Ai, Ax, b, fact_prec="f32", maxiter=10, device=0):
@@ -324,6 +350,31 @@ class GmresLDLIR:
         _check(lib().mpir_solver_solve_many(self._h, B.shape[0], _p(B), _p(X), reps))
         self.last_reports = [reps[k].as_dict() for k in range(B.shape[0])]
         return X
+
+    def SolveBatch(self, B):
+        """1 to 16 right-hand sides (rows of B) solved in lockstep, every
+        preconditioner application one several-vector triangular solve;
+        returns X of B's shape; reports in last_reports."""
+        B = np.ascontiguousarray(B, dtype=np.float64)
+        if B.ndim != 2 or B.shape[1] != self.n:
+            return np.zeros((0, self.n), np.float64)
+        X = np.zeros_like(B)
+        reps = (Report * B.shape[0])()
+        _check(lib().mpir_solver_solve_batch(self._h, B.shape[0], _p(B), _p(X), reps))
+        self.last_reports = [reps[k].as_dict() for k in range(B.shape[0])]
+        return X
+
+    def apply_factor(self, X):
+        """X (rows = vectors, internal permuted and scaled order) <-
+        (L D L^T)^{-1} X for 1 to 16 vectors; returns a new array."""
+        X = np.array(X, dtype=np.float64, order="C", copy=True)
+        _check(lib().mpir_solver_apply_factor(self._h, X.shape[0], _p(X)))
+        return X
+
+    def set_wait_controls(self, poll_log2=0, withhold_item=-1):
+        """Failure-test controls of the bounded device waits (see
+        mpir_solver_set_wait_controls)."""
+        _check(lib().mpir_solver_set_wait_controls(self._h, int(poll_log2), int(withhold_item)))
 
     def luir(self, b, maxiter=10):
         """Plain iterative refinement with the current factor (LUIR_QDLDL's

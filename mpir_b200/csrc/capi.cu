@@ -31,6 +31,9 @@ static auto guard(F &&f) -> decltype(f()) {
   } catch (const StatusError &e) {
     g_err = e.what();
     return e.code;
+  } catch (const WaitTimeout &e) {
+    g_err = e.what();
+    return MPIR_ERR_TIMEOUT;
   } catch (const CudaError &e) {
     g_err = e.what();
     return e.code == cudaErrorMemoryAllocation ? MPIR_ERR_NOMEM : MPIR_ERR_CUDA;
@@ -472,12 +475,64 @@ int mpir_solver_solve_many(mpir_solver s, int64_t nrhs, const double *B, double 
   return guard([&]() -> int {
     if (nrhs < 0 || (nrhs > 0 && (!B || !X)))
       throw StatusError(MPIR_ERR_ARGUMENT, "invalid argument");
-    const int64_t n = s->impl->plan().S.n;
-    for (int64_t k = 0; k < nrhs; k++) {
-      const int rc = s->impl->solve(B + k * n, X + k * n,
-                                    reps ? reinterpret_cast<Report *>(reps + k) : nullptr);
+    const int64_t n  = s->impl->plan().S.n;
+    const int64_t mb = Solver::kMaxBatch;
+    for (int64_t k0 = 0; k0 < nrhs; k0 += mb) {
+      const int nb = static_cast<int>(std::min(mb, nrhs - k0));
+      Report   *r  = reps ? reinterpret_cast<Report *>(reps + k0) : nullptr;
+      const int rc = nb == 1 ? s->impl->solve(B + k0 * n, X + k0 * n, r)
+                             : s->impl->solve_batch(nb, B + k0 * n, X + k0 * n, r);
       if (rc != MPIR_OK) return rc;
     }
+    return MPIR_OK;
+  });
+}
+
+int mpir_solver_solve_batch(mpir_solver s, int nrhs, const double *B, double *X,
+                            mpir_report *reps) {
+  MPIR_NEED(s);
+  return guard([&]() -> int {
+    if (nrhs < 1 || nrhs > Solver::kMaxBatch || !B || !X)
+      throw StatusError(MPIR_ERR_ARGUMENT, "1 <= nrhs <= 16 right-hand sides, non-NULL B and X");
+    return s->impl->solve_batch(nrhs, B, X, reinterpret_cast<Report *>(reps));
+  });
+}
+
+int mpir_solver_solve_batch_device(mpir_solver s, int nrhs, const double *d_B, double *d_X,
+                                   mpir_report *reps) {
+  MPIR_NEED(s);
+  return guard([&]() -> int {
+    if (nrhs < 1 || nrhs > Solver::kMaxBatch || !d_B || !d_X)
+      throw StatusError(MPIR_ERR_ARGUMENT, "1 <= nrhs <= 16 right-hand sides, non-NULL B and X");
+    return s->impl->solve_batch_device(nrhs, d_B, d_X, reinterpret_cast<Report *>(reps));
+  });
+}
+
+int mpir_solver_apply_factor(mpir_solver s, int nrhs, double *X) {
+  MPIR_NEED(s);
+  return guard([&]() -> int {
+    if (nrhs < 1 || nrhs > Solver::kMaxBatch || !X)
+      throw StatusError(MPIR_ERR_ARGUMENT, "1 <= nrhs <= 16 vectors, non-NULL X");
+    Solver       &sv = *s->impl;
+    const int64_t n  = sv.plan().S.n;
+    if (n == 0) return MPIR_OK;
+    DeviceBuffer d(n * nrhs * sizeof(double));
+    MPIR_CUDA(cudaMemcpyAsync(d.as<void>(), X, n * nrhs * sizeof(double), cudaMemcpyHostToDevice,
+                              sv.stream()));
+    sv.precond_device(nrhs, d.as<double>());
+    MPIR_CUDA(cudaMemcpyAsync(X, d.as<void>(), n * nrhs * sizeof(double), cudaMemcpyDeviceToHost,
+                              sv.stream()));
+    MPIR_CUDA(cudaStreamSynchronize(sv.stream()));
+    return MPIR_OK;
+  });
+}
+
+int mpir_solver_set_wait_controls(mpir_solver s, int poll_log2, int withhold_item) {
+  MPIR_NEED(s);
+  return guard([&]() -> int {
+    if (poll_log2 < 0 || poll_log2 > 30)
+      throw StatusError(MPIR_ERR_ARGUMENT, "poll_log2 in 0 .. 30");
+    s->impl->set_wait_controls(poll_log2, withhold_item);
     return MPIR_OK;
   });
 }

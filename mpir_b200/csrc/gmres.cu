@@ -55,6 +55,8 @@ Solver::Solver(int uf_, int uw_, int ur_, int dev)
 Solver::~Solver() {
   cudaSetDevice(device);
   if (own_stream_) cudaStreamSynchronize(own_stream_);
+  if (stream_ && stream_ != own_stream_) cudaStreamSynchronize(stream_);
+  if (hpin_) cudaFreeHost(hpin_);
   if (ev0_) cudaEventDestroy(ev0_);
   if (ev1_) cudaEventDestroy(ev1_);
   plan_.reset();
@@ -86,6 +88,13 @@ int Solver::analyze(int64_t n, const int64_t *Ap, const int64_t *Ai,
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   vec_.allocate(n, sms);
   vec_m_ = -1;
+  // The batch buffers belong to the previous pattern.
+  bw_  = 0;
+  bm_  = -1;
+  mws_ = MultiSolveWorkspace{};
+  if (wait_ctl_[0] || wait_ctl_[1])
+    MPIR_CUDA(cudaMemcpy(ws_.err.as<int32_t>() + 1, wait_ctl_, sizeof wait_ctl_,
+                         cudaMemcpyHostToDevice));
   return kOk;
 }
 
@@ -133,6 +142,21 @@ int Solver::factor(const double *Ax) {
   MPIR_CUDA(cudaMemcpyAsync(num_.Ax.as<void>(), Ax, plan_->S.nnz * sizeof(double),
                             cudaMemcpyHostToDevice, stream_));
   return factor_device(num_.Ax.as<double>());
+}
+
+void Solver::set_wait_controls(int poll_log2, int withhold_item) {
+  if (!plan_) throw std::logic_error("no analysed pattern");
+  MPIR_CUDA(cudaSetDevice(device));
+  wait_ctl_[0] = poll_log2;
+  wait_ctl_[1] = withhold_item < 0 ? 0 : withhold_item + 1;
+  // Words 1 and 2 of each workspace's SolveCtl (word 0 is the error flag);
+  // a several-vector workspace allocated later takes them in ensure_batch.
+  MPIR_CUDA(cudaMemcpyAsync(ws_.err.as<int32_t>() + 1, wait_ctl_, sizeof wait_ctl_,
+                            cudaMemcpyHostToDevice, stream_));
+  if (mws_.nr)
+    MPIR_CUDA(cudaMemcpyAsync(mws_.err.as<int32_t>() + 1, wait_ctl_, sizeof wait_ctl_,
+                              cudaMemcpyHostToDevice, stream_));
+  MPIR_CUDA(cudaStreamSynchronize(stream_));
 }
 
 // PrecondGmres, gmres_ir.hpp:636-741.

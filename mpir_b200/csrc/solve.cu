@@ -22,6 +22,7 @@
 #include "common.cuh"
 #include "engine.hpp"
 #include "solve.hpp"
+#include "solve_dev.cuh"
 
 namespace mpir {
 
@@ -35,20 +36,6 @@ constexpr int kSmallH      = kWarpSolveH;
 // this when it starts, so the product at the end of its wait chain reads
 // shared memory only, and each thread reads only what it copied itself.
 constexpr int kTri = kNB * (kNB + 1) / 2;
-
-__device__ __forceinline__ void cp_async8(double *dst, const double *src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(
-                   static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
-               "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async16(double *dst, const double *src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
-                   static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
-               "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() {
-  asm volatile("cp.async.wait_all;" ::: "memory");
-}
 
 // Thread layout of the forward block product: lane l of warp v takes row
 // i = 8 v + l / 4 of the block and its slice q = l % 4; the four slices of i
@@ -205,44 +192,10 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta)
 }
 
 
-// Block results go from the CTA that computes them to the CTAs that wait on
-// them through the ready buffer: each entry holds the pending marker (a
-// signalling NaN, which no arithmetic produces) until its value is stored,
-// and a waiting lane polls its own entry at GPU scope, so the value is its
-// own ready signal (no flag, no fence, no second load).  The producer stores
-// kReadyCopies copies; the warps of the ~150 CTAs that wait for the same
-// block poll different copies.  A wait gives up after a few seconds, sets
-// the sticky error word and returns 0; it looks at that word every 64 polls,
-// so one failure ends the launch quickly.
-constexpr unsigned long long kPending = 0x7ff0deadbeef0001ull;
-constexpr int kReadyCopies = 16;
-
-__device__ __forceinline__ unsigned long long ld_relaxed_u64(const double *p) {
-  unsigned long long v;
-  asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ void st_relaxed_f64(double *p, double v) {
-  asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(__double_as_longlong(v))
-               : "memory");
-}
-__device__ __forceinline__ double wait_value(const double *p, int32_t *err) {
-  for (long it = 0; it < (1L << 22); it++) {
-    const unsigned long long v = ld_relaxed_u64(p);
-    if (v != kPending) return __longlong_as_double(static_cast<long long>(v));
-    if ((it & 63) == 63) {
-      if (*reinterpret_cast<volatile int32_t *>(err) != 0) return 0.0;
-      __nanosleep(32);
-    }
-  }
-  atomicExch(err, 1);
-  return 0.0;
-}
-
 // Waits for this lane's entries p[lane + 32 i] (i < 4) of a block result, the
 // entries at or past lim reading as 0; each round polls all four at once.
 __device__ __forceinline__ void wait_block4(const double *p, int lim, double (&v)[4],
-                                            int32_t *err) {
+                                            int32_t *err, long polls) {
   const int lane = threadIdx.x % 32;
   unsigned  need = 0;
 #pragma unroll
@@ -250,7 +203,7 @@ __device__ __forceinline__ void wait_block4(const double *p, int lim, double (&v
     v[i] = 0.0;
     if (lane + 32 * i < lim) need |= 1u << i;
   }
-  for (long it = 0; need != 0 && it < (1L << 22); it++) {
+  for (long it = 0; need != 0 && it < polls; it++) {
     unsigned long long raw[4];
 #pragma unroll
     for (int i = 0; i < 4; i++) raw[i] = (need >> i & 1u) ? ld_relaxed_u64(p + lane + 32 * i) : 0ull;
@@ -271,8 +224,9 @@ __device__ __forceinline__ void wait_block4(const double *p, int lim, double (&v
 // The value at p from a load issued ahead (raw) when that load already saw
 // it, else the wait for it.
 __device__ __forceinline__ double take_value(unsigned long long raw, const double *p,
-                                             int32_t *err) {
-  return raw != kPending ? __longlong_as_double(static_cast<long long>(raw)) : wait_value(p, err);
+                                             int32_t *err, long polls) {
+  return raw != kPending ? __longlong_as_double(static_cast<long long>(raw))
+                         : wait_value(p, err, polls);
 }
 
 __global__ void k_mark_pending(int64_t n, double *ready) {
@@ -308,16 +262,22 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   // memory that took a round trip past an L1 the tiles had flushed.
   __shared__ SolveFront sF;
   __shared__ int        sR, sItem;
+  __shared__ long       sPolls;
+  __shared__ bool       sPublish;
   if (threadIdx.x == 0) {
     const int it = atomicAdd(tickets, 1);
     sItem        = it;
     sF           = items[it].f;
     sR           = items[it].r;
+    const volatile SolveCtl *c = reinterpret_cast<const volatile SolveCtl *>(err);
+    sPolls       = poll_limit(c->poll_log2);
+    sPublish     = c->withhold != it + 1;
   }
   __syncthreads();
   const int         item = sItem;
   const SolveFront &F    = sF;
   const int         R    = sR;
+  const long        polls = sPolls;
   if (R < F.nb)
     stage_lower(linv64t + F.linv + static_cast<int64_t>(R) * kNB * kNB, tri);
   const int     tid = threadIdx.x, rr = tid % kNB, qq = tid / kNB;
@@ -374,7 +334,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
     const int c0 = b * kNB + qq * 32;
     load_tile(lvn, b + 1);
     if (b + 2 < tiles) yvn = load_y(b + 1);
-    yw[warp][lane] = c0 + lane < w ? take_value(yv, yr + c0 + lane, err) : 0.0;
+    yw[warp][lane] = c0 + lane < w ? take_value(yv, yr + c0 + lane, err, polls) : 0.0;
     __syncwarp();
 #pragma unroll
     for (int k = 0; k < 32; k++) acc += static_cast<double>(lv[k]) * yw[warp][k];
@@ -393,7 +353,8 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
     for (int k = 0; k < 32; k++) ld[k] = static_cast<double>(lv[k]);
     if (warp % 4 == 0)
       ylast[qq * 32 + lane] =
-          c0 + lane < w ? wait_value(ready + ((item + qq) % kReadyCopies) * n + F.col0 + c0 + lane, err)
+          c0 + lane < w ? wait_value(ready + ((item + qq) % kReadyCopies) * n + F.col0 + c0 + lane,
+                                     err, polls)
                         : 0.0;
     asm volatile("bar.sync %0, %1;" ::"r"(1 + qq), "r"(kNB) : "memory");
 #pragma unroll
@@ -409,7 +370,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
     __syncthreads();
     const double y  = block_lower_apply(tri, ys);
     const int    iy = blk_i();
-    if (blk_q() == 0 && iy < nbk) {
+    if (blk_q() == 0 && iy < nbk && sPublish) {
       const int64_t j = F.col0 + R * kNB + iy;
 #pragma unroll
       for (int c = 0; c < kReadyCopies; c++) st_relaxed_f64(ready + c * n + j, y);
@@ -548,16 +509,19 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   // Ticket and item record as in k_fwd_fronts.
   __shared__ SolveFront sF;
   __shared__ int        sB, sItem;
+  __shared__ long       sPolls;
   if (threadIdx.x == 0) {
     const int it = atomicAdd(tickets, 1);
     sItem        = it;
     sF           = items[it].f;
     sB           = items[it].r;
+    sPolls       = poll_limit(reinterpret_cast<const volatile SolveCtl *>(err)->poll_log2);
   }
   __syncthreads();
   const int         item = sItem;
   const SolveFront &F    = sF;
   const int         b    = sB;
+  const long        polls = sPolls;
   stage_upper(linv64t + F.linv + static_cast<int64_t>(b) * kNB * kNB, tri,
               min(kNB, F.w - b * kNB));
   const int         tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
@@ -612,7 +576,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
 #pragma unroll
     for (int i = 0; i < 4; i++) {
       const int    rr = lane + 32 * i;
-      const double zv = rr < rows ? wait_value(xr + rb + rr, err) : 0.0;
+      const double zv = rr < rows ? wait_value(xr + rb + rr, err, polls) : 0.0;
 #pragma unroll
       for (int j = 0; j < 8; j++) acc[j] += static_cast<double>(lv[j][i]) * zv;
     }
@@ -633,7 +597,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
       for (int i = 0; i < 4; i++) ld[j][i] = static_cast<double>(lv[j][i]);
     if (warp == 0) {
       double xv[4];
-      wait_block4(ready + (item % kReadyCopies) * n + F.col0 + rb, rows, xv, err);
+      wait_block4(ready + (item % kReadyCopies) * n + F.col0 + rb, rows, xv, err, polls);
 #pragma unroll
       for (int i = 0; i < 4; i++) xlast[lane + 32 * i] = xv[i];
     }
@@ -690,8 +654,8 @@ void SolveWorkspace::allocate(const Plan &P) {
   part.resize(std::max<int64_t>(P.spart_elems, 1) * sizeof(double));
   sync.resize(std::max<int64_t>(P.sync_elems, 1) * sizeof(int32_t));
   ready.resize(std::max<int64_t>(kReadyCopies * P.S.n, 1) * sizeof(double));
-  err.resize(sizeof(int32_t));
-  MPIR_CUDA(cudaMemset(err.as<void>(), 0, sizeof(int32_t)));
+  err.resize(sizeof(SolveCtl));
+  MPIR_CUDA(cudaMemset(err.as<void>(), 0, sizeof(SolveCtl)));
   xbuf.resize(std::max<int64_t>(P.S.n, 1) * sizeof(double));
 }
 

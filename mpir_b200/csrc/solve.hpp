@@ -12,7 +12,8 @@ struct SolveWorkspace {
   DeviceBuffer sync;      // tickets (Plan::sync_elems int32)
   DeviceBuffer ready;     // block results for the CTAs that wait on them (n
                           // doubles, the pending marker until written)
-  DeviceBuffer err;       // int32, set to 1 when a bounded wait gave up
+  DeviceBuffer err;       // SolveCtl: err = 1 when a bounded wait gave up, then
+                          // the test controls of the waits (solve_dev.cuh)
   DeviceBuffer xbuf;      // fixed vector the captured solve works on
   cudaGraphExec_t graph = nullptr;  // captured L D L^T solve (all phases)
   int64_t graph_launches = 0;       // kernels one replay runs
@@ -34,6 +35,24 @@ void ldlt_solve(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
 // into and out of the workspace vector the graph was captured on.
 void ldlt_solve_graph(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
                       cudaStream_t s, cudaStream_t capture_stream);
+
+// Workspace of the several-vector solves (solve_multi.cu) for one width.
+struct MultiSolveWorkspace {
+  int          nr = 0;  // vectors per application (4, 8 or 16)
+  DeviceBuffer zbuf, part, sync, ready, err;
+  void         allocate(const Plan &P, int width);
+  static size_t bytes_for(const Plan &P, int width);
+};
+
+// Vectors per several-vector application for nrhs right-hand sides (the
+// kernels are instantiated for 4, 8 and 16; unused columns are zero).
+int multi_width(int nrhs);
+
+// X (n x width, column-major, leading dimension n, permuted order, float64,
+// device) <- (L D L^T)^{-1} X, or the phases selected, for all width columns
+// at once (solve_multi.cu).
+void ldlt_solve_multi(const Plan &P, const Numeric &F, double *X, int width,
+                      MultiSolveWorkspace &ws, cudaStream_t s, int phases = kAllPhases);
 
 // QDLDL_solve (float32 factor, float64 x, host arrays) whose device data
 // lives in a fixed file-scope array instead of allocated memory; see

@@ -14,6 +14,11 @@ namespace mpir {
 
 enum Prec : int { kF64 = 0, kF32 = 1, kBF16 = 2, kF16 = 3, kDD = 4 };
 
+// A bounded device wait of the triangular solves ran out (status -5).
+struct WaitTimeout : std::runtime_error {
+  WaitTimeout() : std::runtime_error("a bounded device wait of the triangular solves ran out") {}
+};
+
 struct Report {
   int32_t status           = 0;
   int32_t ir_iterations    = 0;
@@ -63,6 +68,17 @@ class Solver {
   // Device entry points (caller arrays already on this device).
   int factor_device(const double *d_Ax);
   int solve_device(const double *d_b, double *d_x, Report *rep);
+  // nrhs GMRES-IR solves in lockstep (gmres_batch.cu): B and X hold nrhs
+  // vectors of length n (column-major, caller order, device); every
+  // preconditioner application takes all of them at once.  reps: nrhs
+  // reports (NULL allowed).  nrhs <= kMaxBatch.
+  int solve_batch_device(int nrhs, const double *d_B, double *d_X, Report *reps);
+  int solve_batch(int nrhs, const double *B, double *X, Report *reps);
+  // X (n x nrhs, column-major, the solver's permuted and scaled order,
+  // device) <- (L D L^T)^{-1} X with the current factor: one vector by the
+  // single-vector kernels, several by the several-vector kernels.
+  void precond_device(int nrhs, double *d_X);
+  static constexpr int kMaxBatch = 16;
   // Plain iterative refinement with the factor (LUIR_QDLDL); host and
   // device vectors.
   int luir(const double *b, double *x, int maxiter, Report *rep);
@@ -71,6 +87,10 @@ class Solver {
   std::string dump_log();
 
   void set_stream(cudaStream_t s) { stream_ = s ? s : own_stream_; }
+  // Test controls of the bounded waits (SolveCtl): 2^poll_log2 polls per
+  // wait (0: the default), and the work item of the forward block solves
+  // whose result is not published (-1: none).  For failure tests only.
+  void set_wait_controls(int poll_log2, int withhold_item);
   cudaStream_t stream() const { return stream_; }
 
   bool analyzed() const { return plan_ != nullptr; }
@@ -85,6 +105,12 @@ class Solver {
  private:
   void precond_gmres(const double *b, double *res, Report &st);
   void ensure_vectors();
+  // Batched GMRES (gmres_batch.cu): vectors of the batch k*n apart inside
+  // blocks of width bw_ (n * bw_ doubles per block).
+  void ensure_batch(int width);
+  void precond_gmres_batch(int nb, const double *b, double *res, std::vector<Report> &st,
+                           const std::vector<int32_t> &active);
+  void multi_apply(double *block);
 
   cudaStream_t          own_stream_ = nullptr, stream_ = nullptr;
   std::unique_ptr<Plan> plan_;
@@ -93,6 +119,16 @@ class Solver {
   VecOps                vec_;
   DeviceBuffer          V_, bs_, bp_, ADp_, x_, r_, t_, d_, hd_, y_, hb_, hx_;
   int64_t               vec_m_ = -1;
+  // Batch state: width, basis and vectors, host staging of the per-vector
+  // scalars (pinned), the several-vector solve workspace.
+  int                   bw_ = 0;
+  int64_t               bm_ = -1;
+  VecOps                vecb_;
+  MultiSolveWorkspace   mws_;
+  DeviceBuffer          bV_, bbs_, bbp_, bx_, br_, bt_, bd_, bhd_, by_, bfac_, bact_, bkq_, bin_,
+                        bout_, bpre_;
+  double               *hpin_ = nullptr;  // pinned host scalars (fac, y, act, kq)
+  int32_t               wait_ctl_[2] = {0, 0};  // SolveCtl words 1-2 (set_wait_controls)
   cudaEvent_t           ev0_ = nullptr, ev1_ = nullptr;
   std::vector<IrEvent>  log_;
 };

@@ -65,10 +65,24 @@ __device__ __forceinline__ void warp_max_abs(unsigned long long *slot, double v,
 //   MODE 0: y = K x
 //   MODE 1: y = b - K x,           max|y| into inf[0]
 //   MODE 2: y = b - K x in double-double, rounded to float64, max into inf[0]
+//
+// Batched form (all kernels below): blockIdx.y selects vector k of a batch,
+// the vectors k*vs apart, its max-norm slots at inf + 8k, and k is skipped
+// when act[k] == 0 (act NULL: every k).  One vector is gridDim.y == 1.
+__device__ __forceinline__ bool batch_skip(const int32_t *vact) {
+  return vact != nullptr && vact[blockIdx.y] == 0;
+}
+
 template <int G, int MODE>
 __global__ void k_spmv(int64_t n, const int64_t *Kp, const int32_t *Kj,
                        const double *Kv, const double *x, const double *b,
-                       double *y, unsigned long long *inf) {
+                       double *y, unsigned long long *inf, int64_t vs,
+                       const int32_t *vact) {
+  if (batch_skip(vact)) return;
+  x += blockIdx.y * vs;
+  y += blockIdx.y * vs;
+  if (b) b += blockIdx.y * vs;
+  if (inf) inf += 8 * blockIdx.y;
   const int64_t gid  = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const int64_t row  = gid / G;
   const int     lane = threadIdx.x % G;
@@ -117,7 +131,12 @@ template <int G>
 __global__ void k_backward_terms(int64_t n, const int64_t *Kp, const int32_t *Kj,
                                  const double *Korig, const double *x,
                                  const double *ADp, const double *b,
-                                 unsigned long long *inf) {
+                                 unsigned long long *inf, int64_t vs,
+                                 const int32_t *vact) {
+  if (batch_skip(vact)) return;
+  x += blockIdx.y * vs;
+  b += blockIdx.y * vs;
+  inf += 8 * blockIdx.y;
   const int64_t gid  = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const int64_t row  = gid / G;
   const int     lane = threadIdx.x % G;
@@ -214,11 +233,24 @@ __device__ __forceinline__ bool last_block(unsigned int *count) {
 
 // MGS pass: w -= h * v (h read from *hsrc, skipped when hsrc is null), then
 // either dot(w, u) (mode 0) or ||w||_2 (mode 1) into *out.
+// Batched: vectors k*vs apart, h and out k*hs apart, scratch part + 2048 k
+// and count + k.
 __global__ void __launch_bounds__(kRedThreads)
     k_mgs_pass(int64_t n, double *w, const double *v, const double *hsrc,
                const double *u, int mode, double *part, unsigned int *count,
-               double *out) {
+               double *out, int64_t vs, int64_t hs, const int32_t *vact) {
   __shared__ double sh[2 * kRedThreads / 32];
+  if (batch_skip(vact)) return;
+  {
+    const int64_t k = blockIdx.y;
+    w += k * vs;
+    if (v) v += k * vs;
+    if (u) u += k * vs;
+    if (hsrc) hsrc += k * hs;
+    out += k * hs;
+    part += 2048 * k;
+    count += k;
+  }
   const double      h = hsrc ? *hsrc : 0.0;
   double            acc = 0.0, sc = 0.0, sq = 1.0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
@@ -262,15 +294,28 @@ __global__ void __launch_bounds__(kRedThreads)
   if (threadIdx.x == 0) *count = 0;
 }
 
-// y = a * x (a read from the host argument).
-__global__ void k_scale(int64_t n, const double *x, double a, double *y) {
+// y = a * x (a the host argument, or fac[k] for vector k when fac is given).
+__global__ void k_scale(int64_t n, const double *x, double a, double *y, int64_t vs,
+                        const double *fac, const int32_t *vact) {
+  if (batch_skip(vact)) return;
+  x += blockIdx.y * vs;
+  y += blockIdx.y * vs;
+  if (fac) a = fac[blockIdx.y];
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) y[i] = x[i] * a;
 }
 
 // res = sum_j V_j y_j for j < k (gmres_ir.hpp:735-739).
+// Batched: vector q's basis at V + q*vs (ldv apart), its coefficients at
+// y + q*ys and its count kq[q] (kq NULL: k for all).
 __global__ void k_combine(int64_t n, const double *V, int64_t ldv, int k,
-                          const double *y, double *res) {
+                          const double *y, double *res, int64_t vs, int64_t ys,
+                          const int32_t *kq, const int32_t *vact) {
+  if (batch_skip(vact)) return;
+  V += blockIdx.y * vs;
+  res += blockIdx.y * vs;
+  y += blockIdx.y * ys;
+  if (kq) k = kq[blockIdx.y];
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   double r = 0.0;
@@ -281,7 +326,13 @@ __global__ void k_combine(int64_t n, const double *V, int64_t ldv, int k,
 // d *= scale; inf[0] = max|d|; inf[1] = max|x_old|; x += d
 // (gmres_ir.hpp:574-577).
 __global__ void k_ir_update(int64_t n, double *d, double scale, double *x,
-                            const double *w, unsigned long long *inf) {
+                            const double *w, unsigned long long *inf, int64_t vs,
+                            const double *fac, const int32_t *vact) {
+  if (batch_skip(vact)) return;
+  d += blockIdx.y * vs;
+  x += blockIdx.y * vs;
+  inf += 8 * blockIdx.y;
+  if (fac) scale = fac[blockIdx.y];
   const int64_t i   = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const bool    act = i < n;
   double        di = 0.0, xi = 0.0, wi = 1.0;
@@ -311,9 +362,15 @@ __global__ void k_round_to(int64_t n, int prec, double *x) {
 
 // bs[i] = b[perm[i]] * AD[perm[i]]; ADp[i] = AD[perm[i]]; bp[i] = b[perm[i]];
 // inf[0] = max|bs|.
+// Batched: b, bs, bp of vector k at k*vs; ADp is written by k == 0 only.
 __global__ void k_rhs_in(int64_t n, const int64_t *perm, const double *AD,
                          const double *b, double *bs, double *ADp, double *bp,
-                         unsigned long long *inf) {
+                         unsigned long long *inf, int64_t vs) {
+  b += blockIdx.y * vs;
+  bs += blockIdx.y * vs;
+  bp += blockIdx.y * vs;
+  inf += 8 * blockIdx.y;
+  if (blockIdx.y != 0) ADp = nullptr;
   const int64_t i   = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const bool    act = i < n;
   double        v   = 0.0;
@@ -322,7 +379,7 @@ __global__ void k_rhs_in(int64_t n, const int64_t *perm, const double *AD,
     const double  a = AD[o];
     v               = b[o] * a;
     bs[i]           = v;
-    ADp[i]          = a;
+    if (ADp) ADp[i] = a;
     bp[i]           = b[o];
   }
   warp_max_abs(inf, v, act);
@@ -330,7 +387,9 @@ __global__ void k_rhs_in(int64_t n, const int64_t *perm, const double *AD,
 
 // out[perm[i]] = x[i] * ADp[i].
 __global__ void k_sol_out(int64_t n, const int64_t *perm, const double *ADp,
-                          const double *x, double *out) {
+                          const double *x, double *out, int64_t vs) {
+  x += blockIdx.y * vs;
+  out += blockIdx.y * vs;
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) out[perm[i]] = x[i] * ADp[i];
 }
@@ -341,19 +400,107 @@ static unsigned blocks_for(int64_t n, int t) {
   return static_cast<unsigned>(std::max<int64_t>(1, (n + t - 1) / t));
 }
 
-void VecOps::allocate(int64_t n_, int sms) {
+void VecOps::allocate(int64_t n_, int sms, int batch_) {
   n       = n_;
+  batch   = std::max(batch_, 1);
   nblocks = std::max(1, std::min<int>(2 * sms, static_cast<int>((n + kRedThreads - 1) / kRedThreads)));
-  part.resize(sizeof(double) * 2 * 1024);
-  count.resize(sizeof(unsigned int));
-  infbits.resize(sizeof(unsigned long long) * 8);
-  MPIR_CUDA(cudaMemset(count.as<void>(), 0, sizeof(unsigned int)));
+  part.resize(sizeof(double) * 2048 * batch);
+  count.resize(sizeof(unsigned int) * batch);
+  infbits.resize(sizeof(unsigned long long) * 8 * batch);
+  MPIR_CUDA(cudaMemset(count.as<void>(), 0, sizeof(unsigned int) * batch));
+}
+
+// Zeroes slots [first, first + cnt) of banks 0 .. nb-1.
+static void clear_slots(unsigned long long *bits, int nb, int first, int cnt, cudaStream_t s) {
+  MPIR_CUDA(cudaMemset2DAsync(bits + first, 8 * sizeof(unsigned long long), 0,
+                              cnt * sizeof(unsigned long long), nb, s));
+}
+
+static dim3 grid_b(int64_t work, int threads, int nb) {
+  return dim3(blocks_for(work, threads), static_cast<unsigned>(nb), 1);
+}
+
+void VecOps::spmv_b(int nb, const int64_t *Kp, const int32_t *Kj, const double *Kv,
+                    const double *x, double *y, int64_t vs, const int32_t *act,
+                    cudaStream_t s) {
+  constexpr int G = 8;
+  launch(k_spmv<G, 0>, grid_b(n * G, 256, nb), 256, 0, s, n, Kp, Kj, Kv, x, nullptr, y,
+         nullptr, vs, act);
+}
+
+void VecOps::residual_b(int nb, const int64_t *Kp, const int32_t *Kj, const double *Kv,
+                        const double *x, const double *b, double *r, bool dd, int64_t vs,
+                        const int32_t *act, cudaStream_t s) {
+  constexpr int G = 8;
+  unsigned long long *inf = infbits.as<unsigned long long>();
+  clear_slots(inf, nb, 0, 1, s);
+  if (dd)
+    launch(k_spmv<G, 2>, grid_b(n * G, 256, nb), 256, 0, s, n, Kp, Kj, Kv, x, b, r, inf, vs,
+           act);
+  else
+    launch(k_spmv<G, 1>, grid_b(n * G, 256, nb), 256, 0, s, n, Kp, Kj, Kv, x, b, r, inf, vs,
+           act);
+}
+
+void VecOps::backward_terms_b(int nb, const int64_t *Kp, const int32_t *Kj, const double *Korig,
+                              const double *x, const double *ADp, const double *bp, int64_t vs,
+                              cudaStream_t s) {
+  constexpr int G = 8;
+  unsigned long long *inf = infbits.as<unsigned long long>();
+  clear_slots(inf, nb, 4, 4, s);
+  launch(k_backward_terms<G>, grid_b(n * G, 256, nb), 256, 0, s, n, Kp, Kj, Korig, x, ADp, bp,
+         inf + 4, vs, static_cast<const int32_t *>(nullptr));
+}
+
+void VecOps::mgs_pass_b(int nb, double *w, const double *v, const double *hsrc, const double *u,
+                        int mode, double *out, int64_t vs, int64_t hs, const int32_t *act,
+                        cudaStream_t s) {
+  launch(k_mgs_pass, dim3(nblocks, nb, 1), kRedThreads, 0, s, n, w, v, hsrc, u, mode,
+         part.as<double>(), count.as<unsigned int>(), out, vs, hs, act);
+}
+
+void VecOps::scale_b(int nb, const double *x, const double *fac, double *y, int64_t vs,
+                     const int32_t *act, cudaStream_t s) {
+  launch(k_scale, grid_b(n, 256, nb), 256, 0, s, n, x, 0.0, y, vs, fac, act);
+}
+
+void VecOps::combine_b(int nb, const double *V, int64_t ldv, const double *y, int64_t ys,
+                       const int32_t *kq, double *res, int64_t vs, const int32_t *act,
+                       cudaStream_t s) {
+  launch(k_combine, grid_b(n, 256, nb), 256, 0, s, n, V, ldv, 0, y, res, vs, ys, kq, act);
+}
+
+void VecOps::ir_update_b(int nb, double *d, const double *fac, double *x, int64_t vs,
+                         const int32_t *act, cudaStream_t s, const double *w) {
+  unsigned long long *inf = infbits.as<unsigned long long>();
+  clear_slots(inf, nb, 1, 2, s);
+  launch(k_ir_update, grid_b(n, 256, nb), 256, 0, s, n, d, 0.0, x, w, inf + 1, vs, fac, act);
+}
+
+void VecOps::rhs_in_b(int nb, const int64_t *perm, const double *AD, const double *b, double *bs,
+                      double *ADp, double *bp, int64_t vs, cudaStream_t s) {
+  unsigned long long *inf = infbits.as<unsigned long long>();
+  clear_slots(inf, nb, 3, 1, s);
+  launch(k_rhs_in, grid_b(n, 256, nb), 256, 0, s, n, perm, AD, b, bs, ADp, bp, inf + 3, vs);
+}
+
+void VecOps::sol_out_b(int nb, const int64_t *perm, const double *ADp, const double *x,
+                       double *out, int64_t vs, cudaStream_t s) {
+  launch(k_sol_out, grid_b(n, 256, nb), 256, 0, s, n, perm, ADp, x, out, vs);
+}
+
+void VecOps::read_inf_b(int nb, double *h, cudaStream_t s) {
+  static_assert(sizeof(double) == sizeof(unsigned long long), "bit copy");
+  MPIR_CUDA(cudaMemcpyAsync(h, infbits.as<void>(), nb * 8 * sizeof(double), cudaMemcpyDeviceToHost,
+                            s));
+  MPIR_CUDA(cudaStreamSynchronize(s));
 }
 
 void VecOps::spmv(const int64_t *Kp, const int32_t *Kj, const double *Kv,
                   const double *x, double *y, cudaStream_t s) {
   constexpr int G = 8;
-  launch(k_spmv<G, 0>, blocks_for(n * G, 256), 256, 0, s, n, Kp, Kj, Kv, x, nullptr, y, nullptr);
+  launch(k_spmv<G, 0>, blocks_for(n * G, 256), 256, 0, s, n, Kp, Kj, Kv, x, nullptr, y, nullptr,
+         int64_t{0}, nullptr);
 }
 
 void VecOps::residual(const int64_t *Kp, const int32_t *Kj, const double *Kv,
@@ -363,9 +510,11 @@ void VecOps::residual(const int64_t *Kp, const int32_t *Kj, const double *Kv,
   unsigned long long *inf = infbits.as<unsigned long long>() + slot;
   MPIR_CUDA(cudaMemsetAsync(inf, 0, sizeof(unsigned long long), s));
   if (dd)
-    launch(k_spmv<G, 2>, blocks_for(n * G, 256), 256, 0, s, n, Kp, Kj, Kv, x, b, r, inf);
+    launch(k_spmv<G, 2>, blocks_for(n * G, 256), 256, 0, s, n, Kp, Kj, Kv, x, b, r, inf,
+           int64_t{0}, nullptr);
   else
-    launch(k_spmv<G, 1>, blocks_for(n * G, 256), 256, 0, s, n, Kp, Kj, Kv, x, b, r, inf);
+    launch(k_spmv<G, 1>, blocks_for(n * G, 256), 256, 0, s, n, Kp, Kj, Kv, x, b, r, inf,
+           int64_t{0}, nullptr);
 }
 
 void VecOps::backward_terms(const int64_t *Kp, const int32_t *Kj, const double *Korig,
@@ -374,28 +523,31 @@ void VecOps::backward_terms(const int64_t *Kp, const int32_t *Kj, const double *
   constexpr int G = 8;
   unsigned long long *inf = infbits.as<unsigned long long>() + 4;
   MPIR_CUDA(cudaMemsetAsync(inf, 0, 4 * sizeof(unsigned long long), s));
-  launch(k_backward_terms<G>, blocks_for(n * G, 256), 256, 0, s, n, Kp, Kj, Korig, x, ADp, bp, inf);
+  launch(k_backward_terms<G>, blocks_for(n * G, 256), 256, 0, s, n, Kp, Kj, Korig, x, ADp, bp, inf,
+         int64_t{0}, nullptr);
 }
 
 void VecOps::mgs_pass(double *w, const double *v, const double *hsrc, const double *u,
                       int mode, double *out, cudaStream_t s) {
   launch(k_mgs_pass, nblocks, kRedThreads, 0, s, n, w, v, hsrc, u, mode, part.as<double>(),
-                                             count.as<unsigned int>(), out);
+         count.as<unsigned int>(), out, int64_t{0}, int64_t{0}, nullptr);
 }
 
 void VecOps::scale(const double *x, double a, double *y, cudaStream_t s) {
-  launch(k_scale, blocks_for(n, 256), 256, 0, s, n, x, a, y);
+  launch(k_scale, blocks_for(n, 256), 256, 0, s, n, x, a, y, int64_t{0}, nullptr, nullptr);
 }
 
 void VecOps::combine(const double *V, int64_t ldv, int k, const double *y, double *res,
                      cudaStream_t s) {
-  launch(k_combine, blocks_for(n, 256), 256, 0, s, n, V, ldv, k, y, res);
+  launch(k_combine, blocks_for(n, 256), 256, 0, s, n, V, ldv, k, y, res, int64_t{0}, int64_t{0},
+         nullptr, nullptr);
 }
 
 void VecOps::ir_update(double *d, double scale, double *x, cudaStream_t s, const double *w) {
   unsigned long long *inf = infbits.as<unsigned long long>() + 1;
   MPIR_CUDA(cudaMemsetAsync(inf, 0, 2 * sizeof(unsigned long long), s));
-  launch(k_ir_update, blocks_for(n, 256), 256, 0, s, n, d, scale, x, w, inf);
+  launch(k_ir_update, blocks_for(n, 256), 256, 0, s, n, d, scale, x, w, inf, int64_t{0}, nullptr,
+         nullptr);
 }
 
 void VecOps::round_to(int prec, double *x, cudaStream_t s) {
@@ -407,12 +559,12 @@ void VecOps::rhs_in(const int64_t *perm, const double *AD, const double *b, doub
                     double *ADp, double *bp, cudaStream_t s) {
   unsigned long long *inf = infbits.as<unsigned long long>() + 3;
   MPIR_CUDA(cudaMemsetAsync(inf, 0, sizeof(unsigned long long), s));
-  launch(k_rhs_in, blocks_for(n, 256), 256, 0, s, n, perm, AD, b, bs, ADp, bp, inf);
+  launch(k_rhs_in, blocks_for(n, 256), 256, 0, s, n, perm, AD, b, bs, ADp, bp, inf, int64_t{0});
 }
 
 void VecOps::sol_out(const int64_t *perm, const double *ADp, const double *x, double *out,
                      cudaStream_t s) {
-  launch(k_sol_out, blocks_for(n, 256), 256, 0, s, n, perm, ADp, x, out);
+  launch(k_sol_out, blocks_for(n, 256), 256, 0, s, n, perm, ADp, x, out, int64_t{0});
 }
 
 void VecOps::read_inf(double *h, int first, int cnt, cudaStream_t s) {

@@ -244,6 +244,9 @@ class Reference(_Common):
             f.restype = C.c_int
             f.argtypes = [_i64, _i64p, _i64p, _f64p, _f64p, _f64p, _i64, _i64, C.c_double,
                           _f64p, _f64p]
+        L.ref_gmres_ir_f32_ex.restype = C.c_int
+        L.ref_gmres_ir_f32_ex.argtypes = [_i64, _i64p, _i64p, _f64p, _f64p, _f64p, _i64, _i64,
+                                          C.c_double, _f64p, _f64p, _f32p, _f32p]
 
     def etree(self, n, Ap, Ai):
         Ap, Ai = _i(Ap), _i(Ai)
@@ -331,6 +334,29 @@ class Reference(_Common):
             raise RuntimeError(f"reference gmres_ir failed: {r}")
         keys = ("factor_s", "solve_s", "ir_steps", "reorth", "nnzL", "npos")
         return x, AD, dict(zip(keys, info.tolist()))
+
+    def gmres_ir_with_factor(self, n, Ap, Ai, Ax, b, ir_iter=10, gmres_iter=10, tol=1e-10):
+        """As gmres_ir with UF = float, also returning the reference's float32
+        QDLDL factor of the scaled matrix it preconditions with.
+
+        Returns (x, AD, info, Lx, D): info adds etree_s (QDLDL_etree) and
+        compute_s (the shipped Compute, run only for the diagonal scaling);
+        Lx is in QDLDL's CSC order for the pattern of QDLDL_etree on (Ap, Ai)."""
+        s, Lnz, _ = self.etree(n, Ap, Ai)
+        if s < 0:
+            raise RuntimeError(f"reference etree failed: {s}")
+        x = np.zeros(n, np.float64)
+        AD = np.zeros(n, np.float64)
+        info = np.zeros(8, np.float64)
+        Lx = np.zeros(max(s, 1), np.float32)
+        D = np.zeros(max(n, 1), np.float32)
+        r = self.lib.ref_gmres_ir_f32_ex(n, _i(Ap), _i(Ai), _d(Ax), _d(b), x, int(ir_iter),
+                                         int(gmres_iter), float(tol), AD, info, Lx, D)
+        if r != 0:
+            raise RuntimeError(f"reference gmres_ir failed: {r}")
+        keys = ("factor_s", "solve_s", "ir_steps", "reorth", "nnzL", "npos", "etree_s",
+                "compute_s")
+        return x, AD, dict(zip(keys, info.tolist())), Lx[:s], D[:n]
 
     def time_factor_leading(self, k, Ap, Ai, Ax):
         return self.lib.ref_time_factor_leading_f32(int(k), _i(Ap), _i(Ai), _d(Ax))

@@ -249,21 +249,31 @@ void ref_vector_op(int op, I n, const double *a, const double *b, double *c) {
 }  // extern "C"
 
 // ---- GMRES-IR preconditioned by the QDLDL factor -----------------------------
+// Optional outputs: the QDLDL factor of the scaled matrix (L_out / D_out:
+// nnz(L) and n entries of T, NULL to skip) and info entries 6 and 7 (the
+// QDLDL_etree seconds and the seconds of the shipped Compute, which the
+// harness runs only for the diagonal scaling) when info_len >= 8.
 template <class S>
 static int gmres_ir(I n, const I *Ap, const I *Ai, const double *Ax,
                     const double *b, double *x_out, I ir_iter, I gmres_iter,
-                    double tol, double *AD_out, double *info) {
+                    double tol, double *AD_out, double *info,
+                    typename Members<S>::T *L_out = nullptr,
+                    typename Members<S>::T *D_out = nullptr, int info_len = 6) {
   using M = Members<S>;
   using T = typename M::T;
   S  s;
   VZ ap(Ap, Ap + n + 1), ai(Ai, Ai + Ap[n]);
   VD ax(Ax, Ax + Ap[n]);
+  const double tc0 = now_s();
   s.template Compute<double, (std::size_t{1} << 21), 1, 64>(ap, ai, ax, 0);
+  const double tc1 = now_s();
 
   // QDLDL on the scaled matrix the solver holds.
   const VD      &axs = M::Ax(s);
   std::vector<I> work(n), Lnz(n), et(n);
+  const double   te0 = now_s();
   I sum = QDLDL_etree<I>(n, Ap, Ai, work.data(), Lnz.data(), et.data());
+  const double   te1 = now_s();
   if (sum < 0) return -1;
   std::vector<I> Lp(n + 1), Li(sum > 0 ? sum : 1);
   std::vector<T> Lx(sum > 0 ? sum : 1), D(n), Dinv(n);
@@ -272,6 +282,12 @@ static int gmres_ir(I n, const I *Ap, const I *Ai, const double *Ax,
                        D.data(), Dinv.data(), Lnz.data(), et.data());
   const double t1 = now_s();
   if (pos < 0) return -2;
+  if (L_out && sum > 0) std::memcpy(L_out, Lx.data(), sizeof(T) * sum);
+  if (D_out) std::memcpy(D_out, D.data(), sizeof(T) * n);
+  if (info && info_len >= 8) {
+    info[6] = te1 - te0;
+    info[7] = tc1 - tc0;
+  }
 
   // CSR of strictly lower L = transpose of QDLDL's CSC.
   VZ             rp(n + 1, 0), ci(sum > 0 ? sum : 0);
@@ -335,6 +351,16 @@ int ref_gmres_ir_f64(I n, const I *Ap, const I *Ai, const double *Ax,
                      double tol, double *AD_out, double *info) {
   return gmres_ir<S64>(n, Ap, Ai, Ax, b, x, ir_iter, gmres_iter, tol, AD_out,
                        info);
+}
+// As ref_gmres_ir_f32, also returning the float32 factor values of the scaled
+// matrix (Lx in QDLDL's CSC order, D) and info[6] = QDLDL_etree seconds,
+// info[7] = seconds of the shipped Compute (info holds 8 entries).
+int ref_gmres_ir_f32_ex(I n, const I *Ap, const I *Ai, const double *Ax,
+                        const double *b, double *x, I ir_iter, I gmres_iter,
+                        double tol, double *AD_out, double *info, float *Lx,
+                        float *D) {
+  return gmres_ir<S32>(n, Ap, Ai, Ax, b, x, ir_iter, gmres_iter, tol, AD_out,
+                       info, Lx, D, 8);
 }
 }  // extern "C"
 
