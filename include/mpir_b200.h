@@ -277,6 +277,15 @@ int mpir_solver_supernodes(mpir_solver s, int64_t *sfirst, int64_t *srowptr,
 int mpir_solver_export_factor(mpir_solver s, int64_t *Lp, int64_t *Li,
                               float *Lx, float *D, float *Dinv);
 
+/* The leading k x k block of the factor (columns < k, rows < k) in QDLDL's
+ * CSC form for the permuted matrix: Lp (k+1), Li/Lx (*nnz entries), D (k).
+ * QDLDL_factor computes row r of L from rows < r (qdldl.hpp:228-342), so
+ * this block is the reference's factor of the leading k x k block.  Pass
+ * Li = Lx = NULL first to learn *nnz. */
+int mpir_solver_export_factor_leading(mpir_solver s, int64_t k, int64_t *Lp,
+                                      int64_t *Li, float *Lx, float *D,
+                                      int64_t *nnz);
+
 /* Host-only symbolic analysis (no device needed): the permutation, the
  * elimination tree and column counts of P K P^T, its upper CSC (Cp: n+1, Ci:
  * nnz_upper) and the exact pattern of L in QDLDL's CSC form (Lp: n+1, Li:
@@ -286,6 +295,72 @@ int mpir_analyze_host(int64_t n, const int64_t *Ap, const int64_t *Ai,
                       const double *Ax, int ordering, int64_t *perm,
                       int64_t *etree, int64_t *Lnz, int64_t *Cp, int64_t *Ci,
                       int64_t *Lp, int64_t *Li, mpir_info *info);
+
+/* ---- Serving engine ------------------------------------------------------ */
+/* A request stream of GMRES-IR solves (each one the reference's
+ * GmresLDLIR::Compute + Solve, gmres_ir.hpp:323 and :534-634) served on one
+ * GPU by worker threads with a stream each.  Requests name their pattern and
+ * values by caller-chosen keys; the engine keeps analysed patterns and
+ * factors resident (least recently used evicted first when a new factor
+ * does not fit the device-memory budget), solves the queued requests on one
+ * factor together (up to max_batch right-hand sides in lockstep, as
+ * mpir_solver_solve_batch), and runs requests on different factors
+ * concurrently.  A request whose factor alone exceeds the budget is refused
+ * (status MPIR_ERR_NOMEM in its result). */
+typedef struct mpir_server_s *mpir_server;
+
+typedef struct mpir_server_config {
+  int32_t device;
+  int32_t uf;          /* MPIR_F32, MPIR_BF16 or MPIR_F16 */
+  int32_t ur;          /* MPIR_F64 or MPIR_DD */
+  int32_t workers;     /* concurrent jobs (host threads, one CUDA stream each) */
+  int32_t max_batch;   /* right-hand sides per lockstep solve, 1 .. 16 */
+  int32_t pad;
+  int64_t budget_bytes;           /* device memory for plans and factors */
+  int64_t max_ir_iterations;      /* GmresLDLIR setters (gmres_ir.hpp:291-303) */
+  int64_t max_gmres_iterations;
+  double  tolerance;
+} mpir_server_config;
+
+/* The system (upper CSC in the caller's order), its right-hand side and the
+ * output vector: all host arrays, valid until the request is done.
+ * pattern_key names (n, Ap, Ai) and values_key the values Ax on it: equal
+ * keys must mean equal arrays. */
+typedef struct mpir_server_request {
+  uint64_t       pattern_key, values_key;
+  int64_t        n;
+  const int64_t *Ap, *Ai;
+  const double  *Ax, *b;
+  double        *x;
+} mpir_server_request;
+
+typedef struct mpir_server_result {
+  int64_t     id;
+  int32_t     status;   /* as the solver's entry points */
+  int32_t     path;     /* 0 resident factor, 1 refactorization, 2 new pattern */
+  int32_t     batch;    /* right-hand sides solved in the same lockstep solve */
+  int32_t     pad;
+  double      latency_ms, queue_ms, service_ms;  /* submit -> done, -> start */
+  mpir_report report;
+} mpir_server_result;
+
+typedef struct mpir_server_stats {
+  int64_t submitted, completed, failed, refused;
+  int64_t analyses, factorizations, solves, batched_solves, batched_rhs;
+  int64_t evictions, resident_factors, resident_patterns, queued;
+  int64_t bytes_in_use, peak_bytes;
+} mpir_server_stats;
+
+int mpir_server_create(mpir_server *out, const mpir_server_config *cfg);
+/* Queues a request and returns at once with its id. */
+int mpir_server_submit(mpir_server s, const mpir_server_request *r, int64_t *id);
+/* Blocks until request id is done and returns its result (once). */
+int mpir_server_wait(mpir_server s, int64_t id, mpir_server_result *res);
+/* Blocks until every submitted request is done. */
+int mpir_server_drain(mpir_server s);
+int mpir_server_get_stats(mpir_server s, mpir_server_stats *out);
+/* Drains, then frees every resident plan and factor. */
+int mpir_server_destroy(mpir_server s);
 
 /* ---- Kernel timing (benchmark support) ----------------------------------- */
 /* Classes: 0 small fronts, 1 diagonal blocks, 2 panel solve, 3 trailing

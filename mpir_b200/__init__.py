@@ -67,6 +67,35 @@ class Info(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("device", C.c_int32), ("uf", C.c_int32), ("ur", C.c_int32),
+                ("workers", C.c_int32), ("max_batch", C.c_int32), ("pad", C.c_int32),
+                ("budget_bytes", C.c_int64), ("max_ir_iterations", C.c_int64),
+                ("max_gmres_iterations", C.c_int64), ("tolerance", C.c_double)]
+
+
+class ServerRequest(C.Structure):
+    _fields_ = [("pattern_key", C.c_uint64), ("values_key", C.c_uint64), ("n", C.c_int64),
+                ("Ap", C.c_void_p), ("Ai", C.c_void_p), ("Ax", C.c_void_p), ("b", C.c_void_p),
+                ("x", C.c_void_p)]
+
+
+class ServerResult(C.Structure):
+    _fields_ = [("id", C.c_int64), ("status", C.c_int32), ("path", C.c_int32),
+                ("batch", C.c_int32), ("pad", C.c_int32), ("latency_ms", C.c_double),
+                ("queue_ms", C.c_double), ("service_ms", C.c_double), ("report", Report)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(k, C.c_int64) for k in (
+        "submitted", "completed", "failed", "refused", "analyses", "factorizations", "solves",
+        "batched_solves", "batched_rhs", "evictions", "resident_factors", "resident_patterns",
+        "queued", "bytes_in_use", "peak_bytes")]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _lib = None
 
 
@@ -113,8 +142,15 @@ def lib():
         "mpir_solver_info": (i32, [vp, vp]),
         "mpir_solver_symbolic": (i32, [vp, vp, vp, vp, vp, vp, vp]),
         "mpir_solver_export_factor": (i32, [vp, vp, vp, vp, vp, vp]),
+        "mpir_solver_export_factor_leading": (i32, [vp, i64, vp, vp, vp, vp, vp]),
         "mpir_solver_supernodes": (i32, [vp, vp, vp, vp, vp]),
         "mpir_analyze_host": (i32, [i64, vp, vp, vp, i32, vp, vp, vp, vp, vp, vp, vp, vp]),
+        "mpir_server_create": (i32, [vp, vp]),
+        "mpir_server_submit": (i32, [vp, vp, vp]),
+        "mpir_server_wait": (i32, [vp, i64, vp]),
+        "mpir_server_drain": (i32, [vp]),
+        "mpir_server_get_stats": (i32, [vp, vp]),
+        "mpir_server_destroy": (i32, [vp]),
         "mpir_kernel_timer_enable": (i32, [i32]),
         "mpir_launch_count": (i64, []),
         "mpir_kernel_timer_collect": (i32, [vp, vp, i32]),
@@ -446,6 +482,84 @@ class GmresLDLIR:
         Dinv = np.zeros(max(n, 1), np.float32)
         _check(lib().mpir_solver_export_factor(self._h, _p(Lp), _p(Li), _p(Lx), _p(D), _p(Dinv)))
         return Lp, Li[:nl], Lx[:nl], D[:n], Dinv[:n]
+
+
+class Server:
+    """The serving engine (mpir_server_* in include/mpir_b200.h): GMRES-IR
+    requests of mixed sizes and kinds on one GPU, with resident patterns and
+    factors under a device-memory budget, lockstep batches of the queued
+    right-hand sides on one factor, and concurrent work on different factors.
+
+    ``submit`` takes one request (the system in upper CSC, its values, its
+    right-hand side, and the keys naming its pattern and its values) and
+    returns an id at once; ``wait`` returns that request's solution and
+    result.  Arrays are kept referenced until the request is done."""
+
+    def __init__(self, uf="f32", ur="f64", workers=4, max_batch=16, budget_bytes=150 << 30,
+                 ir_iter=10, gmres_iter=10, tol=1e-10, device=0):
+        cfg = ServerConfig(device=device, uf=_PREC[uf], ur=_PREC[ur], workers=workers,
+                           max_batch=max_batch, pad=0, budget_bytes=int(budget_bytes),
+                           max_ir_iterations=ir_iter, max_gmres_iterations=gmres_iter,
+                           tolerance=tol)
+        self._h = C.c_void_p()
+        _check(lib().mpir_server_create(C.byref(self._h), C.byref(cfg)))
+        self._live = {}
+
+    def submit(self, pattern_key, values_key, Ap, Ai, Ax, b):
+        Ap, Ai, Ax, b = _i64(Ap), _i64(Ai), _f64(Ax), _f64(b)
+        n = len(Ap) - 1
+        x = np.zeros(n, np.float64)
+        req = ServerRequest(pattern_key, values_key, n, Ap.ctypes.data, Ai.ctypes.data,
+                            Ax.ctypes.data, b.ctypes.data, x.ctypes.data)
+        rid = C.c_int64(0)
+        _check(lib().mpir_server_submit(self._h, C.byref(req), C.byref(rid)))
+        self._live[rid.value] = (Ap, Ai, Ax, b, x)
+        return rid.value
+
+    def wait(self, rid):
+        """(x, result dict) of request rid; result["status"] < 0 on failure
+        (result["message"] says why)."""
+        res = ServerResult()
+        _check(lib().mpir_server_wait(self._h, int(rid), C.byref(res)))
+        arrays = self._live.pop(rid)
+        out = {k: getattr(res, k) for k, _ in res._fields_ if k not in ("pad", "report")}
+        out["report"] = res.report.as_dict()
+        out["message"] = last_error() if res.status != 0 else ""
+        return arrays[4], out
+
+    def drain(self):
+        _check(lib().mpir_server_drain(self._h))
+
+    def stats(self):
+        st = ServerStats()
+        _check(lib().mpir_server_get_stats(self._h, C.byref(st)))
+        return st.as_dict()
+
+    def close(self):
+        if self._h:
+            lib().mpir_server_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def export_factor_leading(solver, k):
+    """(Lp, Li, Lx, D) of the leading k x k block of a GmresLDLIR's factor
+    (permuted order, QDLDL's CSC form)."""
+    nnz = C.c_int64(0)
+    Lp = np.zeros(k + 1, np.int64)
+    _check(lib().mpir_solver_export_factor_leading(solver._h, k, _p(Lp), None, None, None,
+                                                   C.byref(nnz)))
+    Li = np.zeros(max(nnz.value, 1), np.int64)
+    Lx = np.zeros(max(nnz.value, 1), np.float32)
+    D = np.zeros(max(k, 1), np.float32)
+    _check(lib().mpir_solver_export_factor_leading(solver._h, k, _p(Lp), _p(Li), _p(Lx), _p(D),
+                                                   C.byref(nnz)))
+    return Lp, Li[:nnz.value], Lx[:nnz.value], D[:k]
 
 
 def analyze_host(Ap, Ai, Ax=None, ordering=ORDER_AUTO, pattern=False):

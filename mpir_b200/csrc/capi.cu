@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/mpir_b200.h"
+#include "server.hpp"
 #include "solver.hpp"
 
 namespace mpir {
@@ -106,6 +107,62 @@ static void export_csc(const Plan &P, const Numeric &F, cudaStream_t s,
   Lx.resize(Li.size());
   for (int64_t J = 0; J < S.ns; J++) {
     const int64_t f = S.sfirst[J], l = S.sfirst[J + 1], h = S.h(J);
+    for (int64_t j = f; j < l; j++)
+      for (int64_t p = Lp[j]; p < Lp[j + 1]; p++) {
+        const int64_t lr = local_row(S, J, Li[p]);
+        Lx[p] = lr < 0 ? 0.0f : pan[S.slofs[J] + (j - f) * h + lr];
+      }
+  }
+}
+
+// The leading k x k block of the factor in QDLDL's CSC form (columns < k,
+// rows < k): row k' of L depends only on rows < k', so the pattern is the
+// row-reach walk of rows < k, and only the panels of the supernodes holding
+// columns < k are copied back.
+static void export_csc_leading(const Plan &P, const Numeric &F, cudaStream_t s, int64_t k,
+                               std::vector<int64_t> &Lp, std::vector<int64_t> &Li,
+                               std::vector<float> &Lx, std::vector<float> &D) {
+  const Symbolic &S = P.S;
+  k = std::min<int64_t>(std::max<int64_t>(k, 0), S.n);
+  // supernodes up to the one holding column k - 1
+  int64_t Jend = 0;
+  while (Jend < S.ns && S.sfirst[Jend] < k) Jend++;
+  const int64_t npan = Jend > 0 ? S.slofs[Jend - 1] + S.w(Jend - 1) * S.h(Jend - 1) : 0;
+  std::vector<float> pan(npan);
+  D.resize(k);
+  if (npan)
+    MPIR_CUDA(cudaMemcpyAsync(pan.data(), F.panel.as<void>(), npan * sizeof(float),
+                              cudaMemcpyDeviceToHost, s));
+  if (k)
+    MPIR_CUDA(cudaMemcpyAsync(D.data(), F.D.as<void>(), k * sizeof(float), cudaMemcpyDeviceToHost,
+                              s));
+  MPIR_CUDA(cudaStreamSynchronize(s));
+  // column counts of the leading block: entries of rows < k
+  std::vector<int64_t> cnt(k + 1, 0), mark(k, -1);
+  for (int64_t r = 0; r < k; r++) {
+    mark[r] = r;
+    for (int64_t p = S.Cp[r]; p < S.Cp[r + 1]; p++)
+      for (int64_t i = S.Ci[p]; mark[i] != r; i = S.etree[i]) {
+        cnt[i + 1]++;
+        mark[i] = r;
+      }
+  }
+  Lp.assign(k + 1, 0);
+  for (int64_t j = 0; j < k; j++) Lp[j + 1] = Lp[j] + cnt[j + 1];
+  Li.resize(Lp[k]);
+  std::vector<int64_t> next(Lp.begin(), Lp.end() - 1);
+  std::fill(mark.begin(), mark.end(), -1);
+  for (int64_t r = 0; r < k; r++) {
+    mark[r] = r;
+    for (int64_t p = S.Cp[r]; p < S.Cp[r + 1]; p++)
+      for (int64_t i = S.Ci[p]; mark[i] != r; i = S.etree[i]) {
+        Li[next[i]++] = r;
+        mark[i]       = r;
+      }
+  }
+  Lx.resize(Li.size());
+  for (int64_t J = 0; J < Jend; J++) {
+    const int64_t f = S.sfirst[J], l = std::min<int64_t>(S.sfirst[J + 1], k), h = S.h(J);
     for (int64_t j = f; j < l; j++)
       for (int64_t p = Lp[j]; p < Lp[j + 1]; p++) {
         const int64_t lr = local_row(S, J, Li[p]);
@@ -678,6 +735,25 @@ int mpir_solver_export_factor(mpir_solver s, int64_t *Lp, int64_t *Li, float *Lx
   });
 }
 
+int mpir_solver_export_factor_leading(mpir_solver s, int64_t k, int64_t *Lp, int64_t *Li,
+                                      float *Lx, float *D, int64_t *nnz) {
+  MPIR_NEED(s);
+  return guard([&]() -> int {
+    const Solver &sv = *s->impl;
+    if (!sv.numeric().valid) throw std::logic_error("no valid factor");
+    if (k < 0 || k > sv.plan().S.n) throw StatusError(MPIR_ERR_ARGUMENT, "0 <= k <= n");
+    std::vector<int64_t> lp, li;
+    std::vector<float>   lx, d;
+    export_csc_leading(sv.plan(), sv.numeric(), sv.stream(), k, lp, li, lx, d);
+    if (nnz) *nnz = static_cast<int64_t>(li.size());
+    if (Lp) std::memcpy(Lp, lp.data(), (k + 1) * sizeof(int64_t));
+    if (Li && !li.empty()) std::memcpy(Li, li.data(), li.size() * sizeof(int64_t));
+    if (Lx && !lx.empty()) std::memcpy(Lx, lx.data(), lx.size() * sizeof(float));
+    if (D && k) std::memcpy(D, d.data(), k * sizeof(float));
+    return MPIR_OK;
+  });
+}
+
 int mpir_analyze_host(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *Ax,
                       int ordering, int64_t *perm, int64_t *etree, int64_t *Lnz, int64_t *Cp,
                       int64_t *Ci, int64_t *Lp, int64_t *Li, mpir_info *info) {
@@ -728,7 +804,125 @@ int mpir_analyze_host(int64_t n, const int64_t *Ap, const int64_t *Ai, const dou
   });
 }
 
-int64_t mpir_launch_count(void) { return launch_counter(); }
+struct mpir_server_s {
+  Server *impl;
+};
+
+int mpir_server_create(mpir_server *out, const mpir_server_config *cfg) {
+  return guard([&]() -> int {
+    if (!out || !cfg) throw StatusError(MPIR_ERR_ARGUMENT, "NULL argument");
+    *out = nullptr;
+    if ((cfg->uf != kF32 && cfg->uf != kBF16 && cfg->uf != kF16) ||
+        (cfg->ur != kF64 && cfg->ur != kDD))
+      throw StatusError(MPIR_ERR_UNSUPPORTED, "provided precisions: UF=F32/BF16/F16, UR=F64/DD");
+    if (cfg->workers < 1 || cfg->max_batch < 1 || cfg->budget_bytes <= 0 ||
+        cfg->max_ir_iterations < 0 || cfg->max_gmres_iterations < 0)
+      throw StatusError(MPIR_ERR_ARGUMENT, "invalid server configuration");
+    ServerConfig c;
+    c.device               = cfg->device;
+    c.uf                   = cfg->uf;
+    c.ur                   = cfg->ur;
+    c.workers              = cfg->workers;
+    c.max_batch            = cfg->max_batch;
+    c.budget_bytes         = cfg->budget_bytes;
+    c.max_ir_iterations    = cfg->max_ir_iterations;
+    c.max_gmres_iterations = cfg->max_gmres_iterations;
+    c.tolerance            = cfg->tolerance;
+    MPIR_CUDA(cudaSetDevice(c.device));
+    *out = new mpir_server_s{new Server(c)};
+    return MPIR_OK;
+  });
+}
+
+int mpir_server_submit(mpir_server s, const mpir_server_request *r, int64_t *id) {
+  return guard([&]() -> int {
+    if (!s || !s->impl || !r || !id) throw StatusError(MPIR_ERR_ARGUMENT, "NULL argument");
+    if (r->n < 0 || (r->n > 0 && (!r->Ap || !r->Ai || !r->Ax || !r->b || !r->x)))
+      throw StatusError(MPIR_ERR_ARGUMENT, "request arrays missing");
+    for (int64_t j = 0; j < r->n; j++) {
+      if (r->Ap[j + 1] <= r->Ap[j])
+        throw StatusError(MPIR_ERR_INPUT, "empty column " + std::to_string(j));
+      if (r->Ai[r->Ap[j + 1] - 1] > j)
+        throw StatusError(MPIR_ERR_INPUT, "entry below the diagonal in column " + std::to_string(j));
+    }
+    ServerRequest q;
+    q.pattern_key = r->pattern_key;
+    q.values_key  = r->values_key;
+    q.n           = r->n;
+    q.Ap          = r->Ap;
+    q.Ai          = r->Ai;
+    q.Ax          = r->Ax;
+    q.b           = r->b;
+    q.x           = r->x;
+    *id           = s->impl->submit(q);
+    return MPIR_OK;
+  });
+}
+
+int mpir_server_wait(mpir_server s, int64_t id, mpir_server_result *res) {
+  return guard([&]() -> int {
+    if (!s || !s->impl) throw StatusError(MPIR_ERR_ARGUMENT, "NULL server");
+    ServerResult r;
+    s->impl->wait(id, &r);
+    if (res) {
+      std::memset(res, 0, sizeof *res);
+      res->id         = r.id;
+      res->status     = r.status;
+      res->path       = r.path;
+      res->batch      = r.batch;
+      res->latency_ms = r.latency_ms;
+      res->queue_ms   = r.queue_ms;
+      res->service_ms = r.service_ms;
+      static_assert(sizeof(mpir_report) == sizeof(Report), "report layout");
+      std::memcpy(&res->report, &r.report, sizeof(Report));
+    }
+    if (r.status != 0) g_err = r.message;
+    return MPIR_OK;
+  });
+}
+
+int mpir_server_drain(mpir_server s) {
+  return guard([&]() -> int {
+    if (!s || !s->impl) throw StatusError(MPIR_ERR_ARGUMENT, "NULL server");
+    s->impl->drain();
+    return MPIR_OK;
+  });
+}
+
+int mpir_server_get_stats(mpir_server s, mpir_server_stats *out) {
+  return guard([&]() -> int {
+    if (!s || !s->impl || !out) throw StatusError(MPIR_ERR_ARGUMENT, "NULL argument");
+    const ServerStats st = s->impl->stats();
+    out->submitted         = st.submitted;
+    out->completed         = st.completed;
+    out->failed            = st.failed;
+    out->refused           = st.refused;
+    out->analyses          = st.analyses;
+    out->factorizations    = st.factorizations;
+    out->solves            = st.solves;
+    out->batched_solves    = st.batched_solves;
+    out->batched_rhs       = st.batched_rhs;
+    out->evictions         = st.evictions;
+    out->resident_factors  = st.resident_factors;
+    out->resident_patterns = st.resident_patterns;
+    out->queued            = st.queued;
+    out->bytes_in_use      = st.bytes_in_use;
+    out->peak_bytes        = st.peak_bytes;
+    return MPIR_OK;
+  });
+}
+
+int mpir_server_destroy(mpir_server s) {
+  return guard([&]() -> int {
+    if (s) {
+      delete s->impl;
+      delete s;
+    }
+    return MPIR_OK;
+  });
+}
+
+int64_t mpir_launch_count(void) { return launch_total(); }
 
 int mpir_kernel_timer_enable(int on) {
   KernelTimer &t = kernel_timer();

@@ -24,15 +24,30 @@ struct CudaError : std::runtime_error {
 #define MPIR_CHECK_LAUNCH() MPIR_CUDA(cudaGetLastError())
 
 // Host-side count of kernel launches issued by this library (read by the
-// benchmark for its launch figure).
-int64_t &launch_counter();
-#define MPIR_COUNT(n) (::mpir::launch_counter() += (n))
+// benchmark for its launch figure); safe from several host threads.  While a
+// thread records a CUDA graph (LaunchCapture), its launches are counted for
+// the graph instead, and each replay adds the graph's count.
+int64_t launch_total();
+void    launch_add(int64_t n);
+class LaunchCapture {
+ public:
+  LaunchCapture();
+  ~LaunchCapture();
+  LaunchCapture(const LaunchCapture &)            = delete;
+  LaunchCapture &operator=(const LaunchCapture &) = delete;
+  int64_t count() const { return count_; }
+  void    add(int64_t n) { count_ += n; }
+
+ private:
+  LaunchCapture *outer_;
+  int64_t        count_ = 0;
+};
 
 // Launch helper: counts the launch, then issues it.
 template <class... KArgs, class... Args>
 inline void launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
                    cudaStream_t s, Args &&...args) {
-  ++launch_counter();
+  launch_add(1);
   kernel<<<grid, block, smem, s>>>(static_cast<KArgs>(args)...);
 }
 

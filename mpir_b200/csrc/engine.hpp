@@ -128,6 +128,8 @@ class Plan {
   int64_t              pk_elems = 0, pd_elems = 0;
 
   void build(Symbolic &&sym, cudaStream_t s);
+  // Device memory the plan holds.
+  size_t device_bytes() const;
   bool is_large(int64_t J) const { return S.h(J) > kSmallFront; }
   // Packed-front geometry (PackedFront): first packed row of the
   // off-diagonal rows, K-groups per row tile, row tiles.
@@ -162,6 +164,17 @@ class Numeric {
   int          update_mode = -1;
 
   void allocate(const Plan &P);
+  // The buffers only the factorization uses (update arena, packed fronts,
+  // split partials, converted operands, float32 block inverses, the values):
+  // trim() releases them once a factor is done (a resident factor keeps what
+  // the solves read: L, the float64 block inverses, D, K), ensure_scratch()
+  // brings them back before the next factorization.
+  void ensure_scratch(const Plan &P);
+  void trim();
+  bool has_scratch = false;
+  // Device memory allocate() takes for P, and what this factor holds.
+  static size_t bytes_for(const Plan &P);
+  size_t        device_bytes() const;
   // Scale the caller's values (device, caller order), assemble and factor.
   void run(const Plan &P, const double *d_Ax, double eps_uf, cudaStream_t s);
   // The same, replayed from a CUDA graph captured on capture_stream at the

@@ -15,6 +15,7 @@
 //     (W = F L^{-T}, L = W D^{-1}) and a GEMM-shaped trailing update
 //     C -= (L D) L^T.
 // D is left on each panel's diagonal and copied to D / Dinv (permuted order).
+#include <atomic>
 #include <algorithm>
 #include <climits>
 #include <cmath>
@@ -1289,10 +1290,25 @@ void Numeric::allocate(const Plan &P) {
   release_graph();
   const Symbolic &S = P.S;
   panel.resize(std::max<int64_t>(S.panel_elems, 1) * sizeof(float));
-  uarena.resize(std::max<int64_t>(S.uarena_elems, 1) * sizeof(float));
-  linv.resize(std::max<int64_t>(P.linv_elems, 1) * sizeof(float));
   linv64.resize(std::max<int64_t>(P.linv_elems, 1) * sizeof(double));
   linv64t.resize(std::max<int64_t>(P.linv_elems, 1) * sizeof(double));
+  D.resize(std::max<int64_t>(S.n, 1) * sizeof(float));
+  Dinv.resize(std::max<int64_t>(S.n, 1) * sizeof(float));
+  status.resize(sizeof(FactorStatus));
+  AD.resize(std::max<int64_t>(S.n, 1) * sizeof(double));
+  Kval.resize(std::max<int64_t>(P.nnz_full, 1) * sizeof(double));
+  Korig.resize(std::max<int64_t>(P.nnz_full, 1) * sizeof(double));
+  has_scratch = false;
+  ensure_scratch(P);
+  valid = false;
+}
+
+void Numeric::ensure_scratch(const Plan &P) {
+  if (has_scratch) return;
+  release_graph();  // a recorded factorization points at the old buffers
+  const Symbolic &S = P.S;
+  uarena.resize(std::max<int64_t>(S.uarena_elems, 1) * sizeof(float));
+  linv.resize(std::max<int64_t>(P.linv_elems, 1) * sizeof(float));
   ws.resize(std::max<int64_t>(P.ws_elems, 1) * sizeof(float));
   // Packed fronts: positions that hold no value of L are never written and
   // stay zero from here on.
@@ -1301,15 +1317,43 @@ void Numeric::allocate(const Plan &P) {
   packd.resize(std::max<int64_t>(2 * P.pd_elems, 1) * sizeof(float));
   MPIR_CUDA(cudaMemset(pack.as<void>(), 0, pack.bytes()));
   MPIR_CUDA(cudaMemset(packd.as<void>(), 0, packd.bytes()));
-  D.resize(std::max<int64_t>(S.n, 1) * sizeof(float));
-  Dinv.resize(std::max<int64_t>(S.n, 1) * sizeof(float));
-  status.resize(sizeof(FactorStatus));
-  AD.resize(std::max<int64_t>(S.n, 1) * sizeof(double));
   Axs.resize(std::max<int64_t>(S.nnz, 1) * sizeof(double));
-  Kval.resize(std::max<int64_t>(P.nnz_full, 1) * sizeof(double));
-  Korig.resize(std::max<int64_t>(P.nnz_full, 1) * sizeof(double));
   Ax.resize(std::max<int64_t>(S.nnz, 1) * sizeof(double));
-  valid = false;
+  has_scratch = true;
+}
+
+void Numeric::trim() {
+  release_graph();
+  for (DeviceBuffer *b : {&uarena, &linv, &ws, &bconv, &pack, &packd, &Axs, &Ax}) b->release();
+  has_scratch = false;
+}
+
+size_t Numeric::bytes_for(const Plan &P) {
+  const Symbolic &S  = P.S;
+  auto            at = [](int64_t e, size_t b) { return std::max<int64_t>(e, 1) * b; };
+  return at(S.panel_elems, 4) + at(S.uarena_elems, 4) + at(P.linv_elems, 4) +
+         2 * at(P.linv_elems, 8) + at(P.ws_elems, 4) + at(P.bconv_elems, 4) +
+         at(P.pk_elems, 4) + at(2 * P.pd_elems, 4) + 2 * at(S.n, 4) + sizeof(FactorStatus) +
+         at(S.n, 8) + 2 * at(S.nnz, 8) + 2 * at(P.nnz_full, 8);
+}
+
+size_t Numeric::device_bytes() const {
+  size_t b = 0;
+  for (const DeviceBuffer *d : {&panel, &uarena, &linv, &linv64, &linv64t, &D, &Dinv, &status,
+                                &ws, &pack, &packd, &bconv, &AD, &Axs, &Kval, &Korig, &Ax})
+    b += d->bytes();
+  return b;
+}
+
+size_t Plan::device_bytes() const {
+  size_t b = 0;
+  for (const DeviceBuffer *d :
+       {&amap, &arow, &acol, &diag_pos, &Kp, &Kj, &Ksrc, &sfirst, &srowptr, &srows, &srel,
+        &slofs, &uofs, &zofs, &child_ptr, &child_list, &perm, &ea_seq, &small_list,
+        &large_list, &steps, &ea_tasks, &linv_ofs_d, &gemm_probs, &solve_fronts, &swarp_list,
+        &sblock_list, &gp, &gsrc, &fwd_item, &chunk_map, &own_item})
+    b += d->bytes();
+  return b;
 }
 
 static unsigned grid_for(int64_t n, int threads) {
@@ -1336,18 +1380,16 @@ void Numeric::run_graph(const Plan &P, const double *d_Ax, double eps, cudaStrea
     cudaGraph_t g = nullptr;
     MPIR_CUDA(cudaStreamSynchronize(capture_stream));
     MPIR_CUDA(cudaStreamBeginCapture(capture_stream, cudaStreamCaptureModeThreadLocal));
-    const int64_t before = launch_counter();
+    LaunchCapture cap;
     try {
       run(P, d_Ax, eps, capture_stream);
     } catch (...) {
       cudaStreamEndCapture(capture_stream, &g);
       if (g) cudaGraphDestroy(g);
-      launch_counter() = before;
       throw;
     }
     MPIR_CUDA(cudaStreamEndCapture(capture_stream, &g));
-    graph_launches   = launch_counter() - before;
-    launch_counter() = before;
+    graph_launches = cap.count();
     const cudaError_t e = cudaGraphInstantiate(&graph, g, 0);
     cudaGraphDestroy(g);
     MPIR_CUDA(e);
@@ -1357,11 +1399,12 @@ void Numeric::run_graph(const Plan &P, const double *d_Ax, double eps, cudaStrea
   }
   eps_uf = eps;
   MPIR_CUDA(cudaGraphLaunch(graph, s));
-  launch_counter() += graph_launches;
+  launch_add(graph_launches);
   valid = true;
 }
 
 void Numeric::run(const Plan &P, const double *d_Ax, double eps, cudaStream_t s) {
+  if (!has_scratch) throw std::logic_error("factorization scratch released (ensure_scratch)");
   const Symbolic &S  = P.S;
   KernelTimer    &kt = kernel_timer();
   eps_uf             = eps;
@@ -1382,14 +1425,14 @@ void Numeric::run(const Plan &P, const double *d_Ax, double eps, cudaStream_t s)
   MPIR_CHECK_LAUNCH();
   float        *pan = panel.as<float>(), *ua = uarena.as<float>();
   FactorStatus *st  = status.as<FactorStatus>();
-  static bool   trsm_attr = false;
+  static std::atomic<bool> trsm_attr{false};
   const int     trsm_smem = kBM * (kBN + 1) * sizeof(float);
   if (!trsm_attr) {
     MPIR_CUDA(cudaFuncSetAttribute(k_step_gemm<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    trsm_smem));
     trsm_attr = true;
   }
-  static bool   diag_attr = false;
+  static std::atomic<bool> diag_attr{false};
   const int     diag_smem = kDiagSmemFloats * sizeof(float);
   if (!diag_attr) {
     MPIR_CUDA(cudaFuncSetAttribute(k_diag_block, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1486,10 +1529,22 @@ int64_t Numeric::result(cudaStream_t s, int32_t *zero_col, bool *nonfinite) cons
 }
 
 // ---------------------------------------------------------------------------
-int64_t &launch_counter() {
-  static int64_t c = 0;
-  return c;
+namespace {
+std::atomic<int64_t>        g_launches{0};
+thread_local LaunchCapture *t_capture = nullptr;
+}  // namespace
+
+int64_t launch_total() { return g_launches.load(std::memory_order_relaxed); }
+
+void launch_add(int64_t n) {
+  if (t_capture)
+    t_capture->add(n);
+  else
+    g_launches.fetch_add(n, std::memory_order_relaxed);
 }
+
+LaunchCapture::LaunchCapture() : outer_(t_capture) { t_capture = this; }
+LaunchCapture::~LaunchCapture() { t_capture = outer_; }
 
 KernelTimer &kernel_timer() {
   static KernelTimer t;

@@ -12,6 +12,7 @@
 #include <string>
 #include <vector>
 
+#include "solve_dev.cuh"
 #include "solver.hpp"
 
 namespace mpir {
@@ -78,8 +79,15 @@ int Solver::analyze(int64_t n, const int64_t *Ap, const int64_t *Ai,
   const int   rc = mpir::analyze(n, Ap, Ai, Ax ? sign.data() : nullptr,
                                  static_cast<Ordering>(ordering), S, err);
   if (rc != kOk) throw std::invalid_argument(err.empty() ? "analysis failed" : err);
-  auto P = std::make_unique<Plan>();
+  auto P = std::make_shared<Plan>();
   P->build(std::move(S), stream_);
+  adopt(std::move(P));
+  return kOk;
+}
+
+void Solver::adopt(std::shared_ptr<Plan> P) {
+  MPIR_CUDA(cudaSetDevice(device));
+  const int64_t n = P->S.n;
   plan_ = std::move(P);
   num_.allocate(*plan_);
   num_.update_mode = update_mode_for(uf);
@@ -95,7 +103,33 @@ int Solver::analyze(int64_t n, const int64_t *Ap, const int64_t *Ai,
   if (wait_ctl_[0] || wait_ctl_[1])
     MPIR_CUDA(cudaMemcpy(ws_.err.as<int32_t>() + 1, wait_ctl_, sizeof wait_ctl_,
                          cudaMemcpyHostToDevice));
-  return kOk;
+}
+
+size_t Solver::device_bytes() const {
+  size_t b = num_.device_bytes();
+  for (const DeviceBuffer *d : {&ws_.zbuf, &ws_.part, &ws_.sync, &ws_.ready, &ws_.err, &ws_.xbuf,
+                                &mws_.zbuf, &mws_.part, &mws_.sync, &mws_.ready, &mws_.err,
+                                &vec_.part, &vec_.count, &vec_.infbits, &vecb_.part, &vecb_.count,
+                                &vecb_.infbits, &V_, &bs_, &bp_, &ADp_, &x_, &r_, &t_, &d_, &hd_,
+                                &y_, &hb_, &hx_, &bV_, &bbs_, &bbp_, &bx_, &br_, &bt_, &bd_, &bhd_,
+                                &by_, &bfac_, &bact_, &bkq_, &bin_, &bout_})
+    b += d->bytes();
+  return b;
+}
+
+size_t Solver::bytes_for(const Plan &P, int64_t gmres_iter, int width) {
+  const int64_t n  = std::max<int64_t>(P.S.n, 1);
+  const int64_t m  = std::max<int64_t>(std::min(gmres_iter, n), 1);
+  size_t        b  = Numeric::bytes_for(P);
+  // single-vector workspace and vectors
+  b += (std::max<int64_t>(P.S.z_elems, 1) + std::max<int64_t>(P.spart_elems, 1) +
+        static_cast<int64_t>(kReadyCopies) * n + n) * sizeof(double);
+  b += (m + 1 + 10) * n * sizeof(double) + 2048 * sizeof(double);
+  if (width > 1) {
+    b += MultiSolveWorkspace::bytes_for(P, width);
+    b += (m + 1 + 8) * n * width * sizeof(double) + 2048 * width * sizeof(double);
+  }
+  return b;
 }
 
 void Solver::ensure_vectors() {
@@ -120,6 +154,7 @@ void Solver::ensure_vectors() {
 int Solver::factor_device(const double *d_Ax) {
   if (!plan_) throw std::logic_error("factor before analyze");
   MPIR_CUDA(cudaSetDevice(device));
+  num_.ensure_scratch(*plan_);
   MPIR_CUDA(cudaEventRecord(ev0_, stream_));
   num_.run_graph(*plan_, d_Ax, eps_of(uf), stream_, own_stream_);
   MPIR_CUDA(cudaEventRecord(ev1_, stream_));
@@ -139,6 +174,7 @@ int Solver::factor_device(const double *d_Ax) {
 int Solver::factor(const double *Ax) {
   if (!plan_) throw std::logic_error("factor before analyze");
   MPIR_CUDA(cudaSetDevice(device));
+  num_.ensure_scratch(*plan_);
   MPIR_CUDA(cudaMemcpyAsync(num_.Ax.as<void>(), Ax, plan_->S.nnz * sizeof(double),
                             cudaMemcpyHostToDevice, stream_));
   return factor_device(num_.Ax.as<double>());

@@ -1,0 +1,446 @@
+// Serving engine: GMRES-IR requests of mixed sizes and kinds on one GPU.
+//
+// The reference solves one system per GmresLDLIR object, one call at a time:
+// Compute (gmres_ir.hpp:323) then Solve (gmres_ir.hpp:534-634), with
+// QDLDL_etree / QDLDL_factor / QDLDL_solve (qdldl.hpp:48-432) underneath.
+// This engine takes a stream of such requests and keeps what one request
+// leaves behind for the next:
+//
+//   patterns  a request names its pattern (pattern_key) and its values
+//             (values_key).  An unknown pattern is analysed on the host (the
+//             ordering and symbolic analysis) and its plan uploaded once;
+//   factors   a factor is kept per (pattern, values) while memory allows:
+//             a request on a resident factor is only a solve, one with new
+//             values on a known pattern a refactorization (replayed from the
+//             pattern's captured graph) and a solve;
+//   admission every plan and factor is charged its device bytes against the
+//             budget; a factor that does not fit evicts the least recently
+//             used idle factors (then idle plans) first, and a request whose
+//             footprint exceeds the whole budget is refused with
+//             MPIR_ERR_NOMEM;
+//   batching  worker threads, each driving its own CUDA stream, take the
+//             oldest request whose pattern and factor are idle, together with
+//             every queued request on the same factor (up to max_batch): those
+//             are solved in lockstep by one batched GMRES-IR whose
+//             preconditioner applications are several-vector triangular
+//             solves (gmres_batch.cu, solve_multi.cu);
+//   overlap   requests on different factors run on different streams at the
+//             same time, and the host analysis of a new pattern runs on its
+//             worker's thread while the GPU serves the others.
+// Each result is the solve the request would get alone: the same analysis,
+// factor and GMRES-IR control flow; a batched solve differs from a lone one
+// only by the rounding of the several-vector triangular solves.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "server.hpp"
+#include "symbolic.hpp"
+
+namespace mpir {
+
+static double now_s() {
+  using C = std::chrono::steady_clock;
+  return std::chrono::duration<double>(C::now().time_since_epoch()).count();
+}
+
+struct Server::Impl {
+  ServerConfig cfg;
+
+  struct Pattern {
+    std::shared_ptr<Plan> plan;
+    bool                  busy    = true;  // being analysed
+    size_t                bytes   = 0;
+    double                last    = 0;
+    int                   factors = 0;  // resident factors on this plan
+  };
+  struct Factor {
+    std::unique_ptr<Solver> solver;
+    bool                    busy  = false;
+    bool                    valid = false;
+    size_t                  bytes = 0;
+    double                  last  = 0;
+  };
+  using FKey = std::pair<uint64_t, uint64_t>;
+
+  struct Job {
+    enum Kind { kNone, kAnalyse, kFactor, kSolve } kind = kNone;
+    std::vector<ServerRequest> reqs;
+  };
+
+  std::mutex                           mu;
+  std::condition_variable              cv_work, cv_done;
+  std::deque<ServerRequest>            queue;
+  std::map<uint64_t, Pattern>          patterns;
+  std::map<FKey, Factor>               factors;
+  std::unordered_map<int64_t, ServerResult> done;
+  std::vector<std::thread>             workers;
+  ServerStats                          st{};
+  size_t                               used    = 0;
+  int                                  running = 0;
+  int64_t                              next_id = 1;
+  bool                                 stop    = false;
+
+  // ---- scheduling (under mu) -------------------------------------------------
+  // Moves the queued requests on factor key k (at most `room`) into out.
+  void take_same(const FKey &k, size_t room, std::vector<ServerRequest> &out) {
+    for (auto it = queue.begin(); it != queue.end() && out.size() < room;) {
+      if (it->pattern_key == k.first && it->values_key == k.second) {
+        out.push_back(*it);
+        it = queue.erase(it);
+      } else {
+        ++it;
+      }
+    }
+  }
+
+  bool pick(Job &job) {
+    for (auto it = queue.begin(); it != queue.end(); ++it) {
+      const ServerRequest r = *it;
+      const FKey          k{r.pattern_key, r.values_key};
+      auto                p = patterns.find(r.pattern_key);
+      if (p != patterns.end() && p->second.busy) continue;  // being analysed
+      auto f = factors.find(k);
+      if (f != factors.end() && f->second.busy) continue;   // in use
+      queue.erase(it);
+      job.reqs.clear();
+      job.reqs.push_back(r);
+      take_same(k, static_cast<size_t>(cfg.max_batch), job.reqs);
+      if (p == patterns.end()) {
+        Pattern np;
+        np.busy = true;
+        np.last = now_s();
+        patterns.emplace(r.pattern_key, std::move(np));
+        job.kind = Job::kAnalyse;
+      } else if (f != factors.end() && f->second.valid) {
+        job.kind = Job::kSolve;
+      } else {
+        job.kind = Job::kFactor;
+      }
+      Factor &fe = factors[k];  // placeholder while it is built
+      fe.busy    = true;
+      running++;
+      return true;
+    }
+    return false;
+  }
+
+  // Frees room for `need` bytes by evicting idle factors, then idle plans
+  // without factors, least recently used first.  Returns false when it cannot
+  // (the evicted solvers are handed back to be destroyed outside the lock).
+  bool make_room(size_t need, std::vector<std::unique_ptr<Solver>> &graveyard,
+                 std::vector<std::shared_ptr<Plan>> &plan_graveyard) {
+    while (used + need > static_cast<size_t>(cfg.budget_bytes)) {
+      auto victim = factors.end();
+      for (auto it = factors.begin(); it != factors.end(); ++it)
+        if (!it->second.busy && it->second.solver &&
+            (victim == factors.end() || it->second.last < victim->second.last))
+          victim = it;
+      if (victim != factors.end()) {
+        used -= victim->second.bytes;
+        auto p = patterns.find(victim->first.first);
+        if (p != patterns.end()) p->second.factors--;
+        graveyard.push_back(std::move(victim->second.solver));
+        factors.erase(victim);
+        st.evictions++;
+        continue;
+      }
+      auto pv = patterns.end();
+      for (auto it = patterns.begin(); it != patterns.end(); ++it) {
+        if (it->second.busy || it->second.factors != 0 || !it->second.plan) continue;
+        bool referenced = false;  // by the placeholder factor of a running job
+        for (auto &f : factors)
+          if (f.first.first == it->first) referenced = true;
+        if (!referenced && (pv == patterns.end() || it->second.last < pv->second.last)) pv = it;
+      }
+      if (pv == patterns.end()) return false;
+      used -= pv->second.bytes;
+      plan_graveyard.push_back(std::move(pv->second.plan));
+      patterns.erase(pv);
+      st.evictions++;
+    }
+    return true;
+  }
+
+  // ---- work (outside mu) ------------------------------------------------------
+  void finish(const ServerRequest &r, int status, int path, int batch, double t0,
+              const Report &rep, const std::string &msg) {
+    ServerResult res{};
+    res.id         = r.id;
+    res.status     = status;
+    res.path       = path;
+    res.batch      = batch;
+    const double t = now_s();
+    res.latency_ms = 1e3 * (t - r.t_submit);
+    res.queue_ms   = 1e3 * (t0 - r.t_submit);
+    res.service_ms = 1e3 * (t - t0);
+    res.report     = rep;
+    res.message    = msg;
+    std::lock_guard<std::mutex> lk(mu);
+    done[r.id] = res;
+    st.completed++;
+    if (status != 0) st.failed++;
+  }
+
+  void run(Job &job) {
+    const double               t0 = now_s();
+    const ServerRequest       &r  = job.reqs.front();
+    const FKey                 k{r.pattern_key, r.values_key};
+    int                        path = job.kind == Job::kAnalyse ? 2 : job.kind == Job::kFactor ? 1 : 0;
+    std::shared_ptr<Plan>      plan;
+    Solver                    *sv = nullptr;
+    std::vector<std::unique_ptr<Solver>> graveyard;
+    std::vector<std::shared_ptr<Plan>>   plan_graveyard;
+    auto fail_all = [&](int code, const std::string &msg) {
+      for (const ServerRequest &q : job.reqs) finish(q, code, path, 1, t0, Report{}, msg);
+    };
+    try {
+      MPIR_CUDA(cudaSetDevice(cfg.device));
+      if (job.kind == Job::kAnalyse) {
+        std::vector<int8_t> sign(r.n, 0);
+        for (int64_t j = 0; j < r.n; j++)
+          for (int64_t p = r.Ap[j]; p < r.Ap[j + 1]; p++)
+            if (r.Ai[p] == j && r.Ax[p] > 0) sign[j] = 1;
+        Symbolic    S;
+        std::string err;
+        const int   rc = analyze(r.n, r.Ap, r.Ai, sign.data(), Ordering::Auto, S, err);
+        if (rc != kOk) {
+          {
+            std::lock_guard<std::mutex> lk(mu);
+            patterns.erase(r.pattern_key);
+            factors.erase(k);
+            st.analyses++;
+          }
+          fail_all(rc, err.empty() ? "analysis failed" : err);
+          return;
+        }
+        plan = std::make_shared<Plan>();
+        {
+          cudaStream_t s = nullptr;
+          MPIR_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+          try {
+            plan->build(std::move(S), s);
+          } catch (...) {
+            cudaStreamDestroy(s);
+            throw;
+          }
+          cudaStreamDestroy(s);
+        }
+        std::lock_guard<std::mutex> lk(mu);
+        const size_t pb = plan->device_bytes();
+        make_room(pb, graveyard, plan_graveyard);  // best effort: plans are small
+        Pattern &p = patterns[r.pattern_key];
+        p.plan     = plan;
+        p.busy     = false;
+        p.bytes    = pb;
+        p.last     = now_s();
+        used += p.bytes;
+        st.analyses++;
+        st.peak_bytes = std::max<int64_t>(st.peak_bytes, used);
+      } else {
+        std::lock_guard<std::mutex> lk(mu);
+        plan = patterns.at(r.pattern_key).plan;
+      }
+      if (job.kind != Job::kSolve) {
+        const int    width = job.reqs.size() > 1 ? multi_width(static_cast<int>(job.reqs.size())) : 1;
+        const size_t need  = Solver::bytes_for(*plan, cfg.max_gmres_iterations, width);
+        {
+          std::unique_lock<std::mutex> lk(mu);
+          if (need > static_cast<size_t>(cfg.budget_bytes)) {
+            factors.erase(k);
+            lk.unlock();
+            fail_all(-4, "factor footprint " + std::to_string(need) +
+                             " bytes exceeds the admission budget");
+            std::lock_guard<std::mutex> lk2(mu);
+            st.refused += static_cast<int64_t>(job.reqs.size());
+            return;
+          }
+          while (!make_room(need, graveyard, plan_graveyard)) {
+            if (running <= 1) {  // nothing else will free memory
+              factors.erase(k);
+              lk.unlock();
+              fail_all(-4, "admission budget held by resident plans");
+              std::lock_guard<std::mutex> lk2(mu);
+              st.refused += static_cast<int64_t>(job.reqs.size());
+              return;
+            }
+            cv_done.wait_for(lk, std::chrono::milliseconds(20));
+          }
+          used += need;  // reserved; corrected to the measured bytes below
+          st.peak_bytes = std::max<int64_t>(st.peak_bytes, used);
+        }
+        graveyard.clear();
+        plan_graveyard.clear();
+        auto solver = std::make_unique<Solver>(cfg.uf, kF64, cfg.ur, cfg.device);
+        solver->ir_iter    = cfg.max_ir_iterations;
+        solver->gmres_iter = cfg.max_gmres_iterations;
+        solver->tol        = cfg.tolerance;
+        solver->adopt(plan);
+        const int fr = solver->factor(r.Ax);
+        // A resident factor keeps only what the solves read.
+        MPIR_CUDA(cudaStreamSynchronize(solver->stream()));
+        solver->trim();
+        {
+          std::lock_guard<std::mutex> lk(mu);
+          Factor &f = factors[k];
+          f.bytes   = solver->device_bytes();
+          used      = used - need + f.bytes;
+          f.solver  = std::move(solver);
+          f.valid   = fr == kOk;
+          f.last    = now_s();
+          patterns[r.pattern_key].factors++;
+          st.factorizations++;
+          st.peak_bytes = std::max<int64_t>(st.peak_bytes, used);
+          sv = f.solver.get();
+        }
+        if (fr != kOk) {
+          fail_all(fr, fr == -5 ? "a bounded device wait ran out" : "zero pivot");
+          std::lock_guard<std::mutex> lk(mu);
+          factors[k].busy = false;
+          return;
+        }
+      } else {
+        std::lock_guard<std::mutex> lk(mu);
+        sv = factors.at(k).solver.get();
+      }
+      // Solve the batch: one request alone, several in lockstep.
+      const int64_t n  = plan->S.n;
+      const int     nb = static_cast<int>(job.reqs.size());
+      std::vector<Report> reps(nb);
+      int                 rc = kOk;
+      if (nb == 1) {
+        rc = sv->solve(r.b, r.x, &reps[0]);
+      } else {
+        std::vector<double> B(static_cast<size_t>(n) * nb), X(static_cast<size_t>(n) * nb);
+        for (int q = 0; q < nb; q++)
+          std::copy(job.reqs[q].b, job.reqs[q].b + n, B.begin() + static_cast<size_t>(q) * n);
+        rc = sv->solve_batch(nb, B.data(), X.data(), reps.data());
+        for (int q = 0; q < nb; q++)
+          std::copy(X.begin() + static_cast<size_t>(q) * n, X.begin() + static_cast<size_t>(q + 1) * n,
+                    job.reqs[q].x);
+      }
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        Factor &f = factors[k];
+        // the batch buffers may have grown
+        const size_t b = f.solver->device_bytes();
+        used           = used - f.bytes + b;
+        f.bytes        = b;
+        f.last         = now_s();
+        patterns[r.pattern_key].last = f.last;
+        st.solves++;
+        if (nb > 1) {
+          st.batched_solves++;
+          st.batched_rhs += nb;
+        }
+        st.peak_bytes = std::max<int64_t>(st.peak_bytes, used);
+      }
+      for (int q = 0; q < nb; q++)
+        finish(job.reqs[q], rc, path, nb, t0, reps[q], rc == kOk ? "" : "solve failed");
+      std::lock_guard<std::mutex> lk(mu);
+      factors[k].busy = false;
+    } catch (const std::exception &e) {
+      const bool oom = dynamic_cast<const CudaError *>(&e) &&
+                       static_cast<const CudaError &>(e).code == cudaErrorMemoryAllocation;
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        auto f = factors.find(k);
+        if (f != factors.end()) {
+          if (f->second.solver) {
+            used -= f->second.bytes;
+            patterns[k.first].factors--;
+            graveyard.push_back(std::move(f->second.solver));
+          }
+          factors.erase(f);
+        }
+        auto p = patterns.find(k.first);
+        if (p != patterns.end() && p->second.busy) patterns.erase(p);
+      }
+      fail_all(oom ? -4 : -3, e.what());
+    }
+  }
+
+  void worker_main() {
+    cudaSetDevice(cfg.device);
+    for (;;) {
+      Job job;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv_work.wait(lk, [&] { return stop || pick(job); });
+        if (job.kind == Job::kNone) return;  // stopping, nothing left to pick
+      }
+      run(job);
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        running--;
+      }
+      cv_work.notify_all();
+      cv_done.notify_all();
+    }
+  }
+};
+
+Server::Server(const ServerConfig &cfg) : impl_(new Impl) {
+  impl_->cfg = cfg;
+  if (impl_->cfg.workers < 1) impl_->cfg.workers = 1;
+  impl_->cfg.max_batch = std::max(1, std::min(impl_->cfg.max_batch, Solver::kMaxBatch));
+  for (int w = 0; w < impl_->cfg.workers; w++)
+    impl_->workers.emplace_back([this] { impl_->worker_main(); });
+}
+
+Server::~Server() {
+  drain();
+  {
+    std::lock_guard<std::mutex> lk(impl_->mu);
+    impl_->stop = true;
+  }
+  impl_->cv_work.notify_all();
+  for (auto &t : impl_->workers) t.join();
+  cudaSetDevice(impl_->cfg.device);
+  impl_->factors.clear();
+  impl_->patterns.clear();
+}
+
+int64_t Server::submit(ServerRequest r) {
+  std::lock_guard<std::mutex> lk(impl_->mu);
+  r.id       = impl_->next_id++;
+  r.t_submit = now_s();
+  impl_->queue.push_back(r);
+  impl_->st.submitted++;
+  impl_->cv_work.notify_one();
+  return r.id;
+}
+
+bool Server::wait(int64_t id, ServerResult *out) {
+  std::unique_lock<std::mutex> lk(impl_->mu);
+  impl_->cv_done.wait(lk, [&] { return impl_->done.count(id) != 0; });
+  if (out) *out = impl_->done[id];
+  impl_->done.erase(id);
+  return true;
+}
+
+void Server::drain() {
+  std::unique_lock<std::mutex> lk(impl_->mu);
+  impl_->cv_done.wait(lk, [&] { return impl_->queue.empty() && impl_->running == 0; });
+}
+
+ServerStats Server::stats() {
+  std::lock_guard<std::mutex> lk(impl_->mu);
+  ServerStats s       = impl_->st;
+  s.bytes_in_use      = static_cast<int64_t>(impl_->used);
+  s.resident_factors  = 0;
+  for (auto &f : impl_->factors) s.resident_factors += f.second.solver ? 1 : 0;
+  s.resident_patterns = static_cast<int64_t>(impl_->patterns.size());
+  s.queued            = static_cast<int64_t>(impl_->queue.size());
+  return s;
+}
+
+}  // namespace mpir

@@ -16,6 +16,7 @@
 // are float64, the factor float32 (widened on load), as QDLDL_solve with
 // FACTPREC = float and XPREC = double.  Reductions have a fixed order, so
 // results do not depend on scheduling.
+#include <atomic>
 #include <string>
 #include <vector>
 
@@ -676,17 +677,18 @@ void ldlt_solve_graph(const Plan &P, const Numeric &F, double *x, SolveWorkspace
     cudaGraph_t g = nullptr;
     MPIR_CUDA(cudaStreamSynchronize(capture_stream));
     MPIR_CUDA(cudaStreamBeginCapture(capture_stream, cudaStreamCaptureModeThreadLocal));
-    const int64_t before = launch_counter();
-    ldlt_solve(P, F, ws.xbuf.as<double>(), ws, capture_stream);
+    {
+      LaunchCapture cap;
+      ldlt_solve(P, F, ws.xbuf.as<double>(), ws, capture_stream);
+      ws.graph_launches = cap.count();
+    }
     MPIR_CUDA(cudaStreamEndCapture(capture_stream, &g));
-    ws.graph_launches = launch_counter() - before;
-    launch_counter() = before;
     MPIR_CUDA(cudaGraphInstantiate(&ws.graph, g, 0));
     cudaGraphDestroy(g);
   }
   MPIR_CUDA(cudaMemcpyAsync(ws.xbuf.as<void>(), x, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
   MPIR_CUDA(cudaGraphLaunch(ws.graph, s));
-  launch_counter() += ws.graph_launches;
+  launch_add(ws.graph_launches);
   MPIR_CUDA(cudaMemcpyAsync(x, ws.xbuf.as<void>(), n * sizeof(double), cudaMemcpyDeviceToDevice, s));
 }
 
@@ -710,7 +712,7 @@ void ldlt_solve(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
   const unsigned    nmark  = static_cast<unsigned>((nready + 255) / 256);
   if (block) MPIR_CUDA(cudaMemsetAsync(sync, 0, P.sync_elems * sizeof(int32_t), s));
   if (block && (phases & kForward)) launch(k_mark_pending, nmark, 256, 0, s, nready, ready);
-  static bool attr = false;
+  static std::atomic<bool> attr{false};
   if (!attr) {
     MPIR_CUDA(cudaFuncSetAttribute(k_fwd_fronts, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(kFwdTri * sizeof(double))));

@@ -25,6 +25,7 @@
 // a packed lower triangle).  Sums inside the large-front kernels run in
 // another order than in the single-vector kernels, so their results agree
 // with NR single solves to rounding.
+#include <atomic>
 #include <algorithm>
 
 #include "common.cuh"
@@ -545,7 +546,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
 
 template <int NR>
 void set_smem_attrs() {
-  static bool done = false;  // per process; one device per library instance
+  static std::atomic<bool> done{false};  // idempotent; set once per process
   if (done) return;
   MPIR_CUDA(cudaFuncSetAttribute(k_fwd_fronts_m<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(fwd_m_smem_doubles<NR>() * sizeof(double))));

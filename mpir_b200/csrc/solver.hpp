@@ -63,6 +63,14 @@ class Solver {
   // Host entry points (caller arrays on the host, caller order).
   int analyze(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *Ax,
               int ordering);
+  // Take an analysed pattern built elsewhere (shared with other solvers of
+  // the same pattern) and allocate this solver's factor and workspaces.
+  void adopt(std::shared_ptr<Plan> P);
+  std::shared_ptr<Plan> shared_plan() const { return plan_; }
+  // Device memory this solver holds beyond its plan, and what adopt() plus
+  // one batch of `width` right-hand sides would take for plan P.
+  size_t device_bytes() const;
+  static size_t bytes_for(const Plan &P, int64_t gmres_iter, int width);
   int factor(const double *Ax);
   int solve(const double *b, double *x, Report *rep);
   // Device entry points (caller arrays already on this device).
@@ -99,6 +107,9 @@ class Solver {
     return *plan_;
   }
   const Numeric &numeric() const { return num_; }
+  // Release the factorization-only buffers of the current factor (see
+  // Numeric::trim); the next factor() allocates them again.
+  void trim() { num_.trim(); }
   double last_factor_ms = 0;
   int64_t last_npos     = 0;
 
@@ -113,7 +124,7 @@ class Solver {
   void multi_apply(double *block);
 
   cudaStream_t          own_stream_ = nullptr, stream_ = nullptr;
-  std::unique_ptr<Plan> plan_;
+  std::shared_ptr<Plan> plan_;
   Numeric               num_;
   SolveWorkspace        ws_;
   VecOps                vec_;

@@ -31,6 +31,7 @@
 // Every mbarrier wait is bounded; on expiry the kernel records a timeout in
 // the factor status, stops issuing work, waits (bounded) for its own copies
 // and MMAs, frees its tensor memory and returns.
+#include <atomic>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
@@ -618,7 +619,7 @@ static void launch_mode(const GemmProb *probs, int nprob, int units, const float
                         const float *packd, const float *packs, const float *bconv,
                         float *panel, float *uarena, float *ws, FactorStatus *st,
                         cudaStream_t s) {
-  static bool attr = false;
+  static std::atomic<bool> attr{false};
   const int   smem = tc_gemm_smem_bytes(MODE);
   if (!attr) {
     MPIR_CUDA(cudaFuncSetAttribute(k_gemm_tc<MODE>,
