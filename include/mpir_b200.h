@@ -60,7 +60,9 @@ typedef struct mpir_report {
   int32_t reorth_count;     /* Brown/Hindmarsh re-orthogonalisations */
   int32_t stop_reason;      /* 0 iteration cap, 1 small update, 2 stagnation,
                                3 zero residual, 4 non-finite residual */
-  int32_t pad;
+  int32_t factor_prec;      /* MPIR_F32 / MPIR_BF16 / MPIR_F16: the type the
+                               factor was computed and applied in (MPIR_F32
+                               for a solver created with UF = MPIR_F64) */
   double residual_norm;  /* ||r||_inf / ||b_scaled||_inf at exit (gmres_ir.hpp:580) */
   double backward_error; /* ||b - Kx||_inf / (||K||_inf ||x||_inf + ||b||_inf) */
   double factor_ms;      /* device time of the last numeric factorization */
@@ -130,9 +132,10 @@ int mpir_qdldl_ltsolve(int64_t n, const int64_t *Lp, const int64_t *Li,
                        int device);
 
 /* QDLDL_solve without device allocation (no counterpart in the reference).
- * For callers that cannot call cudaMalloc: code that runs while a CUDA stream
- * capture is open, where allocation is not allowed, and processes whose device
- * memory is handed out entirely by their own pooling allocator.  Same
+ * For callers that cannot call cudaMalloc: processes whose device memory is
+ * reserved up front and handed out entirely by their own pooling allocator
+ * (nothing is left for the library to allocate), and loops that must not
+ * take cudaMalloc's implicit device-wide synchronisation.  Same
  * arithmetic as mpir_qdldl_solve (float32 L and Dinv, float64 x, host
  * arrays), but every device buffer it needs is carved out of one fixed 32 MiB
  * array that each GPU holds for as long as the library is loaded.  Limits:
@@ -143,7 +146,8 @@ int mpir_qdldl_ltsolve(int64_t n, const int64_t *Lp, const int64_t *Li,
  * device address, so make it before any stream capture.  All calls share the
  * array: calls that overlap on the GPU (other host threads, other streams)
  * race and must be serialised by the caller.  Runs on the calling thread's
- * per-thread default stream and returns when x is back on the host. */
+ * per-thread default stream and returns when x is back on the host; the
+ * calling thread's current device is the same on return as before. */
 int mpir_qdldl_solve_noalloc(int64_t n, const int64_t *Lp, const int64_t *Li,
                              const float *Lx, const float *Dinv, double *x,
                              int device);
@@ -153,8 +157,12 @@ int mpir_qdldl_solve_noalloc(int64_t n, const int64_t *Lp, const int64_t *Li,
 /* uf/uw/ur as MPIR_F* above.  Provided: uf = MPIR_F32 (float32 factor),
  * MPIR_BF16 or MPIR_F16 (factor whose trailing updates run on the tensor
  * cores with 16-bit operands and float32 accumulation; panels, diagonal
- * blocks and panel solves stay float32); uw = MPIR_F64; ur = MPIR_F64 or
- * MPIR_DD. */
+ * blocks and panel solves stay float32), or MPIR_F64, the reference
+ * example's GmresLDLIR<double, double, dd_real> (examples/example.cpp:78-80):
+ * the diagonal scaling uses eps(double) as the reference's Compute does
+ * (gmres_ir.hpp:352) and the factor is the float32 one (refinement brings
+ * the solution to the same backward error; rep.factor_prec says MPIR_F32);
+ * uw = MPIR_F64; ur = MPIR_F64 or MPIR_DD. */
 int mpir_solver_create(mpir_solver *out, int uf, int uw, int ur, int device);
 int mpir_solver_destroy(mpir_solver s);
 

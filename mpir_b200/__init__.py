@@ -47,12 +47,12 @@ class Report(C.Structure):
     _fields_ = [("status", C.c_int32), ("ir_iterations", C.c_int32),
                 ("gmres_iterations", C.c_int32), ("precond_applies", C.c_int32),
                 ("spmv_count", C.c_int32), ("reorth_count", C.c_int32),
-                ("stop_reason", C.c_int32), ("pad", C.c_int32),
+                ("stop_reason", C.c_int32), ("factor_prec", C.c_int32),
                 ("residual_norm", C.c_double), ("backward_error", C.c_double),
                 ("factor_ms", C.c_double), ("solve_ms", C.c_double)]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class Info(C.Structure):
@@ -280,8 +280,8 @@ def LUIR_QDLDL(n, Ap, Ai, Ax, b, fact_prec="f32", maxiter=10, device=0):
 
 
 def QDLDL_solve_noalloc(n, Lp, Li, Lx, Dinv, x, device=0):
-    """QDLDL_solve for callers that cannot allocate device memory (inside an
-    open stream capture, or under a process-wide pooling allocator): float32
+    """QDLDL_solve for callers that cannot allocate device memory (device
+    memory reserved by a process-wide pooling allocator): float32
     factor, float64 x in place; all device data lives in the library's fixed
     32 MiB array.  Fronts of at most 64 rows; raises MpirError beyond the
     limits.  Calls overlapping on the GPU share that array and race."""

@@ -7,6 +7,8 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <memory>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -315,6 +317,46 @@ int64_t mpir_qdldl_factor(int64_t n, const int64_t *Ap, const int64_t *Ai, const
   });
 }
 
+// The analysed, uploaded form of a caller's QDLDL factor, kept between
+// QDLDL_solve calls: the reference's usage (LUIR_QDLDL, luir.hpp:165-205)
+// solves with one factor many times, and the analysis of L's pattern, the
+// packing into panels, the upload and the inversion of the diagonal blocks
+// are then done once.  An entry is found by the device, the factor type and
+// hashes of the whole of Lp, Li, Lx and Dinv (a factor rewritten in place
+// misses the cache); the two most recently used entries are kept.
+struct QdldlCached {
+  int                             device = 0, prec = 0;
+  int64_t                         n = 0;
+  uint64_t                        hash = 0;
+  std::unique_ptr<Plan>           P;
+  std::unique_ptr<Numeric>        F;
+  std::unique_ptr<SolveWorkspace> ws;
+  DeviceBuffer                    xd;
+  cudaStream_t                    s = nullptr;
+  ~QdldlCached() {
+    if (s) {
+      cudaSetDevice(device);
+      cudaStreamSynchronize(s);
+      cudaStreamDestroy(s);
+    }
+  }
+};
+static std::mutex                               g_qdldl_mu;
+static std::vector<std::unique_ptr<QdldlCached>> g_qdldl_cache;  // most recent last
+
+static uint64_t hash_words(const void *p, size_t bytes, uint64_t h) {
+  const unsigned char *c = static_cast<const unsigned char *>(p);
+  size_t               i = 0;
+  for (; i + 8 <= bytes; i += 8) {
+    uint64_t w;
+    std::memcpy(&w, c + i, 8);
+    h = (h ^ w) * 0x100000001b3ull;
+    h ^= h >> 29;
+  }
+  for (; i < bytes; i++) h = (h ^ c[i]) * 0x100000001b3ull;
+  return h;
+}
+
 static int qdldl_solve_phases(int64_t n, const int64_t *Lp, const int64_t *Li, const void *Lx,
                               const void *Dinv, int fact_prec, void *x, int x_prec, int device,
                               int phases) {
@@ -324,55 +366,88 @@ static int qdldl_solve_phases(int64_t n, const int64_t *Lp, const int64_t *Li, c
     if (x_prec != kF64 && x_prec != kF32)
       throw StatusError(MPIR_ERR_UNSUPPORTED, "vector type not provided (F64, F32)");
     if (n <= 0) return n < 0 ? MPIR_ERR_ARGUMENT : MPIR_OK;
-    Symbolic    S;
-    std::string err;
-    const int   rc = analyze_from_L(n, Lp, Li, S, err);
-    if (rc != kOk) throw StatusError(rc, err);
-    StreamGuard sg(device);
-    Plan        P;
-    P.build(std::move(S), sg.s);
-    const Symbolic &Sy = P.S;
-    Numeric         F;
-    F.allocate(P);
-    std::vector<float> lx, dv(n, 1.0f);
-    const int64_t      nl = Lp[n];
-    if (fact_prec == kF32) {
-      lx.assign(static_cast<const float *>(Lx), static_cast<const float *>(Lx) + nl);
-      if (Dinv) dv.assign(static_cast<const float *>(Dinv), static_cast<const float *>(Dinv) + n);
-    } else {
-      from_16(Lx, nl, fact_prec, lx, sg.s);
-      if (Dinv) from_16(Dinv, n, fact_prec, dv, sg.s);
-    }
-    std::vector<float> pan(Sy.panel_elems, 0.0f);
-    for (int64_t J = 0; J < Sy.ns; J++) {
-      const int64_t f = Sy.sfirst[J], l = Sy.sfirst[J + 1], h = Sy.h(J);
-      for (int64_t j = f; j < l; j++) {
-        pan[Sy.slofs[J] + (j - f) * h + (j - f)] = 1.0f;
-        for (int64_t p = Lp[j]; p < Lp[j + 1]; p++)
-          pan[Sy.slofs[J] + (j - f) * h + local_row(Sy, J, Li[p])] = lx[p];
+    const int64_t nl    = Lp[n];
+    const size_t  esize = fact_prec == kF32 ? 4 : 2;
+    uint64_t      h     = 0xcbf29ce484222325ull ^ static_cast<uint64_t>(n);
+    h = hash_words(Lp, (n + 1) * sizeof(int64_t), h);
+    h = hash_words(Li, nl * sizeof(int64_t), h);
+    h = hash_words(Lx, nl * esize, h);
+    h = Dinv ? hash_words(Dinv, n * esize, h) : (h ^ 0x5bd1e995ull);
+    std::lock_guard<std::mutex> lock(g_qdldl_mu);
+    QdldlCached *E = nullptr;
+    for (size_t i = 0; i < g_qdldl_cache.size(); i++) {
+      QdldlCached &c = *g_qdldl_cache[i];
+      if (c.device == device && c.prec == fact_prec && c.n == n && c.hash == h) {
+        std::unique_ptr<QdldlCached> keep = std::move(g_qdldl_cache[i]);
+        g_qdldl_cache.erase(g_qdldl_cache.begin() + i);
+        g_qdldl_cache.push_back(std::move(keep));
+        E = g_qdldl_cache.back().get();
+        break;
       }
     }
-    MPIR_CUDA(cudaMemcpyAsync(F.panel.as<void>(), pan.data(), pan.size() * sizeof(float),
-                              cudaMemcpyHostToDevice, sg.s));
-    MPIR_CUDA(cudaMemcpyAsync(F.Dinv.as<void>(), dv.data(), n * sizeof(float),
-                              cudaMemcpyHostToDevice, sg.s));
-    invert_diag_blocks(P, F, sg.s);
-    SolveWorkspace ws;
-    ws.allocate(P);
-    DeviceBuffer        xd(n * sizeof(double));
+    if (!E) {
+      Symbolic    S;
+      std::string err;
+      const int   rc = analyze_from_L(n, Lp, Li, S, err);
+      if (rc != kOk) throw StatusError(rc, err);
+      auto c    = std::make_unique<QdldlCached>();
+      c->device = device;
+      c->prec   = fact_prec;
+      c->n      = n;
+      c->hash   = h;
+      MPIR_CUDA(cudaSetDevice(device));
+      MPIR_CUDA(cudaStreamCreateWithFlags(&c->s, cudaStreamNonBlocking));
+      c->P = std::make_unique<Plan>();
+      c->P->build(std::move(S), c->s);
+      const Symbolic &Sy = c->P->S;
+      c->F = std::make_unique<Numeric>();
+      c->F->allocate(*c->P);
+      std::vector<float> lx, dv(n, 1.0f);
+      if (fact_prec == kF32) {
+        lx.assign(static_cast<const float *>(Lx), static_cast<const float *>(Lx) + nl);
+        if (Dinv) dv.assign(static_cast<const float *>(Dinv), static_cast<const float *>(Dinv) + n);
+      } else {
+        from_16(Lx, nl, fact_prec, lx, c->s);
+        if (Dinv) from_16(Dinv, n, fact_prec, dv, c->s);
+      }
+      std::vector<float> pan(Sy.panel_elems, 0.0f);
+      for (int64_t J = 0; J < Sy.ns; J++) {
+        const int64_t f = Sy.sfirst[J], l = Sy.sfirst[J + 1], hh = Sy.h(J);
+        for (int64_t j = f; j < l; j++) {
+          pan[Sy.slofs[J] + (j - f) * hh + (j - f)] = 1.0f;
+          for (int64_t p = Lp[j]; p < Lp[j + 1]; p++)
+            pan[Sy.slofs[J] + (j - f) * hh + local_row(Sy, J, Li[p])] = lx[p];
+        }
+      }
+      MPIR_CUDA(cudaMemcpyAsync(c->F->panel.as<void>(), pan.data(), pan.size() * sizeof(float),
+                                cudaMemcpyHostToDevice, c->s));
+      MPIR_CUDA(cudaMemcpyAsync(c->F->Dinv.as<void>(), dv.data(), n * sizeof(float),
+                                cudaMemcpyHostToDevice, c->s));
+      invert_diag_blocks(*c->P, *c->F, c->s);
+      c->F->trim();  // the solves read L, Dinv and the block inverses only
+      c->ws = std::make_unique<SolveWorkspace>();
+      c->ws->allocate(*c->P);
+      c->xd.resize(n * sizeof(double));
+      MPIR_CUDA(cudaStreamSynchronize(c->s));
+      if (g_qdldl_cache.size() >= 2) g_qdldl_cache.erase(g_qdldl_cache.begin());
+      g_qdldl_cache.push_back(std::move(c));
+      E = g_qdldl_cache.back().get();
+    }
+    MPIR_CUDA(cudaSetDevice(device));
     std::vector<double> xh(n);
     for (int64_t i = 0; i < n; i++)
       xh[i] = x_prec == kF64 ? static_cast<const double *>(x)[i]
                              : static_cast<double>(static_cast<const float *>(x)[i]);
-    MPIR_CUDA(cudaMemcpyAsync(xd.as<void>(), xh.data(), n * sizeof(double),
-                              cudaMemcpyHostToDevice, sg.s));
-    ldlt_solve(P, F, xd.as<double>(), ws, sg.s, phases);
-    MPIR_CUDA(cudaMemcpyAsync(xh.data(), xd.as<void>(), n * sizeof(double),
-                              cudaMemcpyDeviceToHost, sg.s));
-    MPIR_CUDA(cudaStreamSynchronize(sg.s));
+    MPIR_CUDA(cudaMemcpyAsync(E->xd.as<void>(), xh.data(), n * sizeof(double),
+                              cudaMemcpyHostToDevice, E->s));
+    ldlt_solve(*E->P, *E->F, E->xd.as<double>(), *E->ws, E->s, phases);
+    MPIR_CUDA(cudaMemcpyAsync(xh.data(), E->xd.as<void>(), n * sizeof(double),
+                              cudaMemcpyDeviceToHost, E->s));
+    MPIR_CUDA(cudaStreamSynchronize(E->s));
     int32_t wait_err = 0;
-    MPIR_CUDA(cudaMemcpy(&wait_err, ws.err.as<void>(), sizeof wait_err, cudaMemcpyDeviceToHost));
+    MPIR_CUDA(cudaMemcpy(&wait_err, E->ws->err.as<void>(), sizeof wait_err, cudaMemcpyDeviceToHost));
     if (wait_err != 0) {
+      MPIR_CUDA(cudaMemset(E->ws->err.as<void>(), 0, sizeof wait_err));
       g_err = "a bounded device wait of the triangular solves ran out";
       return MPIR_ERR_TIMEOUT;
     }
@@ -416,9 +491,10 @@ int mpir_solver_create(mpir_solver *out, int uf, int uw, int ur, int device) {
   return guard([&]() -> int {
     if (!out) return MPIR_ERR_ARGUMENT;
     *out = nullptr;
-    if ((uf != kF32 && uf != kBF16 && uf != kF16) || uw != kF64 || (ur != kF64 && ur != kDD))
+    if ((uf != kF64 && uf != kF32 && uf != kBF16 && uf != kF16) || uw != kF64 ||
+        (ur != kF64 && ur != kDD))
       throw StatusError(MPIR_ERR_UNSUPPORTED,
-                        "provided precisions: UF=F32/BF16/F16, UW=F64, UR=F64 or DD");
+                        "provided precisions: UF=F64/F32/BF16/F16, UW=F64, UR=F64 or DD");
     auto *h = new mpir_solver_s{nullptr, {}};
     try {
       h->impl = new Solver(uf, uw, ur, device);

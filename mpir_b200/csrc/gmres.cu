@@ -315,6 +315,7 @@ int Solver::solve_device(const double *d_b, double *d_x, Report *rep) {
   MPIR_CUDA(cudaSetDevice(device));
   ensure_vectors();
   Report        st;
+  st.factor_prec = applied_prec();
   const Plan   &P = *plan_;
   const int64_t n = P.S.n;
   cudaStream_t  s = stream_;
@@ -425,6 +426,7 @@ int Solver::luir_device(const double *d_b, double *d_x, int maxiter, Report *rep
   MPIR_CUDA(cudaSetDevice(device));
   ensure_vectors();
   Report        st;
+  st.factor_prec = applied_prec();
   const Plan   &P = *plan_;
   const int64_t n = P.S.n;
   cudaStream_t  s = stream_;

@@ -324,6 +324,7 @@ int Solver::solve_batch_device(int nrhs, const double *d_B, double *d_X, Report 
   double *ADp = ADp_.as<double>();
   const bool dd = ur == kDD;
   std::vector<Report> st(nb);
+  for (Report &r : st) r.factor_prec = applied_prec();
   std::vector<double> inf(8 * static_cast<size_t>(nb));
   vecb_.rhs_in_b(nb, P.perm.as<int64_t>(), num_.AD.as<double>(), d_B, bs, ADp, bbp_.as<double>(),
                  n, s);

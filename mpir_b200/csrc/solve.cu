@@ -769,9 +769,10 @@ void ldlt_solve(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
 // ---------------------------------------------------------------------------
 // QDLDL_solve without device allocation.
 //
-// For callers that cannot call cudaMalloc: code running while a CUDA stream
-// capture is open (allocation is not allowed there), and processes whose
-// device memory is handed out entirely by their own pooling allocator.  All
+// For callers that cannot call cudaMalloc: processes whose device memory is
+// reserved up front and handed out entirely by their own pooling allocator,
+// and loops that cannot take cudaMalloc's implicit device-wide
+// synchronisation.  All
 // device data of this entry point (the supernodal layout of L, the factor
 // values, Dinv, the fronts' update vectors and x) is packed into the one
 // file-scope array below, of fixed size, that every GPU holds once this
@@ -787,8 +788,20 @@ static __device__ __align__(256) unsigned char g_solve_scratch[kNoAllocScratchBy
 
 namespace {
 // Device address of g_solve_scratch on each device, looked up on the first
-// call that uses that device.
-void *g_solve_scratch_addr[kNoAllocMaxDevices] = {};
+// call that uses that device (atomic: host threads may make their first
+// calls at the same time; they store the same address).
+std::atomic<void *> g_solve_scratch_addr[kNoAllocMaxDevices] = {};
+
+// Restores the calling thread's current device on every return path.
+struct DeviceRestore {
+  int  saved = -1;
+  DeviceRestore() {
+    if (cudaGetDevice(&saved) != cudaSuccess) saved = -1;
+  }
+  ~DeviceRestore() {
+    if (saved >= 0) cudaSetDevice(saved);
+  }
+};
 }  // namespace
 
 int qdldl_solve_noalloc(int64_t n, const int64_t *Lp, const int64_t *Li, const float *Lx,
@@ -858,14 +871,15 @@ int qdldl_solve_noalloc(int64_t n, const int64_t *Lp, const int64_t *Li, const f
           std::to_string(kNoAllocScratchBytes);
     return kBadArgument;
   }
+  DeviceRestore restore;  // the caller's current device is left as it was
   MPIR_CUDA(cudaSetDevice(device));
-  if (!g_solve_scratch_addr[device]) {
-    void             *p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_solve_scratch);
+  void *addr = g_solve_scratch_addr[device].load(std::memory_order_acquire);
+  if (!addr) {
+    const cudaError_t e = cudaGetSymbolAddress(&addr, g_solve_scratch);
     if (e != cudaSuccess) throw CudaError(e, "cudaGetSymbolAddress(g_solve_scratch)");
-    g_solve_scratch_addr[device] = p;
+    g_solve_scratch_addr[device].store(addr, std::memory_order_release);
   }
-  unsigned char     *base = static_cast<unsigned char *>(g_solve_scratch_addr[device]);
+  unsigned char     *base = static_cast<unsigned char *>(addr);
   const cudaStream_t s    = cudaStreamPerThread;
   for (const Region &r : reg)
     if (r.src && r.bytes)

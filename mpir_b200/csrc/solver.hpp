@@ -28,7 +28,7 @@ struct Report {
   int32_t reorth_count     = 0;
   int32_t stop_reason      = 0;  // 0 max iterations, 1 small update,
                                  // 2 stagnation, 3 exact residual
-  int32_t pad              = 0;
+  int32_t factor_prec      = 0;  // type the factor is stored and applied in
   double  residual_norm    = 0;
   double  backward_error   = 0;
   double  factor_ms        = 0;
@@ -87,6 +87,9 @@ class Solver {
   // single-vector kernels, several by the several-vector kernels.
   void precond_device(int nrhs, double *d_X);
   static constexpr int kMaxBatch = 16;
+  // The type the factor is computed and applied in (a double factor type is
+  // served by the float32 factor).
+  int applied_prec() const { return uf == kF64 ? kF32 : uf; }
   // Plain iterative refinement with the factor (LUIR_QDLDL); host and
   // device vectors.
   int luir(const double *b, double *x, int maxiter, Report *rep);

@@ -320,3 +320,23 @@ def test_low_precision_factor_tier_converges(uf):
         x = solver.Solve(s.b)
         be = kkt.backward_error(s.n, s.Ap, s.Ai, s.Ax, x, s.b)
         assert be <= 1e-14, (uf, be, solver.last_report)
+
+
+@pytest.mark.parametrize("name,s", list(small_systems())[:3])
+def test_forward_error_against_fp64_direct_ldlt(ref_lib, name, s):
+    """Forward error of the GPU GMRES-IR solution against an FP64 direct
+    LDL^T solution: the reference's QDLDL_factor<double> and QDLDL_solve on
+    the same permuted matrix."""
+    solver = mp.GmresLDLIR()
+    solver.Compute(s.Ap, s.Ai, s.Ax, 0)
+    x = solver.Solve(s.b)
+    perm = solver.symbolic()["perm"]
+    Cp, Ci, Cx = permuted_upper(s.n, s.Ap, s.Ai, s.Ax, perm)
+    st, Lp, Li, Lx, D, Dinv = ref_lib.factor(s.n, Cp, Ci, Cx, np.float64)
+    xd_p = ref_lib.solve(s.n, Lp, Li, Lx, Dinv, s.b[perm])
+    xd = np.empty_like(xd_p)
+    xd[perm] = xd_p
+    fe_direct = kkt.forward_error(xd, s.x_true)
+    fe = float(np.max(np.abs(x - xd)) / np.max(np.abs(xd)))
+    assert fe <= max(10 * fe_direct, 1e-12), (fe, fe_direct)
+    assert kkt.forward_error(x, s.x_true) <= max(10 * fe_direct, 1e-12)

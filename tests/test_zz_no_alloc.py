@@ -1,8 +1,8 @@
 """QDLDL_solve for callers that cannot allocate device memory.
 
-Some callers cannot call cudaMalloc: code running while a CUDA stream capture
-is open (allocation is refused there) and processes whose device memory is
-owned entirely by their own pooling allocator.  mpir_qdldl_solve_noalloc
+Some callers cannot call cudaMalloc: processes whose device memory is reserved
+up front and owned entirely by their own pooling allocator, and loops that
+cannot take cudaMalloc's implicit device-wide synchronisation.  mpir_qdldl_solve_noalloc
 serves them from a fixed array the library holds on every GPU.  This file
 checks it through the C ABI against the allocating mpir_qdldl_solve on two
 calls in a row, and that out-of-limit factors are refused cleanly.  It is
@@ -44,6 +44,13 @@ def test_noalloc_matches_allocating_solve_twice(oracle_lib):
         assert rel_norm_diff(x, x_ref) <= 1e-10
         x_or = oracle_lib.solve(n, Lp, Li, Lx, Dinv, b)
         assert rel_norm_diff(x, x_or) <= 1e-10
+    # a warmed-up call takes no device memory: the free bytes cudaMemGetInfo
+    # reports are the same before and after it
+    import torch
+    x = rng.standard_normal(n)
+    free0 = torch.cuda.mem_get_info(0)[0]
+    mp.QDLDL_solve_noalloc(n, Lp, Li, Lx, Dinv, x)
+    assert torch.cuda.mem_get_info(0)[0] == free0
 
 
 def test_noalloc_refuses_out_of_limit_factors(oracle_lib):
