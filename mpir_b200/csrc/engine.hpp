@@ -148,6 +148,11 @@ class Numeric {
   // Packed fronts for the tensor-core updates: rows (pack) and pivots
   // (packd: D, then sign(D) sqrt|D|, Plan::pd_elems floats each).
   DeviceBuffer pack, packd;
+  // 16-bit copy of the panels for the solves of the bfloat16 / float16
+  // tiers (store_prec 2 / 3; 1 = the solves read the float32 panels).
+  DeviceBuffer panel16;
+  int          store_prec = 1;
+  int          solve_prec() const { return panel16.bytes() ? store_prec : 1; }
   // B operands converted ahead of the 3xTF32 updates (GemmProb::bc).
   DeviceBuffer bconv;
   DeviceBuffer AD, Axs, Kval, Korig, Ax;
@@ -173,7 +178,7 @@ class Numeric {
   void trim();
   bool has_scratch = false;
   // Device memory allocate() takes for P, and what this factor holds.
-  static size_t bytes_for(const Plan &P);
+  static size_t bytes_for(const Plan &P, int store_prec = 1);
   size_t        device_bytes() const;
   // Scale the caller's values (device, caller order), assemble and factor.
   void run(const Plan &P, const double *d_Ax, double eps_uf, cudaStream_t s);

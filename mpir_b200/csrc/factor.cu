@@ -16,6 +16,9 @@
 //     C -= (L D) L^T.
 // D is left on each panel's diagonal and copied to D / Dinv (permuted order).
 #include <atomic>
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <algorithm>
 #include <climits>
 #include <cmath>
@@ -891,6 +894,22 @@ __global__ void __launch_bounds__(kDiagThreads)
   }
 }
 
+// The panels rounded to bfloat16 (bf != 0) or float16 for the solves of the
+// 16-bit tiers: L is stored in the tier's type and the solves read half the
+// bytes (their arithmetic stays float64).
+__global__ void k_panel_to16(int64_t n, const float *in, uint16_t *out, int bf) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    if (bf) {
+      const __nv_bfloat16 v = __float2bfloat16_rn(in[i]);
+      out[i]                = *reinterpret_cast<const uint16_t *>(&v);
+    } else {
+      const __half v = __float2half_rn(in[i]);
+      out[i]         = *reinterpret_cast<const uint16_t *>(&v);
+    }
+  }
+}
+
 void invert_diag_blocks(const Plan &P, Numeric &F, cudaStream_t s) {
   if (P.ndesc == 0) return;
   const int smem = kNB * (kNB + 1) * (sizeof(double) + sizeof(float));
@@ -1290,6 +1309,10 @@ void Numeric::allocate(const Plan &P) {
   release_graph();
   const Symbolic &S = P.S;
   panel.resize(std::max<int64_t>(S.panel_elems, 1) * sizeof(float));
+  if (store_prec == 2 || store_prec == 3)
+    panel16.resize(std::max<int64_t>(S.panel_elems, 1) * 2);
+  else
+    panel16.release();
   linv64.resize(std::max<int64_t>(P.linv_elems, 1) * sizeof(double));
   linv64t.resize(std::max<int64_t>(P.linv_elems, 1) * sizeof(double));
   D.resize(std::max<int64_t>(S.n, 1) * sizeof(float));
@@ -1307,6 +1330,7 @@ void Numeric::ensure_scratch(const Plan &P) {
   if (has_scratch) return;
   release_graph();  // a recorded factorization points at the old buffers
   const Symbolic &S = P.S;
+  if (!panel.bytes()) panel.resize(std::max<int64_t>(S.panel_elems, 1) * sizeof(float));
   uarena.resize(std::max<int64_t>(S.uarena_elems, 1) * sizeof(float));
   linv.resize(std::max<int64_t>(P.linv_elems, 1) * sizeof(float));
   ws.resize(std::max<int64_t>(P.ws_elems, 1) * sizeof(float));
@@ -1325,13 +1349,14 @@ void Numeric::ensure_scratch(const Plan &P) {
 void Numeric::trim() {
   release_graph();
   for (DeviceBuffer *b : {&uarena, &linv, &ws, &bconv, &pack, &packd, &Axs, &Ax}) b->release();
+  if (panel16.bytes()) panel.release();  // the solves read the 16-bit copy
   has_scratch = false;
 }
 
-size_t Numeric::bytes_for(const Plan &P) {
+size_t Numeric::bytes_for(const Plan &P, int store_prec) {
   const Symbolic &S  = P.S;
   auto            at = [](int64_t e, size_t b) { return std::max<int64_t>(e, 1) * b; };
-  return at(S.panel_elems, 4) + at(S.uarena_elems, 4) + at(P.linv_elems, 4) +
+  return at(S.panel_elems, store_prec == 1 ? 4 : 6) + at(S.uarena_elems, 4) + at(P.linv_elems, 4) +
          2 * at(P.linv_elems, 8) + at(P.ws_elems, 4) + at(P.bconv_elems, 4) +
          at(P.pk_elems, 4) + at(2 * P.pd_elems, 4) + 2 * at(S.n, 4) + sizeof(FactorStatus) +
          at(S.n, 8) + 2 * at(S.nnz, 8) + 2 * at(P.nnz_full, 8);
@@ -1339,7 +1364,7 @@ size_t Numeric::bytes_for(const Plan &P) {
 
 size_t Numeric::device_bytes() const {
   size_t b = 0;
-  for (const DeviceBuffer *d : {&panel, &uarena, &linv, &linv64, &linv64t, &D, &Dinv, &status,
+  for (const DeviceBuffer *d : {&panel, &panel16, &uarena, &linv, &linv64, &linv64t, &D, &Dinv, &status,
                                 &ws, &pack, &packd, &bconv, &AD, &Axs, &Kval, &Korig, &Ax})
     b += d->bytes();
   return b;
@@ -1514,6 +1539,13 @@ void Numeric::run(const Plan &P, const double *d_Ax, double eps, cudaStream_t s)
   kt.begin(kKcDiag, s);
   invert_diag_blocks(P, *this, s);
   kt.end(s);
+  if (panel16.bytes() && S.panel_elems) {
+    kt.begin(kKcScatter, s);
+    launch(k_panel_to16, static_cast<unsigned>(std::min<int64_t>((S.panel_elems + 255) / 256, 148 * 16)),
+           256, 0, s, S.panel_elems, panel.as<float>(), panel16.as<uint16_t>(),
+           store_prec == 2 ? 1 : 0);
+    kt.end(s);
+  }
   valid = true;
 }
 

@@ -89,6 +89,8 @@ void Solver::adopt(std::shared_ptr<Plan> P) {
   MPIR_CUDA(cudaSetDevice(device));
   const int64_t n = P->S.n;
   plan_ = std::move(P);
+  // The 16-bit tiers keep L in their type for the solves.
+  num_.store_prec = uf == kBF16 ? 2 : uf == kF16 ? 3 : 1;
   num_.allocate(*plan_);
   num_.update_mode = update_mode_for(uf);
   ws_.allocate(*plan_);
@@ -117,10 +119,10 @@ size_t Solver::device_bytes() const {
   return b;
 }
 
-size_t Solver::bytes_for(const Plan &P, int64_t gmres_iter, int width) {
+size_t Solver::bytes_for(const Plan &P, int64_t gmres_iter, int width, int uf) {
   const int64_t n  = std::max<int64_t>(P.S.n, 1);
   const int64_t m  = std::max<int64_t>(std::min(gmres_iter, n), 1);
-  size_t        b  = Numeric::bytes_for(P);
+  size_t        b  = Numeric::bytes_for(P, uf == kBF16 ? 2 : uf == kF16 ? 3 : 1);
   // single-vector workspace and vectors
   b += (std::max<int64_t>(P.S.z_elems, 1) + std::max<int64_t>(P.spart_elems, 1) +
         static_cast<int64_t>(kReadyCopies) * n + n) * sizeof(double);

@@ -251,7 +251,7 @@ struct Server::Impl {
       }
       if (job.kind != Job::kSolve) {
         const int    width = job.reqs.size() > 1 ? multi_width(static_cast<int>(job.reqs.size())) : 1;
-        const size_t need  = Solver::bytes_for(*plan, cfg.max_gmres_iterations, width);
+        const size_t need  = Solver::bytes_for(*plan, cfg.max_gmres_iterations, width, cfg.uf);
         {
           std::unique_lock<std::mutex> lk(mu);
           if (need > static_cast<size_t>(cfg.budget_bytes)) {

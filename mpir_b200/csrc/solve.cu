@@ -125,11 +125,12 @@ __device__ __forceinline__ double block_upper_apply(const double *Ls, const doub
 }
 
 // Forward
+template <class T>
 __global__ void __launch_bounds__(32 * kWarpsPerCta)
     k_fwd_small(const int32_t *list, int count, const int64_t *sfirst,
                 const int64_t *srowptr, const int64_t *slofs,
                 const int64_t *child_ptr, const int32_t *child_list,
-                const int32_t *srel, const int64_t *zofs, const float *panel,
+                const int32_t *srel, const int64_t *zofs, const T *panel,
                 double *x, double *zbuf) {
   __shared__ double zs[kWarpsPerCta][kSmallH];
   const int         warp = threadIdx.x / 32, lane = threadIdx.x % 32;
@@ -153,7 +154,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta)
   }
   // Columns four at a time; the next four columns' entries of this lane's
   // rows (lane + 32 t) are loaded while the current four are applied.
-  const float  *P  = panel + slofs[J];
+  const T      *P  = panel + slofs[J];
   constexpr int RT = kSmallH / 32;
   float         cur[4][RT], nxt[4][RT];
   auto          load4 = [&](float (*buf)[RT], int k0) {
@@ -162,7 +163,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta)
 #pragma unroll
       for (int t = 0; t < RT; t++) {
         const int k = k0 + u, i = lane + 32 * t;
-        buf[u][t]   = (k < w && i > k && i < h) ? P[i + (int64_t)k * h] : 0.0f;
+        buf[u][t]   = (k < w && i > k && i < h) ? to_f(P[i + (int64_t)k * h]) : 0.0f;
       }
   };
   load4(cur, 0);
@@ -247,8 +248,9 @@ __global__ void k_mark_pending(int64_t n, double *ready) {
 // A diagonal row block then solves y_R = Linv_R z_R into x and the ready
 // buffer (block product with warp-local slices, see blk_i); rows at or past
 // w are the front's update vector for its parent.
+template <class T>
 __global__ void __launch_bounds__(kSolveThreads, 1)
-    k_fwd_fronts(const SolveItem *items, const float *panel, const double *linv64t, const int64_t *gp,
+    k_fwd_fronts(const SolveItem *items, const T *panel, const double *linv64t, const int64_t *gp,
                  const int64_t *gsrc, double *x, double *zbuf, int32_t *tickets,
                  double *ready, int32_t *err) {
   extern __shared__ __align__(16) double tri[];  // kFwdTri doubles: the staged Linv_R
@@ -286,7 +288,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   const int64_t h = F.h;
   const int     w = F.w;
   const int64_t r = static_cast<int64_t>(R) * kNB + rr;
-  const float  *P  = panel + F.panel;
+  const T      *P  = panel + F.panel;
   const int64_t n  = F.n;
   const double *yr = ready + ((item * 16 + threadIdx.x / 32) % kReadyCopies) * n + F.col0;
   const int     tiles = min(R, F.nb);
@@ -311,7 +313,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
     const int c0 = b * kNB + qq * 32;
 #pragma unroll
     for (int k = 0; k < 32; k++)
-      dst[k] = (r < h && c0 + k < w) ? __ldg(P + r + static_cast<int64_t>(c0 + k) * h) : 0.0f;
+      dst[k] = (r < h && c0 + k < w) ? to_f(__ldg(P + r + static_cast<int64_t>(c0 + k) * h)) : 0.0f;
   };
   // The lane's entry of y_b is loaded ahead with the tile's L values too;
   // only an entry that was still pending then is waited for.
@@ -384,7 +386,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
       double a2 = 0.0;
       if (r >= w && r < h)
         for (int k = qq * 32; k < min(nbk, qq * 32 + 32); k++)
-          a2 += static_cast<double>(P[r + static_cast<int64_t>(R * kNB + k) * h]) * ys2[pad(k)];
+          a2 += static_cast<double>(to_f(P[r + static_cast<int64_t>(R * kNB + k) * h])) * ys2[pad(k)];
       part[qq][rr] = a2;
       __syncthreads();
       if (qq == 0 && r >= w && r < h)
@@ -401,10 +403,11 @@ __global__ void k_dscale(int64_t n, const float *Dinv, double *x) {
 
 // ---------------------------------------------------------------------------
 // Backward
+template <class T>
 __global__ void __launch_bounds__(32 * kWarpsPerCta)
     k_bwd_small(const int32_t *list, int count, const int64_t *sfirst,
                 const int64_t *srowptr, const int32_t *srows,
-                const int64_t *slofs, const float *panel, double *x) {
+                const int64_t *slofs, const T *panel, double *x) {
   __shared__ double zs[kWarpsPerCta][kSmallH];
   const int         warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   const int         idx  = blockIdx.x * kWarpsPerCta + warp;
@@ -419,7 +422,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta)
   __syncwarp();
   // Columns four at a time from the last; the next four columns' entries of
   // this lane's rows (lane + 32 t) are loaded while the current four are used.
-  const float  *P  = panel + slofs[J];
+  const T      *P  = panel + slofs[J];
   constexpr int RT = kSmallH / 32;
   float         cur[4][RT], nxt[4][RT];
   auto          load4 = [&](float (*buf)[RT], int k0) {  // columns k0, k0-1, ..
@@ -428,7 +431,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta)
 #pragma unroll
       for (int t = 0; t < RT; t++) {
         const int k = k0 - u, i = lane + 32 * t;
-        buf[u][t]   = (k >= 0 && i > k && i < h) ? P[i + (int64_t)k * h] : 0.0f;
+        buf[u][t]   = (k >= 0 && i > k && i < h) ? to_f(P[i + (int64_t)k * h]) : 0.0f;
       }
   };
   load4(cur, w - 1);
@@ -461,8 +464,9 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta)
 // Backward solve, off-diagonal rows: CTA c takes rows w + 128c .. of one
 // front and writes t_k = sum_r L_{r,k} z_r for every column k of the front
 // (warp per column, rows over the lanes, shuffle reduction) to its partials.
+template <class T>
 __global__ void __launch_bounds__(kSolveThreads)
-    k_bwd_chunks(const SolveFront *fr, const int32_t *fmap, const float *panel,
+    k_bwd_chunks(const SolveFront *fr, const int32_t *fmap, const T *panel,
                  const int32_t *srows,
                  const double *x, double *part) {
   __shared__ double zr[kNB];
@@ -474,17 +478,17 @@ __global__ void __launch_bounds__(kSolveThreads)
   const int         nr = static_cast<int>(h - r0 < kNB ? h - r0 : kNB);
   if (tid < kNB) zr[tid] = tid < nr ? x[srows[F.rows + r0 + tid]] : 0.0;
   __syncthreads();
-  const float  *P  = panel + F.panel + r0;
+  const T      *P  = panel + F.panel + r0;
   double       *pp = part + F.part + static_cast<int64_t>(c) * w;
   constexpr int kWarps = kSolveThreads / 32;
 #pragma unroll 2
   for (int64_t k = warp; k < w; k += kWarps) {
-    const float *col = P + k * h;
+    const T     *col = P + k * h;
     double       s   = 0.0;
 #pragma unroll
     for (int i = 0; i < 4; i++) {
       const int rr = lane + 32 * i;
-      if (rr < nr) s += static_cast<double>(__ldg(col + rr)) * zr[rr];
+      if (rr < nr) s += static_cast<double>(to_f(__ldg(col + rr))) * zr[rr];
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
@@ -498,8 +502,9 @@ __global__ void __launch_bounds__(kSolveThreads)
 // each as soon as x_R is in the ready buffer); then x_b = Linv_b^T (z_b - t)
 // into x and the ready buffer.  In a tile, warp v takes the block's columns
 // 8v .. 8v+7 and the lanes the rows.
+template <class T>
 __global__ void __launch_bounds__(kSolveThreads, 1)
-    k_bwd_fronts(const SolveItem *items, const float *panel,
+    k_bwd_fronts(const SolveItem *items, const T *panel,
                  const double *linv64t,
                  double *x, const double *part, int32_t *tickets,
                  double *ready, int32_t *err) {
@@ -531,7 +536,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   const int         nbk = min(kNB, w - b * kNB);
   // This block's right-hand side, read now (not on the chain at the end).
   if (tid < nbk) v[tid] = x[F.col0 + b * kNB + tid];
-  const float      *P   = panel + F.panel;
+  const T          *P   = panel + F.panel;
   const int64_t     n   = F.n;
   const double     *xr  = ready + ((item * 16 + threadIdx.x / 32) % kReadyCopies) * n + F.col0;
   {
@@ -561,7 +566,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
       for (int i = 0; i < 4; i++) {
         const int rr = lane + 32 * i;
         dst[j][i]    = (c < nbk && rr < rows)
-                           ? __ldg(P + rb + rr + static_cast<int64_t>(b * kNB + c) * h)
+                           ? to_f(__ldg(P + rb + rr + static_cast<int64_t>(b * kNB + c) * h))
                            : 0.0f;
       }
     }
@@ -692,12 +697,12 @@ void ldlt_solve_graph(const Plan &P, const Numeric &F, double *x, SolveWorkspace
   MPIR_CUDA(cudaMemcpyAsync(x, ws.xbuf.as<void>(), n * sizeof(double), cudaMemcpyDeviceToDevice, s));
 }
 
-void ldlt_solve(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
-                cudaStream_t s, int phases) {
+template <class T>
+static void ldlt_solve_t(const Plan &P, const Numeric &F, const T *pan, double *x,
+                         SolveWorkspace &ws, cudaStream_t s, int phases) {
   const Symbolic &S  = P.S;
   KernelTimer    &kt = kernel_timer();
   if (S.n == 0) return;
-  const float *pan  = F.panel.as<float>();
   const double *lvt = F.linv64t.as<double>();
   double      *zbuf = ws.zbuf.as<double>();
   const int    nl   = static_cast<int>(P.levels.size());
@@ -714,9 +719,9 @@ void ldlt_solve(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
   if (block && (phases & kForward)) launch(k_mark_pending, nmark, 256, 0, s, nready, ready);
   static std::atomic<bool> attr{false};
   if (!attr) {
-    MPIR_CUDA(cudaFuncSetAttribute(k_fwd_fronts, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    MPIR_CUDA(cudaFuncSetAttribute(k_fwd_fronts<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(kFwdTri * sizeof(double))));
-    MPIR_CUDA(cudaFuncSetAttribute(k_bwd_fronts, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    MPIR_CUDA(cudaFuncSetAttribute(k_bwd_fronts<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(kTri * sizeof(double))));
     attr = true;
   }
@@ -724,13 +729,13 @@ void ldlt_solve(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
   for (int t = 0; t < nl && (phases & kForward); t++) {
     const LevelPlan &L = P.levels[t];
     if (L.sw_count > 0)
-      launch(k_fwd_small, (L.sw_count + kWarpsPerCta - 1) / kWarpsPerCta, 32 * kWarpsPerCta, 0,
+      launch(k_fwd_small<T>, (L.sw_count + kWarpsPerCta - 1) / kWarpsPerCta, 32 * kWarpsPerCta, 0,
              s, P.swarp_list.as<int32_t>() + L.sw_begin, L.sw_count, P.sfirst.as<int64_t>(),
              P.srowptr.as<int64_t>(), P.slofs.as<int64_t>(), P.child_ptr.as<int64_t>(),
              P.child_list.as<int32_t>(), P.srel.as<int32_t>(), P.zofs.as<int64_t>(), pan, x,
              zbuf);
     if (L.sf_count > 0) {
-      launch(k_fwd_fronts, L.fwd_items, kSolveThreads, kFwdTri * sizeof(double), s,
+      launch(k_fwd_fronts<T>, L.fwd_items, kSolveThreads, kFwdTri * sizeof(double), s,
              P.fwd_item.as<SolveItem>() + L.fwd_map0, pan, lvt, P.gp.as<int64_t>(),
              P.gsrc.as<int64_t>(), x, zbuf, sync + 2 * t, ready, err);
     }
@@ -746,16 +751,16 @@ void ldlt_solve(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
   for (int t = nl - 1; t >= 0; t--) {
     const LevelPlan &L = P.levels[t];
     if (L.sw_count > 0)
-      launch(k_bwd_small, (L.sw_count + kWarpsPerCta - 1) / kWarpsPerCta, 32 * kWarpsPerCta, 0,
+      launch(k_bwd_small<T>, (L.sw_count + kWarpsPerCta - 1) / kWarpsPerCta, 32 * kWarpsPerCta, 0,
              s, P.swarp_list.as<int32_t>() + L.sw_begin, L.sw_count, P.sfirst.as<int64_t>(),
              P.srowptr.as<int64_t>(), P.srows.as<int32_t>(), P.slofs.as<int64_t>(), pan, x);
     if (L.sf_count > 0) {
       if (L.bwd_chunk_items > 0)
-        launch(k_bwd_chunks, L.bwd_chunk_items, kSolveThreads, 0, s, sf + L.sf_begin,
+        launch(k_bwd_chunks<T>, L.bwd_chunk_items, kSolveThreads, 0, s, sf + L.sf_begin,
                P.chunk_map.as<int32_t>() + L.chunk_map0, pan, P.srows.as<int32_t>(),
                static_cast<const double *>(x),
                ws.part.as<double>());
-      launch(k_bwd_fronts, L.bwd_owner_items, kSolveThreads, kTri * sizeof(double), s,
+      launch(k_bwd_fronts<T>, L.bwd_owner_items, kSolveThreads, kTri * sizeof(double), s,
              P.own_item.as<SolveItem>() + L.own_map0, pan,
              F.linv64t.as<double>(), x,
              static_cast<const double *>(ws.part.as<double>()), sync + 2 * t + 1, ready, err);
@@ -763,6 +768,21 @@ void ldlt_solve(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
   }
   kt.end(s);
   MPIR_CHECK_LAUNCH();
+}
+
+
+void ldlt_solve(const Plan &P, const Numeric &F, double *x, SolveWorkspace &ws,
+                cudaStream_t s, int phases) {
+  switch (F.solve_prec()) {
+    case 2:
+      ldlt_solve_t(P, F, F.panel16.as<__nv_bfloat16>(), x, ws, s, phases);
+      break;
+    case 3:
+      ldlt_solve_t(P, F, F.panel16.as<__half>(), x, ws, s, phases);
+      break;
+    default:
+      ldlt_solve_t(P, F, F.panel.as<float>(), x, ws, s, phases);
+  }
 }
 
 
@@ -901,14 +921,14 @@ int qdldl_solve_noalloc(int64_t n, const int64_t *Lp, const int64_t *Li, const f
   const int      nl      = S.nlevels;
   for (int t = 0; t < nl; t++) {
     const int32_t cnt = static_cast<int32_t>(S.level_ptr[t + 1] - S.level_ptr[t]);
-    launch(k_fwd_small, (cnt + kWarpsPerCta - 1) / kWarpsPerCta, 32 * kWarpsPerCta, 0, s,
+    launch(k_fwd_small<float>, (cnt + kWarpsPerCta - 1) / kWarpsPerCta, 32 * kWarpsPerCta, 0, s,
            level + S.level_ptr[t], cnt, sfirst, srowptr, slofs, cptr, clist, srel, zofs, panel,
            xd, zbuf);
   }
   launch(k_dscale, static_cast<unsigned>((n + 255) / 256), 256, 0, s, n, dinv, xd);
   for (int t = nl - 1; t >= 0; t--) {
     const int32_t cnt = static_cast<int32_t>(S.level_ptr[t + 1] - S.level_ptr[t]);
-    launch(k_bwd_small, (cnt + kWarpsPerCta - 1) / kWarpsPerCta, 32 * kWarpsPerCta, 0, s,
+    launch(k_bwd_small<float>, (cnt + kWarpsPerCta - 1) / kWarpsPerCta, 32 * kWarpsPerCta, 0, s,
            level + S.level_ptr[t], cnt, sfirst, srowptr, srows, slofs, panel, xd);
   }
   MPIR_CHECK_LAUNCH();

@@ -2,9 +2,19 @@
 // solves (solve.cu, solve_multi.cu): asynchronous copies into shared memory
 // and the ready-value hand-over of block results between CTAs.
 #pragma once
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
 #include <cstdint>
 
 namespace mpir {
+
+// Factor values are read as float32, or from the 16-bit copy of the panels
+// that the bfloat16 / float16 tiers keep for the solves; arithmetic is in
+// float64 either way.
+__device__ __forceinline__ float to_f(float v) { return v; }
+__device__ __forceinline__ float to_f(__nv_bfloat16 v) { return __bfloat162float(v); }
+__device__ __forceinline__ float to_f(__half v) { return __half2float(v); }
 
 __device__ __forceinline__ void cp_async8(double *dst, const double *src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(

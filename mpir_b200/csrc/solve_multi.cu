@@ -27,6 +27,7 @@
 // with NR single solves to rounding.
 #include <atomic>
 #include <algorithm>
+#include <type_traits>
 
 #include "common.cuh"
 #include "engine.hpp"
@@ -107,12 +108,12 @@ __global__ void k_dscale_m(int64_t n, int nr, const float *Dinv, double *X) {
 // ---------------------------------------------------------------------------
 // Fronts solved by one warp (w <= 32, h <= 256), forward.  z[k][i] is front
 // row i of vector k; per vector exactly the operations of k_fwd_small.
-template <int NR>
+template <int NR, class T>
 __global__ void __launch_bounds__(32 * kSmallWarpsM)
     k_fwd_small_m(const int32_t *list, int count, const int64_t *sfirst,
                   const int64_t *srowptr, const int64_t *slofs, const int64_t *child_ptr,
                   const int32_t *child_list, const int32_t *srel, const int64_t *zofs,
-                  const float *panel, double *x, int64_t n, double *zbuf, int64_t zld) {
+                  const T *panel, double *x, int64_t n, double *zbuf, int64_t zld) {
   extern __shared__ __align__(16) double zsm[];  // [warps][NR][kWarpSolveH]
   constexpr int H    = kWarpSolveH;
   const int     warp = threadIdx.x / 32, lane = threadIdx.x % 32;
@@ -136,7 +137,7 @@ __global__ void __launch_bounds__(32 * kSmallWarpsM)
       for (int a = lane; a < rc; a += 32) z[k * H + rl[a]] += zbuf[k * zld + zc + a];
     __syncwarp();
   }
-  const float  *P  = panel + slofs[J];
+  const T      *P  = panel + slofs[J];
   constexpr int RT = H / 32;
   float         cur[4][RT], nxt[4][RT];
   auto          load4 = [&](float (*buf)[RT], int k0) {
@@ -145,7 +146,7 @@ __global__ void __launch_bounds__(32 * kSmallWarpsM)
 #pragma unroll
       for (int t = 0; t < RT; t++) {
         const int k = k0 + u, i = lane + 32 * t;
-        buf[u][t]   = (k < w && i > k && i < h) ? P[i + (int64_t)k * h] : 0.0f;
+        buf[u][t]   = (k < w && i > k && i < h) ? to_f(P[i + (int64_t)k * h]) : 0.0f;
       }
   };
   load4(cur, 0);
@@ -181,11 +182,11 @@ __global__ void __launch_bounds__(32 * kSmallWarpsM)
 
 // Backward counterpart of k_fwd_small_m (per vector the operations of
 // k_bwd_small).
-template <int NR>
+template <int NR, class T>
 __global__ void __launch_bounds__(32 * kSmallWarpsM)
     k_bwd_small_m(const int32_t *list, int count, const int64_t *sfirst,
                   const int64_t *srowptr, const int32_t *srows, const int64_t *slofs,
-                  const float *panel, double *x, int64_t n) {
+                  const T *panel, double *x, int64_t n) {
   extern __shared__ __align__(16) double zsm[];
   constexpr int H    = kWarpSolveH;
   const int     warp = threadIdx.x / 32, lane = threadIdx.x % 32;
@@ -200,7 +201,7 @@ __global__ void __launch_bounds__(32 * kSmallWarpsM)
   for (int k = 0; k < NR; k++)
     for (int i = lane; i < h; i += 32) z[k * H + i] = x[k * n + (i < w ? f + i : rw[i])];
   __syncwarp();
-  const float  *P  = panel + slofs[J];
+  const T      *P  = panel + slofs[J];
   constexpr int RT = H / 32;
   float         cur[4][RT], nxt[4][RT];
   auto          load4 = [&](float (*buf)[RT], int k0) {
@@ -209,7 +210,7 @@ __global__ void __launch_bounds__(32 * kSmallWarpsM)
 #pragma unroll
       for (int t = 0; t < RT; t++) {
         const int k = k0 - u, i = lane + 32 * t;
-        buf[u][t]   = (k >= 0 && i > k && i < h) ? P[i + (int64_t)k * h] : 0.0f;
+        buf[u][t]   = (k >= 0 && i > k && i < h) ? to_f(P[i + (int64_t)k * h]) : 0.0f;
       }
   };
   load4(cur, w - 1);
@@ -253,9 +254,9 @@ constexpr int fwd_m_smem_doubles() {
   return kTriM + 2 * NR * kNB + NR * 512;
 }
 
-template <int NR>
+template <int NR, class T>
 __global__ void __launch_bounds__(kSolveThreads, 1)
-    k_fwd_fronts_m(const SolveItem *items, const float *panel, const double *linv64t,
+    k_fwd_fronts_m(const SolveItem *items, const T *panel, const double *linv64t,
                    const int64_t *gp, const int64_t *gsrc, double *x, double *zbuf,
                    int64_t zld, int32_t *tickets, double *ready, int32_t *err) {
   extern __shared__ __align__(16) double sm[];
@@ -286,7 +287,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   const int64_t     h = F.h, n = F.n;
   const int         w = F.w;
   const int64_t     r = static_cast<int64_t>(R) * kNB + rr;
-  const float      *P = panel + F.panel;
+  const T          *P = panel + F.panel;
   if (R < F.nb) stage_tri_m(linv64t + F.linv + static_cast<int64_t>(R) * kNB * kNB, tri,
                             min(kNB, w - R * kNB));
   // Right-hand side rows: x (rows < w) plus the children's update vectors in
@@ -313,7 +314,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
     const int c0 = b * kNB + qq * 32;
 #pragma unroll
     for (int k = 0; k < 32; k++)
-      lv[k] = (r < h && c0 + k < w) ? __ldg(P + r + static_cast<int64_t>(c0 + k) * h) : 0.0f;
+      lv[k] = (r < h && c0 + k < w) ? to_f(__ldg(P + r + static_cast<int64_t>(c0 + k) * h)) : 0.0f;
     wait_many<NR>(yr + c0 + lane, n, c0 + lane < w, yw + lane, 32, err, polls);
     __syncwarp();
 #pragma unroll
@@ -371,7 +372,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
 #pragma unroll
         for (int t = 0; t < KG; t++) a[t] = 0.0;
         for (int k2 = 0; k2 < nbk; k2++) {
-          const double l = static_cast<double>(P[r + static_cast<int64_t>(R * kNB + k2) * h]);
+          const double l = static_cast<double>(to_f(P[r + static_cast<int64_t>(R * kNB + k2) * h]));
 #pragma unroll
           for (int t = 0; t < KG; t++) {
             const int k = qq + 4 * t;
@@ -394,9 +395,9 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
 // Backward, off-diagonal rows: CTA c takes rows w + 128 c .. of one front and
 // writes t_col = sum_r L_{r,col} x_r of every column for all NR vectors (warp
 // per column, rows over the lanes; per vector the sums of k_bwd_chunks).
-template <int NR>
+template <int NR, class T>
 __global__ void __launch_bounds__(kSolveThreads)
-    k_bwd_chunks_m(const SolveFront *fr, const int32_t *fmap, const float *panel,
+    k_bwd_chunks_m(const SolveFront *fr, const int32_t *fmap, const T *panel,
                    const int32_t *srows, const double *x, double *part, int64_t pld) {
   __shared__ double zr[NR][kNB];
   const SolveFront  F = fr[fmap[blockIdx.x]];
@@ -410,15 +411,15 @@ __global__ void __launch_bounds__(kSolveThreads)
     zr[k][i] = i < nr ? x[k * n + srows[F.rows + r0 + i]] : 0.0;
   }
   __syncthreads();
-  const float  *P  = panel + F.panel + r0;
+  const T      *P  = panel + F.panel + r0;
   constexpr int kWarps = kSolveThreads / 32;
   for (int64_t col = warp; col < w; col += kWarps) {
-    const float *cp = P + col * h;
+    const T     *cp = P + col * h;
     double       l[4];
 #pragma unroll
     for (int i = 0; i < 4; i++) {
       const int rr = lane + 32 * i;
-      l[i]         = rr < nr ? static_cast<double>(__ldg(cp + rr)) : 0.0;
+      l[i]         = rr < nr ? static_cast<double>(to_f(__ldg(cp + rr))) : 0.0;
     }
 #pragma unroll
     for (int k = 0; k < NR; k++) {
@@ -444,9 +445,9 @@ constexpr int bwd_m_smem_doubles() {
   return kTriM + (kNB * kLsPitch + 1) / 2 + 2 * NR * kNB;
 }
 
-template <int NR>
+template <int NR, class T>
 __global__ void __launch_bounds__(kSolveThreads, 1)
-    k_bwd_fronts_m(const SolveItem *items, const float *panel, const double *linv64t,
+    k_bwd_fronts_m(const SolveItem *items, const T *panel, const double *linv64t,
                    double *x, const double *part, int64_t pld, int32_t *tickets,
                    double *ready, int32_t *err) {
   constexpr int KG = NR / 4;
@@ -487,7 +488,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
         s += part[k * pld + F.part + static_cast<int64_t>(ch) * w + b * kNB + c];
     acc[t] = s;
   }
-  const float *P    = panel + F.panel;
+  const T     *P    = panel + F.panel;
   const int    copy = (item * 16 + g) % kMultiCopies;
   // Tile R: thread (rr, cg) = (tid % 128, tid / 128) loads row rr, columns
   // 32 cg .. 32 cg + 31 of the block.
@@ -499,8 +500,9 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
 #pragma unroll
     for (int k = 0; k < 32; k++) {
       const int cc = tcg * 32 + k;
-      lr[k] = (trr < rows && cc < nbk) ? __ldg(P + rb + trr + static_cast<int64_t>(b * kNB + cc) * h)
-                                       : 0.0f;
+      lr[k] = (trr < rows && cc < nbk)
+                  ? to_f(__ldg(P + rb + trr + static_cast<int64_t>(b * kNB + cc) * h))
+                  : 0.0f;
     }
   };
   if (F.nb - 1 > b) load_tile(F.nb - 1);
@@ -544,30 +546,29 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   }
 }
 
-template <int NR>
+template <int NR, class T>
 void set_smem_attrs() {
   static std::atomic<bool> done{false};  // idempotent; set once per process
   if (done) return;
-  MPIR_CUDA(cudaFuncSetAttribute(k_fwd_fronts_m<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  MPIR_CUDA(cudaFuncSetAttribute(k_fwd_fronts_m<NR, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(fwd_m_smem_doubles<NR>() * sizeof(double))));
-  MPIR_CUDA(cudaFuncSetAttribute(k_bwd_fronts_m<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  MPIR_CUDA(cudaFuncSetAttribute(k_bwd_fronts_m<NR, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(bwd_m_smem_doubles<NR>() * sizeof(double))));
   const int small = static_cast<int>(kSmallWarpsM * NR * kWarpSolveH * sizeof(double));
-  MPIR_CUDA(cudaFuncSetAttribute(k_fwd_small_m<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  MPIR_CUDA(cudaFuncSetAttribute(k_fwd_small_m<NR, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  small));
-  MPIR_CUDA(cudaFuncSetAttribute(k_bwd_small_m<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  MPIR_CUDA(cudaFuncSetAttribute(k_bwd_small_m<NR, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  small));
   done = true;
 }
 
-template <int NR>
-void solve_multi_nr(const Plan &P, const Numeric &F, double *X, MultiSolveWorkspace &ws,
-                    cudaStream_t s, int phases) {
+template <int NR, class T>
+void solve_multi_nr(const Plan &P, const Numeric &F, const T *pan, double *X,
+                    MultiSolveWorkspace &ws, cudaStream_t s, int phases) {
   const Symbolic &S  = P.S;
   KernelTimer    &kt = kernel_timer();
-  set_smem_attrs<NR>();
+  set_smem_attrs<NR, T>();
   const int64_t     n     = S.n;
-  const float      *pan   = F.panel.as<float>();
   const double     *lvt   = F.linv64t.as<double>();
   double           *zbuf  = ws.zbuf.as<double>();
   const int64_t     zld   = std::max<int64_t>(S.z_elems, 1);
@@ -587,13 +588,13 @@ void solve_multi_nr(const Plan &P, const Numeric &F, double *X, MultiSolveWorksp
   for (int t = 0; t < nl && (phases & kForward); t++) {
     const LevelPlan &L = P.levels[t];
     if (L.sw_count > 0)
-      launch(k_fwd_small_m<NR>, (L.sw_count + kSmallWarpsM - 1) / kSmallWarpsM, 32 * kSmallWarpsM,
+      launch(k_fwd_small_m<NR, T>, (L.sw_count + kSmallWarpsM - 1) / kSmallWarpsM, 32 * kSmallWarpsM,
              small_smem, s, P.swarp_list.as<int32_t>() + L.sw_begin, L.sw_count,
              P.sfirst.as<int64_t>(), P.srowptr.as<int64_t>(), P.slofs.as<int64_t>(),
              P.child_ptr.as<int64_t>(), P.child_list.as<int32_t>(), P.srel.as<int32_t>(),
              P.zofs.as<int64_t>(), pan, X, n, zbuf, zld);
     if (L.sf_count > 0)
-      launch(k_fwd_fronts_m<NR>, L.fwd_items, kSolveThreads,
+      launch(k_fwd_fronts_m<NR, T>, L.fwd_items, kSolveThreads,
              fwd_m_smem_doubles<NR>() * sizeof(double), s,
              P.fwd_item.as<SolveItem>() + L.fwd_map0, pan, lvt, P.gp.as<int64_t>(),
              P.gsrc.as<int64_t>(), X, zbuf, zld, sync + 2 * t, ready, err);
@@ -609,16 +610,16 @@ void solve_multi_nr(const Plan &P, const Numeric &F, double *X, MultiSolveWorksp
   for (int t = nl - 1; t >= 0; t--) {
     const LevelPlan &L = P.levels[t];
     if (L.sw_count > 0)
-      launch(k_bwd_small_m<NR>, (L.sw_count + kSmallWarpsM - 1) / kSmallWarpsM, 32 * kSmallWarpsM,
+      launch(k_bwd_small_m<NR, T>, (L.sw_count + kSmallWarpsM - 1) / kSmallWarpsM, 32 * kSmallWarpsM,
              small_smem, s, P.swarp_list.as<int32_t>() + L.sw_begin, L.sw_count,
              P.sfirst.as<int64_t>(), P.srowptr.as<int64_t>(), P.srows.as<int32_t>(),
              P.slofs.as<int64_t>(), pan, X, n);
     if (L.sf_count > 0) {
       if (L.bwd_chunk_items > 0)
-        launch(k_bwd_chunks_m<NR>, L.bwd_chunk_items, kSolveThreads, 0, s, sf + L.sf_begin,
+        launch(k_bwd_chunks_m<NR, T>, L.bwd_chunk_items, kSolveThreads, 0, s, sf + L.sf_begin,
                P.chunk_map.as<int32_t>() + L.chunk_map0, pan, P.srows.as<int32_t>(),
                static_cast<const double *>(X), ws.part.as<double>(), pld);
-      launch(k_bwd_fronts_m<NR>, L.bwd_owner_items, kSolveThreads,
+      launch(k_bwd_fronts_m<NR, T>, L.bwd_owner_items, kSolveThreads,
              bwd_m_smem_doubles<NR>() * sizeof(double), s,
              P.own_item.as<SolveItem>() + L.own_map0, pan, lvt, X,
              static_cast<const double *>(ws.part.as<double>()), pld, sync + 2 * t + 1, ready,
@@ -661,11 +662,18 @@ void ldlt_solve_multi(const Plan &P, const Numeric &F, double *X, int width,
                       MultiSolveWorkspace &ws, cudaStream_t s, int phases) {
   if (P.S.n == 0) return;
   if (ws.nr != width) throw std::logic_error("multi-vector workspace of another width");
-  switch (width) {
-    case 4: solve_multi_nr<4>(P, F, X, ws, s, phases); break;
-    case 8: solve_multi_nr<8>(P, F, X, ws, s, phases); break;
-    case 16: solve_multi_nr<16>(P, F, X, ws, s, phases); break;
-    default: throw std::invalid_argument("multi-vector solve width must be 4, 8 or 16");
+  if (width != 4 && width != 8 && width != 16)
+    throw std::invalid_argument("multi-vector solve width must be 4, 8 or 16");
+  auto run = [&](auto *pan) {
+    using T = std::remove_const_t<std::remove_pointer_t<decltype(pan)>>;
+    if (width == 4) solve_multi_nr<4, T>(P, F, pan, X, ws, s, phases);
+    if (width == 8) solve_multi_nr<8, T>(P, F, pan, X, ws, s, phases);
+    if (width == 16) solve_multi_nr<16, T>(P, F, pan, X, ws, s, phases);
+  };
+  switch (F.solve_prec()) {
+    case 2: run(F.panel16.as<const __nv_bfloat16>()); break;
+    case 3: run(F.panel16.as<const __half>()); break;
+    default: run(F.panel.as<const float>());
   }
 }
 

@@ -70,7 +70,7 @@ class Solver {
   // Device memory this solver holds beyond its plan, and what adopt() plus
   // one batch of `width` right-hand sides would take for plan P.
   size_t device_bytes() const;
-  static size_t bytes_for(const Plan &P, int64_t gmres_iter, int width);
+  static size_t bytes_for(const Plan &P, int64_t gmres_iter, int width, int uf = kF32);
   int factor(const double *Ax);
   int solve(const double *b, double *x, Report *rep);
   // Device entry points (caller arrays already on this device).

@@ -320,6 +320,17 @@ def test_low_precision_factor_tier_converges(uf):
         x = solver.Solve(s.b)
         be = kkt.backward_error(s.n, s.Ap, s.Ai, s.Ax, x, s.b)
         assert be <= 1e-14, (uf, be, solver.last_report)
+        # L is stored and applied in the tier's type
+        assert solver.last_report["factor_prec"] == mp._PREC[uf]
+        # lockstep solves read the same 16-bit L through the several-vector
+        # kernels
+        X = solver.SolveBatch(np.stack([s.b, 2 * s.b, -s.b]))
+        for k, scale in enumerate((1, 2, -1)):
+            assert kkt.backward_error(s.n, s.Ap, s.Ai, s.Ax, X[k], scale * s.b) <= 1e-14
+        Y = np.random.default_rng(2).standard_normal((4, s.n))
+        Z = solver.apply_factor(Y)
+        for k in range(4):
+            assert rel_norm_diff(Z[k], solver.apply_factor(Y[k:k + 1])[0]) <= 1e-12
 
 
 @pytest.mark.parametrize("name,s", list(small_systems())[:3])
