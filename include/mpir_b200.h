@@ -304,6 +304,31 @@ int mpir_analyze_host(int64_t n, const int64_t *Ap, const int64_t *Ai,
                       int64_t *etree, int64_t *Lnz, int64_t *Cp, int64_t *Ci,
                       int64_t *Lp, int64_t *Li, mpir_info *info);
 
+/* ---- Factor groups ------------------------------------------------------- */
+/* k value sets on the pattern a solver has analysed, refactorized by one CUDA
+ * graph launch: the reference factors one matrix per QDLDL_factor /
+ * GmresLDLIR::Compute call (qdldl.hpp:172-345, gmres_ir.hpp:323); a group
+ * records every member's factorization once, joins them as parallel branches
+ * of one graph and replays it for every new set of values (same-pattern
+ * instances such as interior-point iterations).  Members take the solver's
+ * precisions and settings at creation and share its analysis; each has its
+ * own factor storage. */
+typedef struct mpir_group_s *mpir_group;
+
+int mpir_group_create(mpir_group *out, mpir_solver s, int k);
+/* Ax: k value sets of the analysed pattern (k x nnz_upper, row i for member
+ * i, host, caller order).  npos: NULL or k entries receiving each factor's
+ * positive pivots (-1 on a zero pivot).  Returns 0, or the first member's
+ * failure (-1 zero pivot, -5 timeout). */
+int mpir_group_factor(mpir_group g, const double *Ax, int64_t *npos);
+/* GMRES-IR with member `member`'s factor: one right-hand side, or 1 .. 16 in
+ * lockstep (as mpir_solver_solve / mpir_solver_solve_batch). */
+int mpir_group_solve(mpir_group g, int member, const double *b, double *x,
+                     mpir_report *rep);
+int mpir_group_solve_batch(mpir_group g, int member, int nrhs, const double *B,
+                           double *X, mpir_report *reps);
+int mpir_group_destroy(mpir_group g);
+
 /* ---- Serving engine ------------------------------------------------------ */
 /* A request stream of GMRES-IR solves (each one the reference's
  * GmresLDLIR::Compute + Solve, gmres_ir.hpp:323 and :534-634) served on one

@@ -145,6 +145,11 @@ def lib():
         "mpir_solver_export_factor_leading": (i32, [vp, i64, vp, vp, vp, vp, vp]),
         "mpir_solver_supernodes": (i32, [vp, vp, vp, vp, vp]),
         "mpir_analyze_host": (i32, [i64, vp, vp, vp, i32, vp, vp, vp, vp, vp, vp, vp, vp]),
+        "mpir_group_create": (i32, [vp, vp, i32]),
+        "mpir_group_factor": (i32, [vp, vp, vp]),
+        "mpir_group_solve": (i32, [vp, i32, vp, vp, vp]),
+        "mpir_group_solve_batch": (i32, [vp, i32, i32, vp, vp, vp]),
+        "mpir_group_destroy": (i32, [vp]),
         "mpir_server_create": (i32, [vp, vp]),
         "mpir_server_submit": (i32, [vp, vp, vp]),
         "mpir_server_wait": (i32, [vp, i64, vp]),
@@ -482,6 +487,55 @@ class GmresLDLIR:
         Dinv = np.zeros(max(n, 1), np.float32)
         _check(lib().mpir_solver_export_factor(self._h, _p(Lp), _p(Li), _p(Lx), _p(D), _p(Dinv)))
         return Lp, Li[:nl], Lx[:nl], D[:n], Dinv[:n]
+
+
+class FactorGroup:
+    """k value sets on the pattern a GmresLDLIR has analysed, refactorized by
+    one CUDA graph launch (mpir_group_* in include/mpir_b200.h); each member
+    is then solved like a solver of its own."""
+
+    def __init__(self, solver, k):
+        self.k = int(k)
+        self.n = solver.n
+        self._h = C.c_void_p()
+        _check(lib().mpir_group_create(C.byref(self._h), solver._h, self.k))
+
+    def factor(self, Axs):
+        """Axs: k value arrays (rows).  Returns the positive-pivot counts."""
+        A = np.ascontiguousarray(np.stack([_f64(a) for a in Axs]))
+        npos = np.zeros(self.k, np.int64)
+        r = lib().mpir_group_factor(self._h, _p(A), _p(npos))
+        if r < -1:
+            raise MpirError(int(r), last_error())
+        self.last_status = int(r)
+        return npos
+
+    def Solve(self, member, b):
+        b = _f64(b)
+        x = np.zeros(self.n, np.float64)
+        rep = Report()
+        _check(lib().mpir_group_solve(self._h, int(member), _p(b), _p(x), C.byref(rep)))
+        self.last_report = rep.as_dict()
+        return x
+
+    def SolveBatch(self, member, B):
+        B = np.ascontiguousarray(B, dtype=np.float64)
+        X = np.zeros_like(B)
+        reps = (Report * B.shape[0])()
+        _check(lib().mpir_group_solve_batch(self._h, int(member), B.shape[0], _p(B), _p(X), reps))
+        self.last_reports = [reps[k].as_dict() for k in range(B.shape[0])]
+        return X
+
+    def close(self):
+        if self._h:
+            lib().mpir_group_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Server:

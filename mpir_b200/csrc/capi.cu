@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "../../include/mpir_b200.h"
+#include "group.hpp"
 #include "server.hpp"
 #include "solver.hpp"
 
@@ -875,6 +876,71 @@ int mpir_analyze_host(int64_t n, const int64_t *Ap, const int64_t *Ai, const dou
       for (int64_t j = 0; j < S.n; j++) fl += static_cast<double>(S.Lnz[j]) * S.Lnz[j];
       info->factor_flops = fl;
       info->solve_bytes  = 2.0 * 4.0 * S.nnzL + 4.0 * S.n + 4.0 * 8.0 * S.n;
+    }
+    return MPIR_OK;
+  });
+}
+
+struct mpir_group_s {
+  FactorGroup *impl;
+};
+
+int mpir_group_create(mpir_group *out, mpir_solver s, int k) {
+  MPIR_NEED(s);
+  return guard([&]() -> int {
+    if (!out || k < 1) throw StatusError(MPIR_ERR_ARGUMENT, "NULL output or k < 1");
+    *out = nullptr;
+    auto *g = new mpir_group_s{nullptr};
+    try {
+      g->impl = new FactorGroup(*s->impl, k);
+    } catch (...) {
+      delete g;
+      throw;
+    }
+    *out = g;
+    return MPIR_OK;
+  });
+}
+
+int mpir_group_factor(mpir_group g, const double *Ax, int64_t *npos) {
+  return guard([&]() -> int {
+    if (!g || !g->impl || !Ax) throw StatusError(MPIR_ERR_ARGUMENT, "NULL argument");
+    const int64_t nnz = g->impl->member(0).plan().S.nnz;
+    const int     rc  = g->impl->factor(Ax, nnz, npos);
+    if (rc == kBadInput) g_err = "zero pivot in a member of the group";
+    if (rc == MPIR_ERR_TIMEOUT) g_err = "a bounded device wait ran out";
+    return rc;
+  });
+}
+
+int mpir_group_solve(mpir_group g, int member, const double *b, double *x, mpir_report *rep) {
+  return guard([&]() -> int {
+    if (!g || !g->impl || !b || !x) throw StatusError(MPIR_ERR_ARGUMENT, "NULL argument");
+    if (member < 0 || member >= g->impl->size())
+      throw StatusError(MPIR_ERR_ARGUMENT, "member out of range");
+    return g->impl->member(member).solve(b, x, reinterpret_cast<Report *>(rep));
+  });
+}
+
+int mpir_group_solve_batch(mpir_group g, int member, int nrhs, const double *B, double *X,
+                           mpir_report *reps) {
+  return guard([&]() -> int {
+    if (!g || !g->impl || !B || !X) throw StatusError(MPIR_ERR_ARGUMENT, "NULL argument");
+    if (member < 0 || member >= g->impl->size())
+      throw StatusError(MPIR_ERR_ARGUMENT, "member out of range");
+    if (nrhs < 1 || nrhs > Solver::kMaxBatch)
+      throw StatusError(MPIR_ERR_ARGUMENT, "1 <= nrhs <= 16 right-hand sides");
+    Solver &m = g->impl->member(member);
+    return nrhs == 1 ? m.solve(B, X, reinterpret_cast<Report *>(reps))
+                     : m.solve_batch(nrhs, B, X, reinterpret_cast<Report *>(reps));
+  });
+}
+
+int mpir_group_destroy(mpir_group g) {
+  return guard([&]() -> int {
+    if (g) {
+      delete g->impl;
+      delete g;
     }
     return MPIR_OK;
   });

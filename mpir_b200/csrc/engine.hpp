@@ -188,6 +188,11 @@ class Numeric {
   void run_graph(const Plan &P, const double *d_Ax, double eps_uf, cudaStream_t s,
                  cudaStream_t capture_stream);
   void release_graph();
+  // Records the whole factorization of d_Ax on capture_stream as a graph
+  // (not run, not instantiated; the caller owns it); *launches receives the
+  // kernel launches it holds.
+  cudaGraph_t record(const Plan &P, const double *d_Ax, double eps, cudaStream_t capture_stream,
+                     int64_t *launches);
   ~Numeric() { release_graph(); }
   // Reads the status; returns #positive D, -1 on a zero pivot or -5 when a
   // bounded device wait ran out.

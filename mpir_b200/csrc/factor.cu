@@ -1394,6 +1394,25 @@ void Numeric::release_graph() {
   graph = nullptr;
 }
 
+cudaGraph_t Numeric::record(const Plan &P, const double *d_Ax, double eps,
+                            cudaStream_t capture_stream, int64_t *launches) {
+  cudaGraph_t g = nullptr;
+  MPIR_CUDA(cudaStreamSynchronize(capture_stream));
+  MPIR_CUDA(cudaStreamBeginCapture(capture_stream, cudaStreamCaptureModeThreadLocal));
+  LaunchCapture cap;
+  try {
+    run(P, d_Ax, eps, capture_stream);
+  } catch (...) {
+    cudaStreamEndCapture(capture_stream, &g);
+    if (g) cudaGraphDestroy(g);
+    throw;
+  }
+  MPIR_CUDA(cudaStreamEndCapture(capture_stream, &g));
+  valid = false;  // recorded, not run
+  if (launches) *launches = cap.count();
+  return g;
+}
+
 void Numeric::run_graph(const Plan &P, const double *d_Ax, double eps, cudaStream_t s,
                         cudaStream_t capture_stream) {
   if (kernel_timer().enabled || P.S.n == 0) {  // per-class timing needs the plain launches
@@ -1402,19 +1421,7 @@ void Numeric::run_graph(const Plan &P, const double *d_Ax, double eps, cudaStrea
   }
   if (!graph || graph_ax != d_Ax || graph_eps != eps || graph_mode != update_mode) {
     release_graph();
-    cudaGraph_t g = nullptr;
-    MPIR_CUDA(cudaStreamSynchronize(capture_stream));
-    MPIR_CUDA(cudaStreamBeginCapture(capture_stream, cudaStreamCaptureModeThreadLocal));
-    LaunchCapture cap;
-    try {
-      run(P, d_Ax, eps, capture_stream);
-    } catch (...) {
-      cudaStreamEndCapture(capture_stream, &g);
-      if (g) cudaGraphDestroy(g);
-      throw;
-    }
-    MPIR_CUDA(cudaStreamEndCapture(capture_stream, &g));
-    graph_launches = cap.count();
+    cudaGraph_t g = record(P, d_Ax, eps, capture_stream, &graph_launches);
     const cudaError_t e = cudaGraphInstantiate(&graph, g, 0);
     cudaGraphDestroy(g);
     MPIR_CUDA(e);

@@ -182,6 +182,29 @@ int Solver::factor(const double *Ax) {
   return factor_device(num_.Ax.as<double>());
 }
 
+double *Solver::values_device() {
+  if (!plan_) throw std::logic_error("no analysed pattern");
+  num_.ensure_scratch(*plan_);
+  return num_.Ax.as<double>();
+}
+
+cudaGraph_t Solver::record_factor(int64_t *launches) {
+  if (!plan_) throw std::logic_error("factor before analyze");
+  MPIR_CUDA(cudaSetDevice(device));
+  num_.ensure_scratch(*plan_);
+  num_.release_graph();
+  return num_.record(*plan_, num_.Ax.as<double>(), eps_of(uf), own_stream_, launches);
+}
+
+int Solver::finish_recorded_factor(double ms) {
+  num_.eps_uf    = eps_of(uf);
+  last_npos      = num_.result(stream_);
+  last_factor_ms = ms;
+  num_.valid     = last_npos >= 0;
+  if (last_npos < 0) return last_npos == -5 ? -5 : kBadInput;
+  return kOk;
+}
+
 void Solver::set_wait_controls(int poll_log2, int withhold_item) {
   if (!plan_) throw std::logic_error("no analysed pattern");
   MPIR_CUDA(cudaSetDevice(device));

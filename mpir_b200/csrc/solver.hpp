@@ -113,6 +113,12 @@ class Solver {
   // Release the factorization-only buffers of the current factor (see
   // Numeric::trim); the next factor() allocates them again.
   void trim() { num_.trim(); }
+  // Factor groups (group.cu): the factorization of the values in this
+  // solver's own value buffer recorded as a graph (scratch allocated first),
+  // and the status check after a launch that ran it.
+  cudaGraph_t record_factor(int64_t *launches);
+  double     *values_device();
+  int         finish_recorded_factor(double ms);
   double last_factor_ms = 0;
   int64_t last_npos     = 0;
 

@@ -108,3 +108,29 @@ def test_solve_batch_argument_errors():
         solver.SolveBatch(np.zeros((17, s.n)))
     assert solver.SolveBatch(np.zeros((2, s.n - 1))).size == 0
     solver.close()
+
+
+def test_factor_group_one_launch_matches_solo_factors():
+    """Same-pattern instances refactorized together by one graph launch give
+    the factors (and so the solutions) each gets alone."""
+    insts = kkt.batch2d(instances=3, grid=24, nrhs=4, seed=7)
+    base = mp.GmresLDLIR()
+    base.analyze(insts[0].Ap, insts[0].Ai, insts[0].Ax)
+    grp = mp.FactorGroup(base, len(insts))
+    for rounds in range(2):  # the recorded launch is replayed for new values
+        if rounds:
+            insts = insts[::-1]
+        npos = grp.factor([s.Ax for s in insts])
+        assert grp.last_status == 0 and np.all(npos > 0)
+        for i, s in enumerate(insts):
+            X = grp.SolveBatch(i, s.b)
+            solo = mp.GmresLDLIR()
+            solo.Compute(s.Ap, s.Ai, s.Ax)
+            for k in range(s.b.shape[0]):
+                assert kkt.backward_error(s.n, s.Ap, s.Ai, s.Ax, X[k], s.b[k]) <= 1e-14
+                x1 = grp.Solve(i, s.b[k])
+                xs = solo.Solve(s.b[k])
+                assert np.max(np.abs(x1 - xs)) / np.max(np.abs(xs)) <= 1e-13
+            solo.close()
+    grp.close()
+    base.close()
