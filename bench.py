@@ -80,6 +80,7 @@ def parse():
     ap.add_argument("--budget-gb", type=float, default=150.0)
     ap.add_argument("--no-latency-pass", action="store_true")
     ap.add_argument("--no-dropin", action="store_true")
+    ap.add_argument("--group", type=int, default=8, help="batch2d: instances per graph launch")
     return ap.parse_args()
 
 
@@ -920,10 +921,13 @@ def run_stream(args):
 
 
 def run_batch2d(args):
-    """Config 4: 64 same-pattern instances, 16 right-hand sides each; per
-    step one instance refactorized and its 16 right-hand sides solved in
-    lockstep (one several-vector triangular solve per preconditioner
-    application)."""
+    """Config 4: same-pattern instances, 16 right-hand sides each.  One step
+    = one group of --group instances: their refactorizations in one graph
+    launch (mpir_group_factor), then each instance's 16 right-hand sides
+    solved in lockstep (one several-vector triangular solve per
+    preconditioner application).  --steps 8 with groups of 8 covers the 64
+    instances; the drop-in comparison (one factor + 16 one-at-a-time solves
+    per instance, through GmresLDLIR) runs on the first group."""
     import torch
 
     import mpir_b200 as mp
@@ -931,15 +935,27 @@ def run_batch2d(args):
     rank, world, local = dist_env()
     pg, dev = init_dist(local)
     uf = args.uf or "f32"
-    insts = kkt.batch2d(instances=max(args.steps, 1), grid=args.grid or 256, nrhs=16,
+    G = args.group
+    ninst = G * max(args.steps, 1)
+    insts = kkt.batch2d(instances=ninst, grid=args.grid or 256, nrhs=16,
                         seed=replica_seed(args.seed, rank))
     solver = mp.GmresLDLIR(uf=uf, device=local)
     solver.analyze(insts[0].Ap, insts[0].Ai, insts[0].Ax)
     info = solver.info()
+    grp = mp.FactorGroup(solver, G)
+
+    def step(i):
+        group = insts[(i * G) % ninst:(i * G) % ninst + G]
+        assert np.all(grp.factor([s.Ax for s in group]) > 0)
+        be, solves = 0.0, 0
+        for j, s in enumerate(group):
+            X = grp.SolveBatch(j, s.b)
+            solves += X.shape[0]
+            be = max(be, max(r["backward_error"] for r in grp.last_reports))
+        return be, solves
+
     for i in range(args.warmup):
-        s = insts[i % len(insts)]
-        solver.factor(s.Ax)
-        solver.SolveBatch(s.b)
+        step(i)
     torch.cuda.synchronize()
     if pg is not None:
         pg.barrier()
@@ -949,38 +965,50 @@ def run_batch2d(args):
     t0 = time.perf_counter()
     be, lat, solves = 0.0, [], 0
     for i in range(args.steps):
-        s = insts[i % len(insts)]
         t1 = time.perf_counter()
-        assert solver.factor(s.Ax) == 0
-        X = solver.SolveBatch(s.b)
+        b_i, s_i = step(i)
         lat.append(1e3 * (time.perf_counter() - t1))
-        solves += X.shape[0]
-        be = max(be, max(r["backward_error"] for r in solver.last_reports))
+        be, solves = max(be, b_i), solves + s_i
     seconds = rank_max(pg, time.perf_counter() - t0, dev)
     launches = mp.launch_count() - launches0
     clk = clocks.stop()
     value = rank_sum(pg, solves, dev) / seconds
+    fe = None
+    # the same first group one at a time through the drop-in: a factor and
+    # 16 single-right-hand-side solves per instance
+    t1 = time.perf_counter()
+    for s in insts[:G]:
+        assert solver.factor(s.Ax) == 0
+        for k in range(s.b.shape[0]):
+            x = solver.Solve(s.b[k])
+            fe = max(fe or 0.0, kkt.forward_error(x, s.x_true[k]))
+    drop = G * 16 / (time.perf_counter() - t1)
     n = insts[0].n
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * seconds / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": f"{uf} factor / f64 solve", "data": "synthetic (seeded same-pattern batch)",
-        "config": {"workload": f"batch2d: {len(insts)} instances of n={n} on one pattern "
+        "config": {"workload": f"batch2d: {ninst} instances of n={n} on one pattern "
                                "(L2D 256^2 + diag(s), s log-uniform [1e-6, 1e2], m=16384 x 4, "
-                               "delta 1e-8), 16 RHS each; per step one refactorization + 16 "
-                               "lockstep GMRES-IR solves (host arrays through the C ABI)",
-                   "global_batch": world * 16},
+                               f"delta 1e-8), 16 RHS each; per step {G} refactorizations in one "
+                               f"graph launch + {G} x 16 lockstep GMRES-IR solves (host arrays "
+                               "through the C ABI)",
+                   "global_batch": world * G * 16, "group": G},
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
-                       "note": "per instance (factor + 16 solves)"},
-        "backward_error_max": be,
-        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": insts[0].Ax.nbytes + 16 * n * 8,
-                "d2h_bytes_per_step": 16 * n * 8},
+                       "note": f"per step ({G} factors + {G * 16} solves)"},
+        "backward_error_max": be, "forward_error_max_dropin": fe,
+        "drop_in": {"solves_per_s": drop, "note": "first group: per instance one factor + 16 "
+                    "one-at-a-time GmresLDLIR solves"},
+        "e2e": {"value": value, "unit": UNIT,
+                "h2d_bytes_per_step": G * (insts[0].Ax.nbytes + 16 * n * 8),
+                "d2h_bytes_per_step": G * 16 * n * 8},
         "gpu_launches": launches, "clocks": clk,
         "info": {k: info[k] for k in ("n", "nnz_L", "supernodes", "levels", "max_front")},
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
+    grp.close()
     solver.close()
     if pg is not None:
         pg.destroy_process_group()
