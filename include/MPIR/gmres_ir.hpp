@@ -13,9 +13,14 @@
 //    reference's Compute has no error path); Solve returns an empty vector on
 //    a size mismatch, as the reference does (gmres_ir.hpp:639-642), and throws
 //    on a device error.
-//  * Provided precisions: UF = float, UW = double, UR = double or a
-//    double-double type (mpir::double_double, or the QD library's dd_real
-//    with MPIR_USE_QD).  Other combinations throw from Compute.
+//  * Provided precisions: UF = double, float, std::bfloat16_t or
+//    std::float16_t; UW = double; UR = double or a double-double type
+//    (mpir::double_double, or the QD library's dd_real with MPIR_USE_QD).
+//    UF = double (the reference example's instantiation) scales with
+//    eps(double) as the reference's Compute does and preconditions with the
+//    float32 factor (LastReport().factor_prec = MPIR_F32); the 16-bit types
+//    keep L in that type for the solves.  Other combinations throw from
+//    Compute.
 //  * LastReport() gives the iteration counts and the backward error.
 //  * DumpLogText() returns the solver log as JSON text (the schema of the
 //    reference's DumpLog, gmres_ir.hpp:305-313); with VERBOSE defined and
