@@ -89,8 +89,11 @@ void Solver::adopt(std::shared_ptr<Plan> P) {
   MPIR_CUDA(cudaSetDevice(device));
   const int64_t n = P->S.n;
   plan_ = std::move(P);
-  // The 16-bit tiers keep L in their type for the solves.
-  num_.store_prec = uf == kBF16 ? 2 : uf == kF16 ? 3 : 1;
+  // The bfloat16 tier keeps L in bfloat16 for the solves.  The float16 tier
+  // does not: float16's range (largest finite 65504) cannot hold the L of
+  // these scaled quasi-definite systems, whose entries reach 1/delta-sized
+  // values, while bfloat16 has float32's exponent range.
+  num_.store_prec = uf == kBF16 ? 2 : 1;
   num_.allocate(*plan_);
   num_.update_mode = update_mode_for(uf);
   ws_.allocate(*plan_);

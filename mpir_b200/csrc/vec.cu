@@ -52,12 +52,19 @@ __device__ __forceinline__ void atomic_max_abs(unsigned long long *slot, double 
   atomicMax(slot, static_cast<unsigned long long>(__double_as_longlong(fabs(v))));
 }
 
-// Max of |v| over the warp, then one atomic per warp.
+// Max of |v| over the warp, then one atomic per warp.  The maximum is taken
+// on the bit patterns of |v| (non-negative doubles order as their bits), so a
+// NaN (whose |v| pattern lies above infinity's) wins and is reported: fmax
+// would drop it and a non-finite residual would pass for a small one.
 __device__ __forceinline__ void warp_max_abs(unsigned long long *slot, double v,
                                              bool active) {
-  double a = active ? fabs(v) : 0.0;
-  for (int o = 16; o > 0; o >>= 1) a = fmax(a, __shfl_xor_sync(0xffffffffu, a, o));
-  if ((threadIdx.x & 31) == 0) atomic_max_abs(slot, a);
+  unsigned long long a =
+      active ? static_cast<unsigned long long>(__double_as_longlong(fabs(v))) : 0ull;
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long b = __shfl_xor_sync(0xffffffffu, a, o);
+    a                          = b > a ? b : a;
+  }
+  if ((threadIdx.x & 31) == 0) atomicMax(slot, a);
 }
 
 // ---------------------------------------------------------------------------

@@ -35,8 +35,10 @@ def _summary(records, t_total):
     return {"solves_per_s": len(ok) / t_total if t_total > 0 else float("nan"),
             "completed": len(ok), "failed": len(records) - len(ok), "seconds": t_total,
             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-            "backward_error_max": max((r["backward_error"] for r in ok), default=float("nan")),
-            "forward_error_max": max((r["forward_error"] for r in ok), default=float("nan"))}
+            "backward_error_max": max((r.get("backward_error", float("nan")) for r in ok),
+                                      default=float("nan")),
+            "forward_error_max": max((r.get("forward_error", float("nan")) for r in ok),
+                                     default=float("nan"))}
 
 
 def served(stream, arrays, check=True, **server_kwargs):

@@ -185,8 +185,10 @@ def test_tiny_systems():
 def test_same_pattern_batch_many_rhs():
     """The same-pattern batch (several instances sharing Ap/Ai, each with
     several right-hand sides): one analysis, a refactorization per instance,
-    SolveMany per instance; every column at backward error <= 1e-14 and equal
-    to the single-right-hand-side solve of that column."""
+    SolveMany per instance; every column at backward error <= 1e-14 and within
+    rounding of the single-right-hand-side solve of that column (SolveMany
+    runs the columns in lockstep through the several-vector triangular
+    solves, which add in another order: 1e-12 normwise relative)."""
     batch = kkt.batch2d(instances=3, grid=24, nrhs=4, seed=6)
     solver = mp.GmresLDLIR()
     solver.analyze(batch[0].Ap, batch[0].Ai, batch[0].Ax)
@@ -196,7 +198,7 @@ def test_same_pattern_batch_many_rhs():
         assert X.shape == s.b.shape
         for k in range(s.b.shape[0]):
             assert kkt.backward_error(s.n, s.Ap, s.Ai, s.Ax, X[k], s.b[k]) <= 1e-14
-        np.testing.assert_array_equal(X[1], solver.Solve(s.b[1]))
+        assert rel_norm_diff(X[1], solver.Solve(s.b[1])) <= 1e-12
         assert len(solver.last_reports) == s.b.shape[0]
 
 
@@ -320,7 +322,7 @@ def test_low_precision_factor_tier_converges(uf):
         x = solver.Solve(s.b)
         be = kkt.backward_error(s.n, s.Ap, s.Ai, s.Ax, x, s.b)
         assert be <= 1e-14, (uf, be, solver.last_report)
-        # L is stored and applied in the tier's type
+        # the report names the tier the factor was computed in
         assert solver.last_report["factor_prec"] == mp._PREC[uf]
         # lockstep solves read the same 16-bit L through the several-vector
         # kernels
