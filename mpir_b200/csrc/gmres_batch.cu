@@ -62,7 +62,7 @@ void Solver::ensure_batch(int width) {
 }
 
 void Solver::multi_apply(double *block) {
-  ldlt_solve_multi(*plan_, num_, block, bw_, mws_, stream_);
+  ldlt_solve_multi_graph(*plan_, num_, block, bw_, mws_, stream_, own_stream_);
 }
 
 void Solver::precond_device(int nrhs, double *d_X) {

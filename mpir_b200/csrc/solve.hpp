@@ -37,9 +37,35 @@ void ldlt_solve_graph(const Plan &P, const Numeric &F, double *x, SolveWorkspace
                       cudaStream_t s, cudaStream_t capture_stream);
 
 // Workspace of the several-vector solves (solve_multi.cu) for one width.
+// An instantiated CUDA graph, destroyed with its owner (movable).
+struct GraphExec {
+  cudaGraphExec_t g = nullptr;
+  GraphExec()       = default;
+  GraphExec(const GraphExec &) = delete;
+  GraphExec &operator=(const GraphExec &) = delete;
+  GraphExec(GraphExec &&o) noexcept : g(o.g) { o.g = nullptr; }
+  GraphExec &operator=(GraphExec &&o) noexcept {
+    if (this != &o) {
+      reset();
+      g   = o.g;
+      o.g = nullptr;
+    }
+    return *this;
+  }
+  ~GraphExec() { reset(); }
+  void reset() {
+    if (g) cudaGraphExecDestroy(g);
+    g = nullptr;
+  }
+};
+
 struct MultiSolveWorkspace {
   int          nr = 0;  // vectors per application (4, 8 or 16)
   DeviceBuffer zbuf, part, sync, ready, err;
+  // The application recorded as a graph on the fixed block xbuf (n x nr).
+  DeviceBuffer xbuf;
+  GraphExec    graph;
+  int64_t      graph_launches = 0;
   void         allocate(const Plan &P, int width);
   static size_t bytes_for(const Plan &P, int width);
 };
@@ -53,6 +79,13 @@ int multi_width(int nrhs);
 // at once (solve_multi.cu).
 void ldlt_solve_multi(const Plan &P, const Numeric &F, double *X, int width,
                       MultiSolveWorkspace &ws, cudaStream_t s, int phases = kAllPhases);
+// The same full application replayed from a graph recorded on first use on
+// capture_stream (X copied into and out of the workspace block): one launch
+// instead of a few per level, which is most of an application's cost for
+// small systems.  The plain launches while the per-class kernel timer is on.
+void ldlt_solve_multi_graph(const Plan &P, const Numeric &F, double *X, int width,
+                            MultiSolveWorkspace &ws, cudaStream_t s,
+                            cudaStream_t capture_stream);
 
 // QDLDL_solve (float32 factor, float64 x, host arrays) whose device data
 // lives in a fixed file-scope array instead of allocated memory; see

@@ -641,6 +641,9 @@ int multi_width(int nrhs) {
 void MultiSolveWorkspace::allocate(const Plan &P, int width) {
   const Symbolic &S = P.S;
   nr = width;
+  graph.reset();
+  xbuf.resize(std::max<int64_t>(S.n, 1) * width * sizeof(double));
+  MPIR_CUDA(cudaMemset(xbuf.as<void>(), 0, xbuf.bytes()));
   zbuf.resize(std::max<int64_t>(S.z_elems, 1) * width * sizeof(double));
   part.resize(std::max<int64_t>(P.spart_elems, 1) * width * sizeof(double));
   sync.resize(std::max<int64_t>(P.sync_elems, 1) * sizeof(int32_t));
@@ -653,7 +656,7 @@ void MultiSolveWorkspace::allocate(const Plan &P, int width) {
 size_t MultiSolveWorkspace::bytes_for(const Plan &P, int width) {
   const Symbolic &S = P.S;
   return (std::max<int64_t>(S.z_elems, 1) + std::max<int64_t>(P.spart_elems, 1) +
-          static_cast<int64_t>(kMultiCopies) * S.n) *
+          static_cast<int64_t>(kMultiCopies + 1) * S.n) *
              width * sizeof(double) +
          std::max<int64_t>(P.sync_elems, 1) * sizeof(int32_t) + sizeof(SolveCtl);
 }
@@ -675,6 +678,40 @@ void ldlt_solve_multi(const Plan &P, const Numeric &F, double *X, int width,
     case 3: run(F.panel16.as<const __half>()); break;
     default: run(F.panel.as<const float>());
   }
+}
+
+void ldlt_solve_multi_graph(const Plan &P, const Numeric &F, double *X, int width,
+                            MultiSolveWorkspace &ws, cudaStream_t s,
+                            cudaStream_t capture_stream) {
+  const int64_t n = P.S.n;
+  if (n == 0) return;
+  if (kernel_timer().enabled) {
+    ldlt_solve_multi(P, F, X, width, ws, s);
+    return;
+  }
+  if (!ws.graph.g) {
+    cudaGraph_t g = nullptr;
+    MPIR_CUDA(cudaStreamSynchronize(capture_stream));
+    MPIR_CUDA(cudaStreamBeginCapture(capture_stream, cudaStreamCaptureModeThreadLocal));
+    try {
+      LaunchCapture cap;
+      ldlt_solve_multi(P, F, ws.xbuf.as<double>(), width, ws, capture_stream);
+      ws.graph_launches = cap.count();
+    } catch (...) {
+      cudaStreamEndCapture(capture_stream, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    MPIR_CUDA(cudaStreamEndCapture(capture_stream, &g));
+    const cudaError_t e = cudaGraphInstantiate(&ws.graph.g, g, 0);
+    cudaGraphDestroy(g);
+    MPIR_CUDA(e);
+  }
+  const size_t bytes = static_cast<size_t>(n) * width * sizeof(double);
+  MPIR_CUDA(cudaMemcpyAsync(ws.xbuf.as<void>(), X, bytes, cudaMemcpyDeviceToDevice, s));
+  MPIR_CUDA(cudaGraphLaunch(ws.graph.g, s));
+  launch_add(ws.graph_launches);
+  MPIR_CUDA(cudaMemcpyAsync(X, ws.xbuf.as<void>(), bytes, cudaMemcpyDeviceToDevice, s));
 }
 
 }  // namespace mpir
