@@ -56,7 +56,12 @@ void Solver::ensure_batch(int width) {
   vecb_.allocate(n, sms, width);
   if (hpin_) cudaFreeHost(hpin_);
   hpin_ = nullptr;
-  MPIR_CUDA(cudaMallocHost(&hpin_, sizeof(double) * ((m + 1) * width + 4 * width)));
+  // Pinned staging: kStageSlots slots of (width scale factors, width flags)
+  // used in turn without waiting (every inner step synchronises once, and
+  // takes fewer uploads than slots), then the counts and the coefficients.
+  MPIR_CUDA(cudaMallocHost(&hpin_, sizeof(double) * (kStageSlots * 2 * width + width +
+                                                     (m + 1) * width)));
+  stage_next_ = 0;
   bw_ = width;
   bm_ = m;
 }
@@ -112,20 +117,18 @@ void Solver::precond_gmres_batch(int nb, const double *b, double *res, std::vect
   const int64_t *Kp = P.Kp.as<int64_t>();
   const int32_t *Kj = P.Kj.as<int32_t>();
   const double  *Kv = num_.Kval.as<double>();
-  double        *hfac = hpin_;                        // width doubles
-  int32_t       *hact = reinterpret_cast<int32_t *>(hpin_ + W);
-  int32_t       *hkq  = reinterpret_cast<int32_t *>(hpin_ + 2 * W);
-  double        *hy   = hpin_ + 4 * W;                // width x (m + 1)
+  int32_t       *hkq  = reinterpret_cast<int32_t *>(hpin_ + kStageSlots * 2 * W);
+  double        *hy   = hpin_ + kStageSlots * 2 * W + W;  // width x (m + 1)
   double        *dfac = bfac_.as<double>();
   int32_t       *dact = bact_.as<int32_t>();
   std::vector<double> banks(static_cast<size_t>(HS) * nb);
   auto put_act = [&](const std::vector<int32_t> &a) {
-    MPIR_CUDA(cudaStreamSynchronize(s));  // the staging area is free again
+    int32_t *hact = reinterpret_cast<int32_t *>(stage_slot());
     for (int k = 0; k < W; k++) hact[k] = k < nb ? a[k] : 0;
     MPIR_CUDA(cudaMemcpyAsync(dact, hact, W * sizeof(int32_t), cudaMemcpyHostToDevice, s));
   };
   auto put_fac = [&](const std::vector<double> &f) {
-    MPIR_CUDA(cudaStreamSynchronize(s));
+    double *hfac = stage_slot();
     for (int k = 0; k < W; k++) hfac[k] = k < nb ? f[k] : 1.0;
     MPIR_CUDA(cudaMemcpyAsync(dfac, hfac, W * sizeof(double), cudaMemcpyHostToDevice, s));
   };
@@ -288,6 +291,7 @@ void Solver::precond_gmres_batch(int nb, const double *b, double *res, std::vect
     any_y |= K > 0;
   }
   if (any_y) {
+    int32_t *hact = reinterpret_cast<int32_t *>(stage_slot());
     for (int k = 0; k < W; k++) hact[k] = k < nb && act[k] && hkq[k] > 0;
     MPIR_CUDA(cudaMemcpyAsync(dact, hact, W * sizeof(int32_t), cudaMemcpyHostToDevice, s));
     MPIR_CUDA(cudaMemcpyAsync(bkq_.as<int32_t>(), hkq, W * sizeof(int32_t),
@@ -351,14 +355,15 @@ int Solver::solve_batch_device(int nrhs, const double *d_B, double *d_X, Report 
   const double eps_w = eps_of(uw);
   std::vector<double> fac(nb, 1.0);
   auto put = [&](const std::vector<int32_t> &a, const std::vector<double> &f) {
-    MPIR_CUDA(cudaStreamSynchronize(s));
+    double  *hf = stage_slot();
+    int32_t *ha = reinterpret_cast<int32_t *>(hf + bw_);
     for (int k = 0; k < bw_; k++) {
-      reinterpret_cast<int32_t *>(hpin_ + bw_)[k] = k < nb ? a[k] : 0;
-      hpin_[k]                                   = k < nb ? f[k] : 1.0;
+      ha[k] = k < nb ? a[k] : 0;
+      hf[k] = k < nb ? f[k] : 1.0;
     }
-    MPIR_CUDA(cudaMemcpyAsync(bact_.as<void>(), hpin_ + bw_, bw_ * sizeof(int32_t),
+    MPIR_CUDA(cudaMemcpyAsync(bact_.as<void>(), ha, bw_ * sizeof(int32_t),
                               cudaMemcpyHostToDevice, s));
-    MPIR_CUDA(cudaMemcpyAsync(bfac_.as<void>(), hpin_, bw_ * sizeof(double),
+    MPIR_CUDA(cudaMemcpyAsync(bfac_.as<void>(), hf, bw_ * sizeof(double),
                               cudaMemcpyHostToDevice, s));
   };
   for (int64_t iter = 1; iter <= ir_iter; iter++) {

@@ -148,6 +148,16 @@ class Solver {
   DeviceBuffer          bV_, bbs_, bbp_, bx_, br_, bt_, bd_, bhd_, by_, bfac_, bact_, bkq_, bin_,
                         bout_, bpre_;
   double               *hpin_ = nullptr;  // pinned host scalars (fac, y, act, kq)
+  static constexpr int  kStageSlots = 16;
+  int                   stage_next_ = 0;
+  // The next staging slot (2 * bw_ doubles) for an upload of per-vector
+  // scalars; slots are reused after kStageSlots uploads, and the batched
+  // solve synchronises its stream at least once in fewer uploads than that.
+  double *stage_slot() {
+    double *p   = hpin_ + static_cast<size_t>(stage_next_) * 2 * bw_;
+    stage_next_ = (stage_next_ + 1) % kStageSlots;
+    return p;
+  }
   int32_t               wait_ctl_[2] = {0, 0};  // SolveCtl words 1-2 (set_wait_controls)
   cudaEvent_t           ev0_ = nullptr, ev1_ = nullptr;
   std::vector<IrEvent>  log_;
