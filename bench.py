@@ -801,6 +801,7 @@ def run_stream(args):
     seconds = rank_max(pg, summ["seconds"], dev)
     completed = rank_sum(pg, summ["completed"], dev)
     value = completed / seconds
+    arrivals_span = st.requests[-1].t_arrival
     lat_pass = None
     if not args.no_latency_pass:
         rate = 0.5 * summ["solves_per_s"]
@@ -845,7 +846,7 @@ def run_stream(args):
                    "l2": "inputs larger than L2 (factors up to tens of GB)"},
         "latency_ms": {"p50": summ["p50_ms"], "p99": summ["p99_ms"],
                        "note": "saturating arrival rate (all requests within ~"
-                               f"{st.requests[-1].t_arrival:.2f}s)"},
+                               f"{arrivals_span:.2f}s)"},
         "latency_half_capacity_ms": lat_pass,
         "drop_in": drop,
         "served_over_drop_in": (value / drop["solves_per_s"]) if drop else None,
@@ -855,7 +856,10 @@ def run_stream(args):
                      "refused_over_budget": stats["refused"],
                      "paths": {p: sum(1 for r in ok if r["path"] == p) for p in (0, 1, 2)},
                      "batched_rhs": stats["batched_rhs"], "evictions": stats["evictions"],
-                     "peak_gb": stats["peak_bytes"] / 1e9},
+                     "peak_gb": stats["peak_bytes"] / 1e9,
+                     "plans_rebuilt_from_kept_analysis": stats["analysis_reuses"],
+                     "worker_seconds": {k: round(stats[k + "_ms"] / 1e3, 2)
+                                        for k in ("analysis", "plan", "factor", "solve")}},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
                 "d2h_bytes_per_step": d2h / args.steps,
                 "note": "the served arm is itself end to end: host arrays in through "

@@ -382,6 +382,11 @@ typedef struct mpir_server_stats {
   int64_t analyses, factorizations, solves, batched_solves, batched_rhs;
   int64_t evictions, resident_factors, resident_patterns, queued;
   int64_t bytes_in_use, peak_bytes;
+  int64_t analysis_reuses;  /* plans rebuilt from the kept host analysis of an
+                               evicted pattern (the ordering is not redone) */
+  /* worker wall time summed over workers: host analysis, plan build and
+   * upload, factorizations (allocation included), solves */
+  double analysis_ms, plan_ms, factor_ms, solve_ms;
 } mpir_server_stats;
 
 int mpir_server_create(mpir_server *out, const mpir_server_config *cfg);

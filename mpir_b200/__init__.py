@@ -90,7 +90,8 @@ class ServerStats(C.Structure):
     _fields_ = [(k, C.c_int64) for k in (
         "submitted", "completed", "failed", "refused", "analyses", "factorizations", "solves",
         "batched_solves", "batched_rhs", "evictions", "resident_factors", "resident_patterns",
-        "queued", "bytes_in_use", "peak_bytes")]
+        "queued", "bytes_in_use", "peak_bytes", "analysis_reuses")] + [
+        (k, C.c_double) for k in ("analysis_ms", "plan_ms", "factor_ms", "solve_ms")]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -1050,6 +1050,11 @@ int mpir_server_get_stats(mpir_server s, mpir_server_stats *out) {
     out->queued            = st.queued;
     out->bytes_in_use      = st.bytes_in_use;
     out->peak_bytes        = st.peak_bytes;
+    out->analysis_reuses   = st.analysis_reuses;
+    out->analysis_ms       = st.analysis_ms;
+    out->plan_ms           = st.plan_ms;
+    out->factor_ms         = st.factor_ms;
+    out->solve_ms          = st.solve_ms;
     return MPIR_OK;
   });
 }

@@ -94,6 +94,14 @@ void Solver::adopt(std::shared_ptr<Plan> P) {
   // these scaled quasi-definite systems, whose entries reach 1/delta-sized
   // values, while bfloat16 has float32's exponent range.
   num_.store_prec = uf == kBF16 ? 2 : 1;
+  if (num_.store_prec == 2) {
+    // The 16-bit copy sits beside the float32 panels during factorization;
+    // where both do not fit, the solves read the float32 panels instead.
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess &&
+        Numeric::bytes_for(*plan_, 2) > free_b / 100 * 97)
+      num_.store_prec = 1;
+  }
   num_.allocate(*plan_);
   num_.update_mode = update_mode_for(uf);
   ws_.allocate(*plan_);

@@ -82,6 +82,8 @@ struct Server::Impl {
   std::map<uint64_t, Pattern>          patterns;
   std::map<FKey, Factor>               factors;
   std::unordered_map<int64_t, ServerResult> done;
+  // Host analyses of every pattern seen (host memory, never evicted).
+  std::map<uint64_t, std::shared_ptr<const Symbolic>> sym_cache;
   std::vector<std::thread>             workers;
   ServerStats                          st{};
   size_t                               used    = 0;
@@ -209,9 +211,29 @@ struct Server::Impl {
         for (int64_t j = 0; j < r.n; j++)
           for (int64_t p = r.Ap[j]; p < r.Ap[j + 1]; p++)
             if (r.Ai[p] == j && r.Ax[p] > 0) sign[j] = 1;
+        // A pattern seen before (its plan since evicted) takes its host
+        // analysis from the cache and only uploads its plan again.
+        std::shared_ptr<const Symbolic> cached;
+        {
+          std::lock_guard<std::mutex> lk(mu);
+          auto it = sym_cache.find(r.pattern_key);
+          if (it != sym_cache.end()) cached = it->second;
+        }
+        const double ta = now_s();
         Symbolic    S;
         std::string err;
-        const int   rc = analyze(r.n, r.Ap, r.Ai, sign.data(), Ordering::Auto, S, err);
+        int         rc = kOk;
+        if (cached) {
+          S = *cached;
+        } else {
+          rc = analyze(r.n, r.Ap, r.Ai, sign.data(), Ordering::Auto, S, err);
+          if (rc == kOk) {
+            auto keep = std::make_shared<const Symbolic>(S);
+            std::lock_guard<std::mutex> lk(mu);
+            sym_cache[r.pattern_key] = std::move(keep);
+          }
+        }
+        const double tb = now_s();
         if (rc != kOk) {
           {
             std::lock_guard<std::mutex> lk(mu);
@@ -244,6 +266,9 @@ struct Server::Impl {
         p.last     = now_s();
         used += p.bytes;
         st.analyses++;
+        if (cached) st.analysis_reuses++;
+        st.analysis_ms += 1e3 * (tb - ta);
+        st.plan_ms += 1e3 * (p.last - tb);
         st.peak_bytes = std::max<int64_t>(st.peak_bytes, used);
       } else {
         std::lock_guard<std::mutex> lk(mu);
@@ -279,6 +304,7 @@ struct Server::Impl {
         }
         graveyard.clear();
         plan_graveyard.clear();
+        const double tf     = now_s();
         auto solver = std::make_unique<Solver>(cfg.uf, kF64, cfg.ur, cfg.device);
         solver->ir_iter    = cfg.max_ir_iterations;
         solver->gmres_iter = cfg.max_gmres_iterations;
@@ -298,6 +324,7 @@ struct Server::Impl {
           f.last    = now_s();
           patterns[r.pattern_key].factors++;
           st.factorizations++;
+          st.factor_ms += 1e3 * (now_s() - tf);
           st.peak_bytes = std::max<int64_t>(st.peak_bytes, used);
           sv = f.solver.get();
         }
@@ -312,6 +339,7 @@ struct Server::Impl {
         sv = factors.at(k).solver.get();
       }
       // Solve the batch: one request alone, several in lockstep.
+      const double  ts = now_s();
       const int64_t n  = plan->S.n;
       const int     nb = static_cast<int>(job.reqs.size());
       std::vector<Report> reps(nb);
@@ -337,6 +365,7 @@ struct Server::Impl {
         f.last         = now_s();
         patterns[r.pattern_key].last = f.last;
         st.solves++;
+        st.solve_ms += 1e3 * (now_s() - ts);
         if (nb > 1) {
           st.batched_solves++;
           st.batched_rhs += nb;

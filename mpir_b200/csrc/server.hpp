@@ -48,6 +48,11 @@ struct ServerStats {
   int64_t analyses = 0, factorizations = 0, solves = 0, batched_solves = 0, batched_rhs = 0;
   int64_t evictions = 0, resident_factors = 0, resident_patterns = 0, queued = 0;
   int64_t bytes_in_use = 0, peak_bytes = 0;
+  int64_t analysis_reuses = 0;  // plans rebuilt from a cached host analysis
+  // Worker time (host wall clock, summed over workers) in the host analysis,
+  // the plan build and upload, the factorizations (allocation included) and
+  // the solves.
+  double analysis_ms = 0, plan_ms = 0, factor_ms = 0, solve_ms = 0;
 };
 
 class Server {
