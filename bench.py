@@ -81,6 +81,8 @@ def parse():
     ap.add_argument("--no-latency-pass", action="store_true")
     ap.add_argument("--no-dropin", action="store_true")
     ap.add_argument("--group", type=int, default=8, help="batch2d: instances per graph launch")
+    ap.add_argument("--update", default=None, choices=["default", "tf32x3", "bf16x3"],
+                    help="trailing-update engine of float32 factors")
     return ap.parse_args()
 
 
@@ -628,6 +630,8 @@ def run_system(args):
 
     s, workload = system_for(args, rank)
     solver = mp.GmresLDLIR(uf=uf, device=local)
+    if args.update:
+        solver.set_update(args.update)
     low = uf != "f32" or args.config == "illcond3d"
     solver.SetMaxGmresIterations(args.gmres_iter or (50 if low else 10))
     solver.SetMaxIRIterations(args.ir_iter or (30 if low else 10))
@@ -778,7 +782,7 @@ def run_stream(args):
     ir_iter = args.ir_iter or (30 if low else 10)
     gmres_iter = args.gmres_iter or (30 if low else 10)
     nreq = args.requests_per_step * args.steps
-    srv_kw = dict(uf=uf, workers=args.workers, max_batch=16,
+    srv_kw = dict(uf=uf, workers=args.workers, max_batch=16, update=args.update or "default",
                   budget_bytes=int(args.budget_gb * (1 << 30)), ir_iter=ir_iter,
                   gmres_iter=gmres_iter, tol=1e-10, device=local)
     st = smod.Stream(nreq, rate=1e4, seed=replica_seed(args.seed, rank))
@@ -841,7 +845,8 @@ def run_stream(args):
         "data": "synthetic (seeded KKT request stream, one stream per rank)",
         "config": {"workload": stream_workload(args, nreq), "global_batch": world * nreq,
                    "seq_len": None, "parallelism": f"replicas{world}",
-                   "served": {"uf": uf, "workers": args.workers, "max_batch": 16,
+                   "served": {"uf": uf, "update": args.update or "default",
+                              "workers": args.workers, "max_batch": 16,
                               "ir_iter": ir_iter, "gmres_iter": gmres_iter},
                    "l2": "inputs larger than L2 (factors up to tens of GB)"},
         "latency_ms": {"p50": summ["p50_ms"], "p99": summ["p99_ms"],
@@ -875,6 +880,8 @@ def run_stream(args):
                   key=lambda i: arrays[i][0].nnz)
         s, Ax, b, _ = arrays[big]
         g = mp.GmresLDLIR(uf=uf, device=local)
+        if args.update:
+            g.set_update(args.update)
         g.SetMaxGmresIterations(gmres_iter)
         g.SetMaxIRIterations(ir_iter)
         g.Compute(s.Ap, s.Ai, Ax)

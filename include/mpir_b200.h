@@ -261,6 +261,15 @@ int mpir_luir_qdldl(int64_t n, const int64_t *Ap, const int64_t *Ai,
                     const double *Ax, const double *b, double *x,
                     int fact_prec, int maxiter, mpir_report *rep, int device);
 
+/* Trailing-update engine of a float32 factor (from the next factorization):
+ * MPIR_UPDATE_TF32X3 (the default: three tf32 tensor-core products per
+ * update, float32-level accuracy) or MPIR_UPDATE_BF16X3 (three bfloat16
+ * products of high and low parts: about 16 significant bits, twice the
+ * rate; a preconditioner for GMRES-IR, not a float32-accurate factor).
+ * 16-bit factor types ignore it. */
+enum { MPIR_UPDATE_DEFAULT = 0, MPIR_UPDATE_TF32X3 = 1, MPIR_UPDATE_BF16X3 = 2 };
+int mpir_solver_set_update(mpir_solver s, int engine);
+
 /* Launch the solver's work on a caller stream (a cudaStream_t; NULL
  * restores the solver's own stream). */
 int mpir_solver_set_stream(mpir_solver s, void *stream);
@@ -348,7 +357,7 @@ typedef struct mpir_server_config {
   int32_t ur;          /* MPIR_F64 or MPIR_DD */
   int32_t workers;     /* concurrent jobs (host threads, one CUDA stream each) */
   int32_t max_batch;   /* right-hand sides per lockstep solve, 1 .. 16 */
-  int32_t pad;
+  int32_t update;      /* MPIR_UPDATE_* engine of float32 factors */
   int64_t budget_bytes;           /* device memory for plans and factors */
   int64_t max_ir_iterations;      /* GmresLDLIR setters (gmres_ir.hpp:291-303) */
   int64_t max_gmres_iterations;

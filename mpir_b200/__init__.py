@@ -33,6 +33,7 @@ ORDER_NATURAL, ORDER_AUTO = 0, 1
 _PREC = {"f64": F64, "double": F64, np.float64: F64, "f32": F32, "float": F32,
          np.float32: F32, "bf16": BF16, "bfloat16": BF16, "f16": F16, "half": F16,
          np.float16: F16, "dd": DD, "dd_real": DD}
+UPDATE = {"default": 0, "tf32x3": 1, "bf16x3": 2}
 STATUS = {0: "ok", -1: "input", -2: "overflow", -3: "cuda", -4: "nomem", -5: "timeout",
           -6: "argument", -7: "unsupported", -8: "state"}
 
@@ -69,7 +70,7 @@ class Info(C.Structure):
 
 class ServerConfig(C.Structure):
     _fields_ = [("device", C.c_int32), ("uf", C.c_int32), ("ur", C.c_int32),
-                ("workers", C.c_int32), ("max_batch", C.c_int32), ("pad", C.c_int32),
+                ("workers", C.c_int32), ("max_batch", C.c_int32), ("update", C.c_int32),
                 ("budget_bytes", C.c_int64), ("max_ir_iterations", C.c_int64),
                 ("max_gmres_iterations", C.c_int64), ("tolerance", C.c_double)]
 
@@ -129,6 +130,7 @@ def lib():
         "mpir_solver_solve": (i32, [vp, vp, vp, vp]),
         "mpir_solver_solve_device": (i32, [vp, vp, vp, vp]),
         "mpir_solver_set_stream": (i32, [vp, vp]),
+        "mpir_solver_set_update": (i32, [vp, i32]),
         "mpir_solver_solve_many": (i32, [vp, i64, vp, vp, vp]),
         "mpir_solver_solve_batch": (i32, [vp, i32, vp, vp, vp]),
         "mpir_solver_solve_batch_device": (i32, [vp, i32, vp, vp, vp]),
@@ -444,6 +446,11 @@ class GmresLDLIR:
             raise MpirError(int(r), last_error())
         return int(r)
 
+    def set_update(self, engine):
+        """Trailing-update engine of a float32 factor: "tf32x3" (default) or
+        "bf16x3" (from the next factorization)."""
+        _check(lib().mpir_solver_set_update(self._h, UPDATE[engine]))
+
     def set_stream(self, stream_handle: int):
         _check(lib().mpir_solver_set_stream(self._h, C.c_void_p(stream_handle)))
 
@@ -551,9 +558,10 @@ class Server:
     result.  Arrays are kept referenced until the request is done."""
 
     def __init__(self, uf="f32", ur="f64", workers=4, max_batch=16, budget_bytes=150 << 30,
-                 ir_iter=10, gmres_iter=10, tol=1e-10, device=0):
+                 ir_iter=10, gmres_iter=10, tol=1e-10, device=0, update="default"):
         cfg = ServerConfig(device=device, uf=_PREC[uf], ur=_PREC[ur], workers=workers,
-                           max_batch=max_batch, pad=0, budget_bytes=int(budget_bytes),
+                           max_batch=max_batch, update=UPDATE[update],
+                           budget_bytes=int(budget_bytes),
                            max_ir_iterations=ir_iter, max_gmres_iterations=gmres_iter,
                            tolerance=tol)
         self._h = C.c_void_p()

@@ -728,6 +728,14 @@ int mpir_luir_qdldl(int64_t n, const int64_t *Ap, const int64_t *Ai, const doubl
   });
 }
 
+int mpir_solver_set_update(mpir_solver s, int engine) {
+  MPIR_NEED(s);
+  return guard([&]() -> int {
+    s->impl->set_update_engine(engine);
+    return MPIR_OK;
+  });
+}
+
 int mpir_solver_set_stream(mpir_solver s, void *stream) {
   MPIR_NEED(s);
   s->impl->set_stream(static_cast<cudaStream_t>(stream));
@@ -966,6 +974,9 @@ int mpir_server_create(mpir_server *out, const mpir_server_config *cfg) {
     c.ur                   = cfg->ur;
     c.workers              = cfg->workers;
     c.max_batch            = cfg->max_batch;
+    if (cfg->update < 0 || cfg->update > 2)
+      throw StatusError(MPIR_ERR_ARGUMENT, "update engine: 0 default, 1 3xTF32, 2 3xBF16");
+    c.update               = cfg->update;
     c.budget_bytes         = cfg->budget_bytes;
     c.max_ir_iterations    = cfg->max_ir_iterations;
     c.max_gmres_iterations = cfg->max_gmres_iterations;

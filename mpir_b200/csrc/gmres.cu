@@ -30,16 +30,19 @@ double eps_of(int prec) {
 
 // Trailing-update engine for a factor type: float32 runs 3xTF32 tensor-core
 // products (float32-level accuracy), bfloat16 / float16 factors single-pass
-// tensor-core products in that type; MPIR_UPDATE ("simt" = float32 SIMT
-// units, "tf32x3", "bf16", "f16") overrides.
-static int update_mode_for(int uf) {
-  int mode = uf == kBF16 ? 0 : uf == kF16 ? 2 : 1;
+// tensor-core products in that type; a float32 factor may instead take
+// 3xBF16 products (about 16 significant bits, twice the 3xTF32 rate:
+// Solver::update_engine = kUpdateBF16x3); MPIR_UPDATE ("simt" = float32 SIMT
+// units, "tf32x3", "bf16x3", "bf16", "f16") overrides.
+static int update_mode_for(int uf, int engine) {
+  int mode = uf == kBF16 ? 0 : uf == kF16 ? 2 : engine == kUpdateBF16x3 ? 3 : 1;
   if (const char *e = std::getenv("MPIR_UPDATE")) {
     const std::string v(e);
     if (v == "simt") mode = -1;
     else if (v == "bf16") mode = 0;
     else if (v == "tf32x3") mode = 1;
     else if (v == "f16") mode = 2;
+    else if (v == "bf16x3") mode = 3;
   }
   return mode;
 }
@@ -103,7 +106,7 @@ void Solver::adopt(std::shared_ptr<Plan> P) {
       num_.store_prec = 1;
   }
   num_.allocate(*plan_);
-  num_.update_mode = update_mode_for(uf);
+  num_.update_mode = update_mode_for(uf, update_engine);
   ws_.allocate(*plan_);
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -191,6 +194,13 @@ int Solver::factor(const double *Ax) {
   MPIR_CUDA(cudaMemcpyAsync(num_.Ax.as<void>(), Ax, plan_->S.nnz * sizeof(double),
                             cudaMemcpyHostToDevice, stream_));
   return factor_device(num_.Ax.as<double>());
+}
+
+void Solver::set_update_engine(int engine) {
+  if (engine != kUpdateDefault && engine != kUpdateTF32x3 && engine != kUpdateBF16x3)
+    throw std::invalid_argument("update engine: 0 default, 1 3xTF32, 2 3xBF16");
+  update_engine = engine;
+  if (plan_) num_.update_mode = update_mode_for(uf, engine);
 }
 
 double *Solver::values_device() {

@@ -31,6 +31,7 @@ FactorGroup::FactorGroup(Solver &base, int k) : device_(base.device) {
     s->ir_iter    = base.ir_iter;
     s->gmres_iter = base.gmres_iter;
     s->tol        = base.tol;
+    s->update_engine = base.update_engine;
     s->adopt(base.shared_plan());
     members_.push_back(std::move(s));
   }

@@ -309,6 +309,7 @@ struct Server::Impl {
         solver->ir_iter    = cfg.max_ir_iterations;
         solver->gmres_iter = cfg.max_gmres_iterations;
         solver->tol        = cfg.tolerance;
+        solver->update_engine = cfg.update;
         solver->adopt(plan);
         const int fr = solver->factor(r.Ax);
         // A resident factor keeps only what the solves read.

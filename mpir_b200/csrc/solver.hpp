@@ -13,6 +13,8 @@
 namespace mpir {
 
 enum Prec : int { kF64 = 0, kF32 = 1, kBF16 = 2, kF16 = 3, kDD = 4 };
+// Trailing-update engines a float32 factor may take (mpir_solver_set_update).
+enum UpdateEngine : int { kUpdateDefault = 0, kUpdateTF32x3 = 1, kUpdateBF16x3 = 2 };
 
 // A bounded device wait of the triangular solves ran out (status -5).
 struct WaitTimeout : std::runtime_error {
@@ -59,6 +61,10 @@ class Solver {
   int64_t ir_iter    = 10;    // gmres_ir.hpp:113-114
   int64_t gmres_iter = 10;    // gmres_ir.hpp:115-116 (clamped to n on use)
   double  tol        = 1e-10; // gmres_ir.hpp:117
+  int     update_engine = kUpdateDefault;  // see set_update_engine
+  // Trailing-update engine of a float32 factor (UpdateEngine); takes effect
+  // at the next factorization.
+  void set_update_engine(int engine);
 
   // Host entry points (caller arrays on the host, caller order).
   int analyze(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *Ax,

@@ -27,6 +27,10 @@
 //                      float32-level accuracy (round-to-nearest splits).
 //   kind::f16 bfloat16 / float16: balanced operands (A sqrt|D| sign D) and
 //                      (A sqrt|D|), which keep both in range.
+//   kind::f16 3xBF16:  the balanced operands split into bfloat16 high and
+//                      low parts, A_hi B_hi + A_hi B_lo + A_lo B_hi per
+//                      16-wide K step (about 16 significant bits: between
+//                      tf32 and float32), at the bfloat16 rate.
 //
 // Every mbarrier wait is bounded; on expiry the kernel records a timeout in
 // the factor status, stops issuing work, waits (bounded) for its own copies
@@ -172,6 +176,16 @@ __device__ __forceinline__ uint32_t pack16(float a, float b) {
   return MODE == 2 ? pack_f16(a, b) : pack_bf16(a, b);
 }
 
+// bfloat16 high part of a and b (round to nearest) and the bfloat16 of what
+// the high part leaves.
+__device__ __forceinline__ void split_bf16(float a, float b, uint32_t &hi, uint32_t &lo) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  const float2         f = __bfloat1622float2(h);
+  const __nv_bfloat162 l = __floats2bfloat162_rn(a - f.x, b - f.y);
+  hi                     = *reinterpret_cast<const uint32_t *>(&h);
+  lo                     = *reinterpret_cast<const uint32_t *>(&l);
+}
+
 // tf32 high and low parts of four values (round to nearest both times).
 __device__ __forceinline__ void split4(const float (&v)[4], uint4 &hi, uint4 &lo) {
   uint32_t *hp = &hi.x, *lp = &lo.x;
@@ -227,6 +241,27 @@ __device__ __forceinline__ void convert_row(uint8_t *stage, int m) {
       bv[4 * g + 1] = b.y * fabsf(s.y);
       bv[4 * g + 2] = b.z * fabsf(s.z);
       bv[4 * g + 3] = b.w * fabsf(s.w);
+    }
+    if (MODE == 3) {
+      // high parts over the first half of each block, low parts over the
+      // second half (row m's 16 bytes of each K-group are this thread's)
+#pragma unroll
+      for (int q = 0; q < C::kKG / 2; q++) {
+        uint4 ah, al, bh, bl;
+        split_bf16(av[8 * q + 0], av[8 * q + 1], ah.x, al.x);
+        split_bf16(av[8 * q + 2], av[8 * q + 3], ah.y, al.y);
+        split_bf16(av[8 * q + 4], av[8 * q + 5], ah.z, al.z);
+        split_bf16(av[8 * q + 6], av[8 * q + 7], ah.w, al.w);
+        split_bf16(bv[8 * q + 0], bv[8 * q + 1], bh.x, bl.x);
+        split_bf16(bv[8 * q + 2], bv[8 * q + 3], bh.y, bl.y);
+        split_bf16(bv[8 * q + 4], bv[8 * q + 5], bh.z, bl.z);
+        split_bf16(bv[8 * q + 6], bv[8 * q + 7], bh.w, bl.w);
+        *reinterpret_cast<uint4 *>(stage + C::kA + q * kGroup + m * 16)                = ah;
+        *reinterpret_cast<uint4 *>(stage + C::kA + (q + C::kKG / 2) * kGroup + m * 16) = al;
+        *reinterpret_cast<uint4 *>(stage + C::kB + q * kGroup + m * 16)                = bh;
+        *reinterpret_cast<uint4 *>(stage + C::kB + (q + C::kKG / 2) * kGroup + m * 16) = bl;
+      }
+      return;
     }
 #pragma unroll
     for (int q = 0; q < C::kKG / 2; q++) {
@@ -293,7 +328,8 @@ __device__ __forceinline__ Unit locate_unit(const GemmProb *probs, int nprob, co
 
 constexpr int kMaxProbSmem = 2048;  // problems whose first units go to shared memory
 
-// MODE 0: bfloat16 single pass; MODE 1: 3xTF32; MODE 2: float16 single pass.
+// MODE 0: bfloat16 single pass; MODE 1: 3xTF32; MODE 2: float16 single pass;
+// MODE 3: 3xBF16.
 // Persistent: CTA b takes units b, b + gridDim.x, ...; the ring stages run on
 // across units (the producer loads the next unit's first stages while the
 // epilogue drains the accumulator of the current one); the accumulator is
@@ -396,7 +432,8 @@ __global__ void __launch_bounds__(tc::kThreads, tc::kStages <= 3 ? 2 : 1)
   } else if (warp == 1) {
     // ---------------- MMA issuer
     if (lane == 0) {
-      const uint32_t idesc = make_idesc(MODE == 0 ? kFmtBF16 : MODE == 1 ? kFmtTF32 : kFmtF16);
+      const uint32_t idesc =
+          make_idesc(MODE == 1 ? kFmtTF32 : MODE == 2 ? kFmtF16 : kFmtBF16);
       long           g     = 0;
       int            jn    = 0;
       for (int u = blockIdx.x; u < units && !s_fail; u += gridDim.x, jn++) {
@@ -431,6 +468,15 @@ __global__ void __launch_bounds__(tc::kThreads, tc::kStages <= 3 ? 2 : 1)
               mma<true>(tmem, ahd, bhd, idesc, acc);
               mma<true>(tmem, ahd, bld, idesc, 1u);
               mma<true>(tmem, ald, bhd, idesc, 1u);
+            } else if (MODE == 3) {
+              constexpr uint32_t kLo = C::kKG / 2 * kGroup;  // low parts' offset
+              const uint64_t ahd = make_desc(base + C::kA + off);
+              const uint64_t bhd = make_desc(base + C::kB + off);
+              const uint64_t ald = make_desc(base + C::kA + kLo + off);
+              const uint64_t bld = make_desc(base + C::kB + kLo + off);
+              mma<false>(tmem, ahd, bhd, idesc, acc);
+              mma<false>(tmem, ahd, bld, idesc, 1u);
+              mma<false>(tmem, ald, bhd, idesc, 1u);
             } else {
               mma<false>(tmem, make_desc(base + C::kA + off), make_desc(base + C::kB + off),
                          idesc, acc);
@@ -639,6 +685,8 @@ void launch_gemm_tc(int mode, const GemmProb *probs, int nprob, int units, const
     launch_mode<0>(probs, nprob, units, pack, packd, packs, bconv, panel, uarena, ws, st, s);
   else if (mode == 1)
     launch_mode<1>(probs, nprob, units, pack, packd, packs, bconv, panel, uarena, ws, st, s);
+  else if (mode == 3)
+    launch_mode<3>(probs, nprob, units, pack, packd, packs, bconv, panel, uarena, ws, st, s);
   else
     launch_mode<2>(probs, nprob, units, pack, packd, packs, bconv, panel, uarena, ws, st, s);
 }

@@ -353,3 +353,29 @@ def test_forward_error_against_fp64_direct_ldlt(ref_lib, name, s):
     fe = float(np.max(np.abs(x - xd)) / np.max(np.abs(xd)))
     assert fe <= max(10 * fe_direct, 1e-12), (fe, fe_direct)
     assert kkt.forward_error(x, s.x_true) <= max(10 * fe_direct, 1e-12)
+
+
+def test_bf16x3_update_engine(oracle_lib, ref_lib):
+    """3xBF16 trailing updates of a float32 factor (bfloat16 high and low
+    parts, three products): about 16 significant bits per product, so L and D
+    within 1e-4 normwise of the reference's float32 factor; GMRES-IR with it
+    still reaches backward error <= 1e-14."""
+    s = kkt.grid3d(grid=12, seed=9)
+    solver = mp.GmresLDLIR()
+    solver.set_update("bf16x3")
+    solver.Compute(s.Ap, s.Ai, s.Ax)
+    sym = solver.symbolic()
+    AD, Axs = oracle_lib.scale(s.n, s.Ap, s.Ai, s.Ax, FLT_EPS)
+    Cp, Ci, Cx = permuted_upper(s.n, s.Ap, s.Ai, Axs, sym["perm"])
+    Lp, Li, Lx, D, Dinv = solver.export_factor()
+    rs, rLp, rLi, rLx, rD, rDinv = ref_lib.factor(s.n, Cp, Ci, Cx, np.float32)
+    np.testing.assert_array_equal(Li, rLi)
+    assert rel_norm_diff(Lx, rLx) <= 1e-4
+    assert rel_norm_diff(D, rD) <= 1e-4
+    x = solver.Solve(s.b)
+    assert kkt.backward_error(s.n, s.Ap, s.Ai, s.Ax, x, s.b) <= 1e-14
+    # the default engine again on the same solver: float32-level factor
+    solver.set_update("tf32x3")
+    solver.factor(s.Ax)
+    Lp, Li, Lx, D, Dinv = solver.export_factor()
+    assert rel_norm_diff(Lx, rLx) <= 1e-5
