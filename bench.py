@@ -879,6 +879,7 @@ def run_stream(args):
                      "batched_rhs": stats["batched_rhs"], "evictions": stats["evictions"],
                      "peak_gb": stats["peak_bytes"] / 1e9,
                      "plans_rebuilt_from_kept_analysis": stats["analysis_reuses"],
+                     "plans_uploaded_again": stats["plan_uploads"],
                      "worker_seconds": {k: round(stats[k + "_ms"] / 1e3, 2)
                                         for k in ("analysis", "plan", "factor", "solve")}},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,

@@ -393,6 +393,8 @@ typedef struct mpir_server_stats {
   int64_t bytes_in_use, peak_bytes;
   int64_t analysis_reuses;  /* plans rebuilt from the kept host analysis of an
                                evicted pattern (the ordering is not redone) */
+  int64_t plan_uploads;     /* evicted plans uploaded again from their kept
+                               host tables (nothing recomputed) */
   /* worker wall time summed over workers: host analysis, plan build and
    * upload, factorizations (allocation included), solves */
   double analysis_ms, plan_ms, factor_ms, solve_ms;

@@ -91,7 +91,7 @@ class ServerStats(C.Structure):
     _fields_ = [(k, C.c_int64) for k in (
         "submitted", "completed", "failed", "refused", "analyses", "factorizations", "solves",
         "batched_solves", "batched_rhs", "evictions", "resident_factors", "resident_patterns",
-        "queued", "bytes_in_use", "peak_bytes", "analysis_reuses")] + [
+        "queued", "bytes_in_use", "peak_bytes", "analysis_reuses", "plan_uploads")] + [
         (k, C.c_double) for k in ("analysis_ms", "plan_ms", "factor_ms", "solve_ms")]
 
     def as_dict(self):

@@ -1062,6 +1062,7 @@ int mpir_server_get_stats(mpir_server s, mpir_server_stats *out) {
     out->bytes_in_use      = st.bytes_in_use;
     out->peak_bytes        = st.peak_bytes;
     out->analysis_reuses   = st.analysis_reuses;
+    out->plan_uploads      = st.plan_uploads;
     out->analysis_ms       = st.analysis_ms;
     out->plan_ms           = st.plan_ms;
     out->factor_ms         = st.factor_ms;

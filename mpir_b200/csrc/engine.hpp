@@ -130,6 +130,20 @@ class Plan {
   void build(Symbolic &&sym, cudaStream_t s);
   // Device memory the plan holds.
   size_t device_bytes() const;
+  // Frees the device arrays (the host arrays stay) / uploads them again.
+  void release_device();
+  void upload_all(cudaStream_t s);
+  bool on_device = false;
+  // Host copies of the launch and solve tables that build() computes.
+  struct HostArrays {
+    std::vector<StepDesc>   descs;
+    std::vector<EaTask>     tasks;
+    std::vector<int32_t>    seq, chunk_map;
+    std::vector<GemmProb>   probs;
+    std::vector<SolveFront> sfronts;
+    std::vector<int64_t>    gp, gsrc;
+    std::vector<SolveItem>  fwd_item, own_item;
+  } host_;
   bool is_large(int64_t J) const { return S.h(J) > kSmallFront; }
   // Packed-front geometry (PackedFront): first packed row of the
   // off-diagonal rows, K-groups per row tile, row tiles.

@@ -1268,7 +1268,23 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
     const double w = static_cast<double>(S.w(J)), h = static_cast<double>(S.h(J));
     panel_read_bytes += 4.0 * (w * h - w * (w - 1) / 2);
   }
-  // Upload.
+  sync_elems = 2 * static_cast<int64_t>(levels.size());
+  // The host arrays stay with the plan, so an evicted plan can go back to
+  // the device without being built again.
+  host_.descs       = std::move(descs);
+  host_.tasks       = std::move(tasks);
+  host_.seq         = std::move(seq_h);
+  host_.probs       = std::move(probs);
+  host_.sfronts     = std::move(sfronts);
+  host_.gp          = std::move(gp_h);
+  host_.gsrc        = std::move(gsrc_h);
+  host_.fwd_item    = std::move(fwd_item_h);
+  host_.chunk_map   = std::move(chunk_map_h);
+  host_.own_item    = std::move(own_item_h);
+  upload_all(s);
+}
+
+void Plan::upload_all(cudaStream_t s) {
   amap       = upload(S.amap, s);
   arow       = upload(S.arow, s);
   acol       = upload(S.acol, s);
@@ -1288,21 +1304,31 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
   perm       = upload(S.perm, s);
   small_list = upload(h_small, s);
   large_list = upload(h_large, s);
-  steps      = upload(descs, s);
-  ea_tasks   = upload(tasks, s);
-  ea_seq     = upload(seq_h, s);
-  gemm_probs = upload(probs, s);
+  steps      = upload(host_.descs, s);
+  ea_tasks   = upload(host_.tasks, s);
+  ea_seq     = upload(host_.seq, s);
+  gemm_probs = upload(host_.probs, s);
   linv_ofs_d = upload(linv_ofs, s);
-  solve_fronts = upload(sfronts, s);
+  solve_fronts = upload(host_.sfronts, s);
   swarp_list   = upload(h_swarp, s);
   sblock_list  = upload(h_sblock, s);
-  gp           = upload(gp_h, s);
-  gsrc         = upload(gsrc_h, s);
-  fwd_item     = upload(fwd_item_h, s);
-  chunk_map    = upload(chunk_map_h, s);
-  own_item     = upload(own_item_h, s);
-  sync_elems   = 2 * static_cast<int64_t>(levels.size());
+  gp           = upload(host_.gp, s);
+  gsrc         = upload(host_.gsrc, s);
+  fwd_item     = upload(host_.fwd_item, s);
+  chunk_map    = upload(host_.chunk_map, s);
+  own_item     = upload(host_.own_item, s);
   MPIR_CUDA(cudaStreamSynchronize(s));
+  on_device = true;
+}
+
+void Plan::release_device() {
+  for (DeviceBuffer *d :
+       {&amap, &arow, &acol, &diag_pos, &Kp, &Kj, &Ksrc, &sfirst, &srowptr, &srows, &srel,
+        &slofs, &uofs, &zofs, &child_ptr, &child_list, &perm, &ea_seq, &small_list,
+        &large_list, &steps, &ea_tasks, &linv_ofs_d, &gemm_probs, &solve_fronts, &swarp_list,
+        &sblock_list, &gp, &gsrc, &fwd_item, &chunk_map, &own_item})
+    d->release();
+  on_device = false;
 }
 
 void Numeric::allocate(const Plan &P) {

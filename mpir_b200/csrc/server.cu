@@ -57,8 +57,9 @@ struct Server::Impl {
 
   struct Pattern {
     std::shared_ptr<Plan> plan;
-    bool                  busy    = true;  // being analysed
-    size_t                bytes   = 0;
+    bool                  busy     = true;   // being analysed, uploaded or offloaded
+    bool                  resident = false;  // plan arrays on the device
+    size_t                bytes    = 0;
     double                last    = 0;
     int                   factors = 0;  // resident factors on this plan
   };
@@ -116,12 +117,14 @@ struct Server::Impl {
       job.reqs.clear();
       job.reqs.push_back(r);
       take_same(k, static_cast<size_t>(cfg.max_batch), job.reqs);
-      if (p == patterns.end()) {
-        Pattern np;
-        np.busy = true;
-        np.last = now_s();
-        patterns.emplace(r.pattern_key, std::move(np));
-        job.kind = Job::kAnalyse;
+      if (p == patterns.end() || !p->second.resident) {
+        if (p == patterns.end()) {
+          Pattern np;
+          np.last = now_s();
+          p       = patterns.emplace(r.pattern_key, std::move(np)).first;
+        }
+        p->second.busy = true;
+        job.kind       = Job::kAnalyse;
       } else if (f != factors.end() && f->second.valid) {
         job.kind = Job::kSolve;
       } else {
@@ -157,22 +160,41 @@ struct Server::Impl {
       }
       auto pv = patterns.end();
       for (auto it = patterns.begin(); it != patterns.end(); ++it) {
-        if (it->second.busy || it->second.factors != 0 || !it->second.plan) continue;
+        if (it->second.busy || it->second.factors != 0 || !it->second.resident) continue;
         bool referenced = false;  // by the placeholder factor of a running job
         for (auto &f : factors)
           if (f.first.first == it->first) referenced = true;
         if (!referenced && (pv == patterns.end() || it->second.last < pv->second.last)) pv = it;
       }
       if (pv == patterns.end()) return false;
+      // The plan leaves the device; its host side (analysis and tables)
+      // stays, so it comes back by an upload.  The arrays are freed outside
+      // the lock, the pattern busy until then.
       used -= pv->second.bytes;
-      plan_graveyard.push_back(std::move(pv->second.plan));
-      patterns.erase(pv);
+      pv->second.bytes    = 0;
+      pv->second.resident = false;
+      pv->second.busy     = true;
+      plan_graveyard.push_back(pv->second.plan);
       st.evictions++;
     }
     return true;
   }
 
   // ---- work (outside mu) ------------------------------------------------------
+  // Frees the device arrays of plans evicted by make_room and clears their
+  // patterns' busy flags.
+  void release_plans(std::vector<std::shared_ptr<Plan>> &plans) {
+    for (auto &pl : plans) pl->release_device();
+    if (!plans.empty()) {
+      std::lock_guard<std::mutex> lk(mu);
+      for (auto &pl : plans)
+        for (auto &pt : patterns)
+          if (pt.second.plan == pl) pt.second.busy = false;
+    }
+    plans.clear();
+    cv_work.notify_all();
+  }
+
   void finish(const ServerRequest &r, int status, int path, int batch, double t0,
               const Report &rep, const std::string &msg) {
     ServerResult res{};
@@ -201,18 +223,59 @@ struct Server::Impl {
     Solver                    *sv = nullptr;
     std::vector<std::unique_ptr<Solver>> graveyard;
     std::vector<std::shared_ptr<Plan>>   plan_graveyard;
+    // Plans evicted on this job's behalf leave the device however the job
+    // ends (after every lock of this function is released).
+    struct ReleaseAtExit {
+      Impl                               *self;
+      std::vector<std::shared_ptr<Plan>> *plans;
+      ~ReleaseAtExit() { self->release_plans(*plans); }
+    } release_at_exit{this, &plan_graveyard};
     auto fail_all = [&](int code, const std::string &msg) {
       for (const ServerRequest &q : job.reqs) finish(q, code, path, 1, t0, Report{}, msg);
     };
     try {
       MPIR_CUDA(cudaSetDevice(cfg.device));
       if (job.kind == Job::kAnalyse) {
+        // A pattern whose plan was evicted uploads its kept host tables
+        // again; one seen before without them takes its host analysis from
+        // the cache and only builds its plan again.
+        std::shared_ptr<Plan> kept;
+        {
+          std::lock_guard<std::mutex> lk(mu);
+          auto pt = patterns.find(r.pattern_key);
+          if (pt != patterns.end() && pt->second.plan && !pt->second.plan->on_device)
+            kept = pt->second.plan;
+        }
+        if (kept) {
+          const double tu = now_s();
+          cudaStream_t s  = nullptr;
+          MPIR_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+          try {
+            kept->upload_all(s);
+          } catch (...) {
+            cudaStreamDestroy(s);
+            throw;
+          }
+          cudaStreamDestroy(s);
+          plan = kept;
+          std::lock_guard<std::mutex> lk(mu);
+          make_room(plan->device_bytes(), graveyard, plan_graveyard);  // best effort
+          Pattern &p = patterns[r.pattern_key];
+          p.busy     = false;
+          p.resident = true;
+          p.bytes    = plan->device_bytes();
+          p.last     = now_s();
+          used += p.bytes;
+          st.plan_uploads++;
+          st.plan_ms += 1e3 * (p.last - tu);
+          st.peak_bytes = std::max<int64_t>(st.peak_bytes, used);
+        }
+      }
+      if (job.kind == Job::kAnalyse && !plan) {
         std::vector<int8_t> sign(r.n, 0);
         for (int64_t j = 0; j < r.n; j++)
           for (int64_t p = r.Ap[j]; p < r.Ap[j + 1]; p++)
             if (r.Ai[p] == j && r.Ax[p] > 0) sign[j] = 1;
-        // A pattern seen before (its plan since evicted) takes its host
-        // analysis from the cache and only uploads its plan again.
         std::shared_ptr<const Symbolic> cached;
         {
           std::lock_guard<std::mutex> lk(mu);
@@ -262,6 +325,7 @@ struct Server::Impl {
         Pattern &p = patterns[r.pattern_key];
         p.plan     = plan;
         p.busy     = false;
+        p.resident = true;
         p.bytes    = pb;
         p.last     = now_s();
         used += p.bytes;
@@ -303,7 +367,7 @@ struct Server::Impl {
           st.peak_bytes = std::max<int64_t>(st.peak_bytes, used);
         }
         graveyard.clear();
-        plan_graveyard.clear();
+        release_plans(plan_graveyard);
         const double tf     = now_s();
         auto solver = std::make_unique<Solver>(cfg.uf, kF64, cfg.ur, cfg.device);
         solver->ir_iter    = cfg.max_ir_iterations;

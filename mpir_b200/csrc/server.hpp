@@ -50,6 +50,7 @@ struct ServerStats {
   int64_t evictions = 0, resident_factors = 0, resident_patterns = 0, queued = 0;
   int64_t bytes_in_use = 0, peak_bytes = 0;
   int64_t analysis_reuses = 0;  // plans rebuilt from a cached host analysis
+  int64_t plan_uploads    = 0;  // evicted plans uploaded again from their host tables
   // Worker time (host wall clock, summed over workers) in the host analysis,
   // the plan build and upload, the factorizations (allocation included) and
   // the solves.
