@@ -257,6 +257,17 @@ int mpir_solver_luir(mpir_solver s, const double *b, double *x, int maxiter,
                      mpir_report *rep);
 int mpir_solver_luir_device(mpir_solver s, const double *d_b, double *d_x,
                             int maxiter, mpir_report *rep);
+
+/* r = b - A x for the solver's current values (original, unscaled matrix;
+ * b, x, r host arrays in caller order), the residual step of
+ * GmresLDLIR::Solve (gmres_ir.hpp:550-551: MatrixMultiply<UR> then
+ * VectorSubtract<UR>, ops.hpp:25-45 and :88-96) on the device: res_prec
+ * MPIR_F64 in float64, MPIR_DD in double-double arithmetic (each product
+ * exact, the sums in double-double) rounded to float64 at the end.
+ * *rinf (may be NULL) = max|r|.  Needs a successful factorization (the
+ * values are those it uploaded); MPIR_ERR_STATE before one. */
+int mpir_solver_residual(mpir_solver s, const double *b, const double *x, double *r,
+                         int res_prec, double *rinf);
 int mpir_luir_qdldl(int64_t n, const int64_t *Ap, const int64_t *Ai,
                     const double *Ax, const double *b, double *x,
                     int fact_prec, int maxiter, mpir_report *rep, int device);

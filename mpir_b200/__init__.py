@@ -140,6 +140,7 @@ def lib():
         "mpir_qdldl_ltsolve": (i32, [i64, vp, vp, vp, i32, vp, i32, i32]),
         "mpir_solver_dump_log": (i32, [vp, vp, i64, vp]),
         "mpir_solver_luir": (i32, [vp, vp, vp, i32, vp]),
+        "mpir_solver_residual": (i32, [vp, vp, vp, vp, i32, vp]),
         "mpir_solver_luir_device": (i32, [vp, vp, vp, i32, vp]),
         "mpir_luir_qdldl": (i32, [i64, vp, vp, vp, vp, vp, i32, i32, vp, i32]),
         "mpir_solver_info": (i32, [vp, vp]),
@@ -431,6 +432,18 @@ class GmresLDLIR:
         _check(lib().mpir_solver_luir(self._h, _p(b), _p(x), int(maxiter), C.byref(rep)))
         self.last_report = rep.as_dict()
         return x
+
+    def residual(self, b, x, prec="dd"):
+        """r = b - A x on the device for the current values (the residual
+        step of GmresLDLIR::Solve, gmres_ir.hpp:550-551) in float64 ("f64")
+        or double-double ("dd") arithmetic; returns r rounded to float64."""
+        b = _f64(b)
+        x = _f64(x)
+        r = np.zeros(self.n, np.float64)
+        rinf = C.c_double(0.0)
+        _check(lib().mpir_solver_residual(self._h, _p(b), _p(x), _p(r), _PREC[prec],
+                                          C.byref(rinf)))
+        return r
 
     def solve_device(self, d_b: int, d_x: int):
         """Device pointers (ints) in the caller's order."""

@@ -692,6 +692,20 @@ int mpir_solver_luir(mpir_solver s, const double *b, double *x, int maxiter, mpi
   });
 }
 
+int mpir_solver_residual(mpir_solver s, const double *b, const double *x, double *r,
+                         int res_prec, double *rinf) {
+  MPIR_NEED(s);
+  return guard([&]() -> int {
+    if (res_prec != MPIR_F64 && res_prec != MPIR_DD)
+      throw StatusError(MPIR_ERR_ARGUMENT, "res_prec must be MPIR_F64 or MPIR_DD");
+    if (s->impl->analyzed() && s->impl->plan().S.n > 0 && (!b || !x || !r))
+      throw StatusError(MPIR_ERR_ARGUMENT, "invalid argument");
+    const double m = s->impl->residual(b, x, r, res_prec == MPIR_DD);
+    if (rinf) *rinf = m;
+    return MPIR_OK;
+  });
+}
+
 int mpir_solver_luir_device(mpir_solver s, const double *d_b, double *d_x, int maxiter,
                             mpir_report *rep) {
   MPIR_NEED(s);

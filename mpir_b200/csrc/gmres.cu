@@ -566,6 +566,36 @@ int Solver::luir(const double *b, double *x, int maxiter, Report *rep) {
   return rc;
 }
 
+// The residual step of GmresLDLIR::Solve (gmres_ir.hpp:550-551 and :578-579:
+// MatrixMultiply then VectorSubtract, ops.hpp:25-45 and :88-96) in the
+// residual type, on its own: the k_spmv residual modes over the unscaled
+// values, with b and x gathered into the factor's order and r scattered
+// back.
+double Solver::residual(const double *b, const double *x, double *r, bool dd) {
+  if (!plan_) throw std::logic_error("residual before analyze");
+  if (!num_.valid) throw std::logic_error("residual before a successful factor");
+  MPIR_CUDA(cudaSetDevice(device));
+  ensure_vectors();
+  const Plan   &P = *plan_;
+  const int64_t n = P.S.n;
+  if (n == 0) return 0.0;
+  cudaStream_t   s    = stream_;
+  const int64_t *perm = P.perm.as<int64_t>();
+  const double  *AD   = num_.AD.as<double>();
+  MPIR_CUDA(cudaMemcpyAsync(hb_.as<void>(), b, n * sizeof(double), cudaMemcpyHostToDevice, s));
+  MPIR_CUDA(cudaMemcpyAsync(hx_.as<void>(), x, n * sizeof(double), cudaMemcpyHostToDevice, s));
+  vec_.rhs_in(perm, AD, hx_.as<double>(), t_.as<double>(), nullptr, x_.as<double>(), s);
+  vec_.rhs_in(perm, AD, hb_.as<double>(), t_.as<double>(), nullptr, bp_.as<double>(), s);
+  vec_.residual(P.Kp.as<int64_t>(), P.Kj.as<int32_t>(), num_.Korig.as<double>(),
+                x_.as<double>(), bp_.as<double>(), r_.as<double>(), dd, 0, s);
+  double rinf = 0;
+  vec_.read_inf(&rinf, 0, 1, s);
+  vec_.sol_out(perm, nullptr, r_.as<double>(), hx_.as<double>(), s);
+  MPIR_CUDA(cudaMemcpyAsync(r, hx_.as<void>(), n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  MPIR_CUDA(cudaStreamSynchronize(s));
+  return rinf;
+}
+
 // The solver log as JSON, the schema of GmresLDLIR::DumpLog
 // (gmres_ir.hpp:305-313, events of gmres_ir.hpp:539-632); clears the events.
 std::string Solver::dump_log() {

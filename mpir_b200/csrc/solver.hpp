@@ -99,6 +99,10 @@ class Solver {
   // Plain iterative refinement with the factor (LUIR_QDLDL); host and
   // device vectors.
   int luir(const double *b, double *x, int maxiter, Report *rep);
+  // r = b - A x on the original matrix (caller order, host vectors), in
+  // float64 or, with dd, in double-double rounded to float64; returns
+  // max|r|.  Needs the values of a successful factorization.
+  double residual(const double *b, const double *x, double *r, bool dd);
   int luir_device(const double *d_b, double *d_x, int maxiter, Report *rep);
   // The log of the solves since the last call, as JSON (GmresLDLIR::DumpLog).
   std::string dump_log();

@@ -392,13 +392,13 @@ __global__ void k_rhs_in(int64_t n, const int64_t *perm, const double *AD,
   warp_max_abs(inf, v, act);
 }
 
-// out[perm[i]] = x[i] * ADp[i].
+// out[perm[i]] = x[i] * ADp[i] (ADp NULL: out[perm[i]] = x[i]).
 __global__ void k_sol_out(int64_t n, const int64_t *perm, const double *ADp,
                           const double *x, double *out, int64_t vs) {
   x += blockIdx.y * vs;
   out += blockIdx.y * vs;
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i < n) out[perm[i]] = x[i] * ADp[i];
+  if (i < n) out[perm[i]] = ADp ? x[i] * ADp[i] : x[i];
 }
 
 // ---------------------------------------------------------------------------
