@@ -75,7 +75,7 @@ def parse():
     ap.add_argument("--gmres-iter", type=int, default=None)
     ap.add_argument("--ir-iter", type=int, default=None)
     # serving stream
-    ap.add_argument("--requests-per-step", type=int, default=16)
+    ap.add_argument("--requests-per-step", type=int, default=8)
     ap.add_argument("--workers", type=int, default=8)
     ap.add_argument("--budget-gb", type=float, default=150.0)
     ap.add_argument("--no-latency-pass", action="store_true")
@@ -815,7 +815,7 @@ def run_stream(args):
     clocks = Clocks(local)
     clocks.start()
     launches0 = mp.launch_count()
-    summ, recs, stats = replay.served(st, arrays, **srv_kw)
+    summ, recs, stats = replay.served(st, arrays, progress=30, **srv_kw)
     launches = mp.launch_count() - launches0
     clk = clocks.stop()
     seconds = rank_max(pg, summ["seconds"], dev)
@@ -826,13 +826,13 @@ def run_stream(args):
     if not args.no_latency_pass:
         rate = 0.5 * summ["solves_per_s"]
         st.retime(rate, seed=replica_seed(args.seed, rank) + 7)
-        lsum, lrecs, _ = replay.served(st, arrays, check=False, **srv_kw)
+        lsum, lrecs, _ = replay.served(st, arrays, check=False, progress=30, **srv_kw)
         lat_pass = {"rate_per_s": rate, "p50_ms": lsum["p50_ms"], "p99_ms": lsum["p99_ms"],
                     "solves_per_s": lsum["solves_per_s"]}
         st.retime(1e4, seed=replica_seed(args.seed, rank))
     drop = None
     if not args.no_dropin:
-        dsum, drecs = replay.dropin(st, arrays, uf="f32")
+        dsum, drecs = replay.dropin(st, arrays, uf="f32", progress=30)
         d_seconds = rank_max(pg, dsum["seconds"], dev)
         d_completed = rank_sum(pg, dsum["completed"], dev)
         drop = {"solves_per_s": d_completed / d_seconds, "p50_ms": dsum["p50_ms"],

@@ -358,8 +358,9 @@ int mpir_group_destroy(mpir_group g);
  * does not fit the device-memory budget), solves the queued requests on one
  * factor together (up to max_batch right-hand sides in lockstep, as
  * mpir_solver_solve_batch), and runs requests on different factors
- * concurrently.  A request whose factor alone exceeds the budget is refused
- * (status MPIR_ERR_NOMEM in its result). */
+ * concurrently.  A request whose factor alone exceeds the budget, or that
+ * finds no room while every other running job waits for room too, or for
+ * two minutes, is refused (status MPIR_ERR_NOMEM in its result). */
 typedef struct mpir_server_s *mpir_server;
 
 typedef struct mpir_server_config {

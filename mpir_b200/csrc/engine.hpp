@@ -179,7 +179,9 @@ class Numeric {
   int             graph_mode     = -2;
   int64_t         graph_launches = 0;
   // Trailing-update engine: -1 float32 SIMT, 0 bfloat16 tensor cores,
-  // 1 3xTF32 tensor cores, 2 float16 tensor cores.
+  // 1 3xTF32 tensor cores, 2 float16 tensor cores, 3 3xBF16 tensor cores.
+  // The panel solves run on the tensor cores (3xTF32) with every tensor-core
+  // engine, on the SIMT units with the SIMT engine or MPIR_TRSM=simt.
   int          update_mode = -1;
 
   void allocate(const Plan &P);
@@ -225,6 +227,10 @@ void launch_convert_b(const GemmProb *probs, int nprob, int convs, const float *
                       const float *packd, float *bconv, cudaStream_t s);
 // Tensor-core GEMM CTAs resident per SM (shared-memory bound).
 int  tc_ctas_per_sm();
+// Panel solves of a block step on the tensor cores (3xTF32), one CTA per
+// 128-row tile; the same outputs as k_step_gemm<true>.
+void launch_trsm_tc(const StepDesc *descs, int ndesc, int tiles, float *panel, const float *linv,
+                    const float *Dinv, float *pack, FactorStatus *st, cudaStream_t s);
 // Streaming multiprocessors of a B200.
 constexpr int kSMs = 148;
 

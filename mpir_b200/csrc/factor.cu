@@ -22,6 +22,8 @@
 #include <algorithm>
 #include <climits>
 #include <cmath>
+#include <cstdlib>
+#include <string>
 
 #include "common.cuh"
 #include "engine.hpp"
@@ -1483,6 +1485,11 @@ void Numeric::run(const Plan &P, const double *d_Ax, double eps, cudaStream_t s)
   MPIR_CHECK_LAUNCH();
   float        *pan = panel.as<float>(), *ua = uarena.as<float>();
   FactorStatus *st  = status.as<FactorStatus>();
+  static const bool trsm_simt_env = [] {
+    const char *e = std::getenv("MPIR_TRSM");
+    return e != nullptr && std::string(e) == "simt";
+  }();
+  const bool trsm_tc = update_mode >= 0 && !trsm_simt_env;
   static std::atomic<bool> trsm_attr{false};
   const int     trsm_smem = kBM * (kBN + 1) * sizeof(float);
   if (!trsm_attr) {
@@ -1559,8 +1566,12 @@ void Numeric::run(const Plan &P, const double *d_Ax, double eps, cudaStream_t s)
       kt.end(s);
       if (stp.trsm_tiles > 0) {
         kt.begin(kKcTrsm, s);
-        launch(k_step_gemm<true>, stp.trsm_tiles, kGemmThreads, trsm_smem, s, 
-            dd, stp.count, pan, ua, linv.as<float>(), Dinv.as<float>(), pack.as<float>());
+        if (trsm_tc)
+          launch_trsm_tc(dd, stp.count, stp.trsm_tiles, pan, linv.as<float>(), Dinv.as<float>(),
+                         pack.as<float>(), st, s);
+        else
+          launch(k_step_gemm<true>, stp.trsm_tiles, kGemmThreads, trsm_smem, s, dd, stp.count,
+                 pan, ua, linv.as<float>(), Dinv.as<float>(), pack.as<float>());
         kt.end(s);
       }
     }

@@ -15,8 +15,10 @@
 //             pattern's captured graph) and a solve;
 //   admission every plan and factor is charged its device bytes against the
 //             budget; a factor that does not fit evicts the least recently
-//             used idle factors (then idle plans) first, and a request whose
-//             footprint exceeds the whole budget is refused with
+//             used idle factors (then idle plans) first (freed before the
+//             job waits or tries again), and a request whose footprint
+//             exceeds the whole budget, or that finds no room while no other
+//             job runs on or within two minutes, is refused with
 //             MPIR_ERR_NOMEM;
 //   batching  worker threads, each driving its own CUDA stream, take the
 //             oldest request whose pattern and factor are idle, together with
@@ -89,6 +91,9 @@ struct Server::Impl {
   ServerStats                          st{};
   size_t                               used    = 0;
   int                                  running = 0;
+  int                                  waiting_room = 0;  // jobs waiting in admission
+  // A factor that finds no room for this long is refused (MPIR_ERR_NOMEM).
+  static constexpr double              kAdmitWaitSeconds = 120.0;
   int64_t                              next_id = 1;
   bool                                 stop    = false;
 
@@ -223,6 +228,7 @@ struct Server::Impl {
     Solver                    *sv = nullptr;
     std::vector<std::unique_ptr<Solver>> graveyard;
     std::vector<std::shared_ptr<Plan>>   plan_graveyard;
+    size_t                               reserved = 0;  // admitted bytes not yet a factor's
     // Plans evicted on this job's behalf leave the device however the job
     // ends (after every lock of this function is released).
     struct ReleaseAtExit {
@@ -352,18 +358,36 @@ struct Server::Impl {
             st.refused += static_cast<int64_t>(job.reqs.size());
             return;
           }
-          while (!make_room(need, graveyard, plan_graveyard)) {
-            if (running <= 1) {  // nothing else will free memory
+          const double t_wait = now_s();
+          for (;;) {
+            if (make_room(need, graveyard, plan_graveyard)) break;
+            if (!graveyard.empty() || !plan_graveyard.empty()) {
+              // What was evicted leaves the device before this job waits or
+              // tries again (the budget already counts it as free).
+              lk.unlock();
+              graveyard.clear();
+              release_plans(plan_graveyard);
+              lk.lock();
+              continue;
+            }
+            // Memory comes free only from jobs that run on: none other than
+            // those waiting for room themselves (or the wait ran too long).
+            const bool none_active = running - waiting_room <= 1;
+            if (none_active || now_s() - t_wait > kAdmitWaitSeconds) {
               factors.erase(k);
               lk.unlock();
-              fail_all(-4, "admission budget held by resident plans");
+              fail_all(-4, none_active ? "admission budget held by resident plans"
+                                       : "admission wait exceeded");
               std::lock_guard<std::mutex> lk2(mu);
               st.refused += static_cast<int64_t>(job.reqs.size());
               return;
             }
+            waiting_room++;
             cv_done.wait_for(lk, std::chrono::milliseconds(20));
+            waiting_room--;
           }
           used += need;  // reserved; corrected to the measured bytes below
+          reserved = need;
           st.peak_bytes = std::max<int64_t>(st.peak_bytes, used);
         }
         graveyard.clear();
@@ -384,6 +408,7 @@ struct Server::Impl {
           Factor &f = factors[k];
           f.bytes   = solver->device_bytes();
           used      = used - need + f.bytes;
+          reserved  = 0;
           f.solver  = std::move(solver);
           f.valid   = fr == kOk;
           f.last    = now_s();
@@ -446,6 +471,7 @@ struct Server::Impl {
                        static_cast<const CudaError &>(e).code == cudaErrorMemoryAllocation;
       {
         std::lock_guard<std::mutex> lk(mu);
+        used -= reserved;
         auto f = factors.find(k);
         if (f != factors.end()) {
           if (f->second.solver) {

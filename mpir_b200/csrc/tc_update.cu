@@ -660,6 +660,227 @@ void launch_convert_b(const GemmProb *probs, int nprob, int convs, const float *
   if (convs > 0) launch(k_convert_b, convs, 256, 0, s, probs, nprob, pack, packd, bconv);
 }
 
+// ---------------------------------------------------------------------------
+// Panel solve of a block step on the tensor cores (3xTF32):
+//   W = F X^T diag(Dinv)
+// for one 128-row tile of the rows below the step's diagonal block: F the
+// tile's nbk columns of the panel, X the inverse of the block's unit-lower
+// factor (linv, column-major, leading dimension kNB), Dinv the block's
+// pivots' reciprocals.  Outputs as k_step_gemm<true>: W over F in the panel
+// and, as whole K-groups, into the packed front.
+//
+// Shared memory (K-major core-matrix layout, K-group g at g * 2048 bytes,
+// row m at m * 16): B = X diag(Dinv) in tf32 high and low parts for all 128
+// columns of K (2 x 64 KB), A in halves of 64 columns (high and low parts,
+// 2 x 32 KB).  All 256 threads convert: B, then A's first half; one lane
+// issues its 8 x 3 MMAs (M = N = 128, K = 8) and commits; the threads load
+// A's second half into registers meanwhile and write it once the commit
+// shows the first half's MMAs done.  Epilogue: warps w and w + 4 drain
+// tensor-memory lanes 32 (w % 4) .. (rows), columns 0-63 and 64-127.
+namespace tc {
+constexpr uint32_t kTrsmB     = 32 * kGroup;           // one part of B (bytes)
+constexpr uint32_t kTrsmA     = 16 * kGroup;           // one part of an A half
+constexpr uint32_t kTrsmSmem  = 2 * kTrsmB + 2 * kTrsmA;  // 192 KB
+}  // namespace tc
+
+__global__ void __launch_bounds__(256, 1)
+    k_trsm_tc(const StepDesc *descs, int ndesc, float *panel, const float *linv,
+              const float *Dinv, float *pack, FactorStatus *st) {
+  using namespace tc;
+  extern __shared__ __align__(1024) uint8_t smem[];
+  __shared__ __align__(8) uint64_t done_bar;
+  __shared__ uint32_t tmem_slot;
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+  const int t   = blockIdx.x;
+  int       lo = 0, hi = ndesc - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    if (descs[mid].trsm_tile0 <= t) lo = mid; else hi = mid - 1;
+  }
+  const StepDesc d  = descs[lo];
+  const int      m0 = (t - d.trsm_tile0) * kTileM;
+  const int64_t  h  = d.h;
+  const int      kb = d.kb, nbk = d.nbk, w = d.w;
+  const int      M  = static_cast<int>(h) - kb - nbk;
+  float         *C  = panel + d.panel + (kb + nbk) + static_cast<int64_t>(kb) * h;
+  const float   *X  = linv + d.linv;
+  const uint32_t bar   = smem_u32(&done_bar);
+  const uint32_t sbase = smem_u32(smem);
+
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 ::"r"(smem_u32(&tmem_slot)), "r"(kTmemCols) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+
+  // Thread (row m, K-group pair) of a half: m = tid % 128, K-groups
+  // tid / 128 + 2 i of the half, i < 8.
+  const int  m    = tid & 127;
+  const int  gsel = tid >> 7;
+  const bool rok  = m0 + m < M;
+  auto load_a = [&](int half, float (&v)[32]) {
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const int k = 64 * half + 4 * (gsel + 2 * i) + j;
+        v[4 * i + j] = (rok && k < nbk) ? C[m0 + m + static_cast<int64_t>(k) * h] : 0.0f;
+      }
+  };
+  auto store_a = [&](const float (&v)[32]) {
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const float av[4] = {v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]};
+      uint4       ah, al;
+      split4(av, ah, al);
+      const uint32_t o = (gsel + 2 * i) * kGroup + m * 16;
+      *reinterpret_cast<uint4 *>(smem + 2 * kTrsmB + o)          = ah;
+      *reinterpret_cast<uint4 *>(smem + 2 * kTrsmB + kTrsmA + o) = al;
+    }
+  };
+  float a[32];
+  load_a(0, a);
+  // B = X diag(Dinv): thread (row n = m, K-groups gsel + 2 i, i < 16), in two
+  // batches of 8 K-groups (all loads of a batch first).
+  {
+    const float dv = m < nbk ? Dinv[static_cast<int64_t>(d.col0) + kb + m] : 0.0f;
+#pragma unroll
+    for (int bt = 0; bt < 2; bt++) {
+      float xv[32];
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          const int k = 4 * (gsel + 2 * (8 * bt + i)) + j;
+          xv[4 * i + j] = X[m + k * kNB];
+        }
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        const float bv[4] = {xv[4 * i] * dv, xv[4 * i + 1] * dv, xv[4 * i + 2] * dv,
+                             xv[4 * i + 3] * dv};
+        uint4       bh, bl;
+        split4(bv, bh, bl);
+        const uint32_t o = (gsel + 2 * (8 * bt + i)) * kGroup + m * 16;
+        *reinterpret_cast<uint4 *>(smem + o)          = bh;
+        *reinterpret_cast<uint4 *>(smem + kTrsmB + o) = bl;
+      }
+    }
+  }
+  store_a(a);
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem   = tmem_slot;
+  const int      halves = nbk > 64 ? 2 : 1;
+  const uint32_t idesc  = make_idesc(kFmtTF32);
+  auto issue = [&](int half) {
+    if (tid != 32) return;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const uint32_t ao  = 2 * kTrsmB + q * 2 * kGroup;
+      const uint32_t bo  = (16 * half + 2 * q) * kGroup;
+      const uint64_t ahd = make_desc(sbase + ao), ald = make_desc(sbase + ao + kTrsmA);
+      const uint64_t bhd = make_desc(sbase + bo), bld = make_desc(sbase + bo + kTrsmB);
+      mma<true>(tmem, ahd, bhd, idesc, (half > 0 || q > 0) ? 1u : 0u);
+      mma<true>(tmem, ahd, bld, idesc, 1u);
+      mma<true>(tmem, ald, bhd, idesc, 1u);
+    }
+    commit(bar);
+  };
+  issue(0);
+  bool ok = true;
+  if (halves == 2) {
+    load_a(1, a);
+    ok = wait_bounded(bar, 0);  // the first half's MMAs have read A
+    if (ok) {
+      store_a(a);
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    ok = __syncthreads_and(ok);
+    if (ok) issue(1);
+  }
+  ok = ok && wait_bounded(bar, (halves - 1) & 1);
+  ok = __syncthreads_and(ok);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (ok) {
+    const int lr = (warp & 3) * 32 + lane;  // tile row of this thread's lane
+    const int r  = m0 + lr;
+    float    *pk = pack != nullptr && d.pk >= 0 ? pack + d.pk : nullptr;
+    int64_t   prow = 0;
+    if (pk) {
+      const int rf = kb + nbk + r;  // row of the front
+      const int p  = rf < w ? rf : rf - w + d.pk_wt;
+      prow = static_cast<int64_t>(p >> 7) * d.pk_g * PackedFront::kGroupFloats + (p & 127) * 4;
+    }
+#pragma unroll
+    for (int cc = 0; cc < 2; cc++) {
+      const int cb = (warp >> 2) * 2 + cc;  // 32-column block
+      if (cb * 32 >= nbk) break;
+      uint32_t       v[32];
+      const uint32_t taddr = tmem + (static_cast<uint32_t>((warp & 3) * 32) << 16) + cb * 32;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+          "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+          "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+            "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
+            "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]),
+            "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+            "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
+            "=r"(v[30]), "=r"(v[31])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (r < M) {
+#pragma unroll
+        for (int q = 0; q < 32; q++) {
+          const int c = cb * 32 + q;
+          if (c < nbk) C[r + static_cast<int64_t>(c) * h] = __uint_as_float(v[q]);
+        }
+        if (pk) {
+#pragma unroll
+          for (int q = 0; q < 8; q++) {
+            const int c0 = cb * 32 + 4 * q;
+            if (c0 >= nbk) break;
+            float4 o;
+            o.x = __uint_as_float(v[4 * q + 0]);
+            o.y = __uint_as_float(v[4 * q + 1]);
+            o.z = __uint_as_float(v[4 * q + 2]);
+            o.w = __uint_as_float(v[4 * q + 3]);
+            *reinterpret_cast<float4 *>(pk + prow +
+                                        static_cast<int64_t>((kb + c0) >> 2) *
+                                            PackedFront::kGroupFloats) = o;
+          }
+        }
+      }
+    }
+  } else if (tid == 0) {
+    atomicExch(&st->timeout, 1);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 1)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kTmemCols) : "memory");
+}
+
+void launch_trsm_tc(const StepDesc *descs, int ndesc, int tiles, float *panel, const float *linv,
+                    const float *Dinv, float *pack, FactorStatus *st, cudaStream_t s) {
+  if (tiles <= 0) return;
+  static std::atomic<bool> attr{false};
+  if (!attr) {
+    MPIR_CUDA(cudaFuncSetAttribute(k_trsm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(tc::kTrsmSmem)));
+    attr = true;
+  }
+  launch(k_trsm_tc, tiles, 256, tc::kTrsmSmem, s, descs, ndesc, panel, linv, Dinv, pack, st);
+}
+
 template <int MODE>
 static void launch_mode(const GemmProb *probs, int nprob, int units, const float *pack,
                         const float *packd, const float *packs, const float *bconv,

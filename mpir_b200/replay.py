@@ -41,8 +41,13 @@ def _summary(records, t_total):
                                      default=float("nan"))}
 
 
-def served(stream, arrays, check=True, **server_kwargs):
-    """(summary, records, server stats)."""
+def served(stream, arrays, check=True, progress=None, **server_kwargs):
+    """(summary, records, server stats).  The errors of each result are
+    computed after the last one arrived (outside the timed span);
+    ``progress`` (seconds) prints the engine's counters to stderr that
+    often while the stream runs."""
+    import sys
+
     import mpir_b200 as mp
     srv = mp.Server(**server_kwargs)
     reqs = stream.requests
@@ -59,16 +64,34 @@ def served(stream, arrays, check=True, **server_kwargs):
             if i == 0:
                 ready.set()
 
+    finished = threading.Event()
+
+    def reporter(t0):
+        while not finished.wait(progress):
+            c = srv.stats()
+            print(f"[served] {time.perf_counter() - t0:7.1f}s completed {c['completed']}"
+                  f"/{len(reqs)} failed {c['failed']} queued {c['queued']} factors "
+                  f"{c['resident_factors']} in use {c['bytes_in_use'] / 1e9:.1f} GB "
+                  f"evictions {c['evictions']}", file=sys.stderr, flush=True)
+
     t0 = time.perf_counter()
     th = threading.Thread(target=submitter, args=(t0,), daemon=True)
     th.start()
-    records = []
+    if progress:
+        threading.Thread(target=reporter, args=(t0,), daemon=True).start()
+    results = []
     t_last = t0
-    for i, r in enumerate(reqs):
+    for i in range(len(reqs)):
         while ids[i] is None:
             time.sleep(0.0002)
-        x, res = srv.wait(ids[i])
+        results.append(srv.wait(ids[i]))
         t_last = max(t_last, time.perf_counter())
+    finished.set()
+    th.join()
+    stats = srv.stats()
+    srv.close()
+    records = []
+    for i, (r, (x, res)) in enumerate(zip(reqs, results)):
         rec = {"index": i, "kind": r.kind, "status": res["status"], "path": res["path"],
                "batch": res["batch"], "latency_ms": res["latency_ms"],
                "queue_ms": res["queue_ms"], "n": arrays[i][0].n,
@@ -79,20 +102,26 @@ def served(stream, arrays, check=True, **server_kwargs):
             rec["backward_error"] = kkt.backward_error(s.n, s.Ap, s.Ai, Ax, x, b)
             rec["forward_error"] = kkt.forward_error(x, xt)
         records.append(rec)
-    th.join()
-    stats = srv.stats()
-    srv.close()
     t_first = t0 + reqs[0].t_arrival
     return _summary(records, t_last - t_first), records, stats
 
 
-def dropin(stream, arrays, uf="f32", ir_iter=10, gmres_iter=10, tol=1e-10, check=True):
-    """(summary, records): one request at a time, nothing kept between them."""
+def dropin(stream, arrays, uf="f32", ir_iter=10, gmres_iter=10, tol=1e-10, check=True,
+           progress=None):
+    """(summary, records): one request at a time, nothing kept between them;
+    ``progress`` (seconds) prints the count done to stderr about that often."""
+    import sys
+
     import mpir_b200 as mp
     records = []
     done_prev = 0.0
     busy = 0.0
+    t_print = time.perf_counter()
     for i, r in enumerate(stream.requests):
+        if progress and time.perf_counter() - t_print >= progress:
+            t_print = time.perf_counter()
+            print(f"[drop-in] {i}/{len(stream.requests)} requests, {busy:.1f}s of service",
+                  file=sys.stderr, flush=True)
         s, Ax, b, xt = arrays[i]
         t0 = time.perf_counter()
         status = 0
