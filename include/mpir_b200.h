@@ -59,7 +59,9 @@ typedef struct mpir_report {
   int32_t spmv_count;       /* products with K */
   int32_t reorth_count;     /* Brown/Hindmarsh re-orthogonalisations */
   int32_t stop_reason;      /* 0 iteration cap, 1 small update, 2 stagnation,
-                               3 zero residual, 4 non-finite residual */
+                               3 zero residual, 4 non-finite residual or
+                               factor (a pivot beyond the factor type's
+                               range; x is then the first solve's) */
   int32_t factor_prec;      /* MPIR_F32 / MPIR_BF16 / MPIR_F16: the type the
                                factor was computed and applied in (MPIR_F32
                                for a solver created with UF = MPIR_F64) */

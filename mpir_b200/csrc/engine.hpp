@@ -172,6 +172,7 @@ class Numeric {
   DeviceBuffer AD, Axs, Kval, Korig, Ax;
   double       eps_uf = 0;
   bool         valid  = false;
+  bool         nonfinite = false;  // a pivot of the last factor is not finite
   // Captured factorization (run_graph) and what it was captured for.
   cudaGraphExec_t graph          = nullptr;
   const double   *graph_ax       = nullptr;

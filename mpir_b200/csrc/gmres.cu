@@ -177,6 +177,7 @@ int Solver::factor_device(const double *d_Ax) {
   int32_t zc  = 0;
   bool    bad = false;
   last_npos   = num_.result(stream_, &zc, &bad);
+  num_.nonfinite = bad;
   float ms    = 0;
   MPIR_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
   last_factor_ms = ms;
@@ -219,7 +220,9 @@ cudaGraph_t Solver::record_factor(int64_t *launches) {
 
 int Solver::finish_recorded_factor(double ms) {
   num_.eps_uf    = eps_of(uf);
-  last_npos      = num_.result(stream_);
+  bool bad       = false;
+  last_npos      = num_.result(stream_, nullptr, &bad);
+  num_.nonfinite = bad;
   last_factor_ms = ms;
   num_.valid     = last_npos >= 0;
   if (last_npos < 0) return last_npos == -5 ? -5 : kBadInput;
@@ -400,7 +403,8 @@ int Solver::solve_device(const double *d_b, double *d_x, Report *rep) {
       st.stop_reason = 3;
       break;
     }
-    if (!std::isfinite(scale)) {  // a non-finite factor or input
+    // a non-finite input, or a factor with a pivot beyond its type's range
+    if (!std::isfinite(scale) || num_.nonfinite) {
       st.stop_reason = 4;
       break;
     }
@@ -604,7 +608,7 @@ std::string Solver::dump_log() {
                                   "non_finite_residual"};
   static const char *details[] = {"", "d_norm <= x_norm * (10*eps)",
                                   "abs(r_norm - r_norm_prev) < tol", "r == 0",
-                                  "r is not finite"};
+                                  "r or the factor is not finite"};
   auto num = [](double v) {
     if (!std::isfinite(v)) return std::string("null");
     char b[64];

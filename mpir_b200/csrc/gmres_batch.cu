@@ -374,7 +374,7 @@ int Solver::solve_batch_device(int nrhs, const double *d_B, double *d_X, Report 
       if (scale == 0.0) {  // exact: nothing left to refine
         st[k].stop_reason = 3;
         act[k]            = 0;
-      } else if (!std::isfinite(scale)) {
+      } else if (!std::isfinite(scale) || num_.nonfinite) {
         st[k].stop_reason = 4;
         act[k]            = 0;
       } else {
