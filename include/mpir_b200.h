@@ -412,6 +412,7 @@ typedef struct mpir_server_stats {
   /* worker wall time summed over workers: host analysis, plan build and
    * upload, factorizations (allocation included), solves */
   double analysis_ms, plan_ms, factor_ms, solve_ms;
+  double factor_device_ms, solve_device_ms;  /* CUDA-event time of those */
 } mpir_server_stats;
 
 int mpir_server_create(mpir_server *out, const mpir_server_config *cfg);

@@ -1081,6 +1081,8 @@ int mpir_server_get_stats(mpir_server s, mpir_server_stats *out) {
     out->plan_ms           = st.plan_ms;
     out->factor_ms         = st.factor_ms;
     out->solve_ms          = st.solve_ms;
+    out->factor_device_ms  = st.factor_device_ms;
+    out->solve_device_ms   = st.solve_device_ms;
     return MPIR_OK;
   });
 }

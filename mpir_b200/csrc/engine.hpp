@@ -11,6 +11,15 @@
 
 namespace mpir {
 
+// Stream-ordered device memory (memory.cu): an allocation on the current
+// device (its device returned in *device), usable from every stream once
+// this returns; a free that does not wait for the device (the caller's work
+// on the buffer has completed); the device's free memory counting what the
+// pool holds unused.
+void  *device_alloc(size_t bytes, int *device);
+void   device_free(void *p, int device);
+size_t device_free_bytes(int device);
+
 // Owning device allocation.
 class DeviceBuffer {
  public:
@@ -19,7 +28,7 @@ class DeviceBuffer {
   ~DeviceBuffer() { release(); }
   DeviceBuffer(const DeviceBuffer &)            = delete;
   DeviceBuffer &operator=(const DeviceBuffer &) = delete;
-  DeviceBuffer(DeviceBuffer &&o) noexcept : p_(o.p_), bytes_(o.bytes_) {
+  DeviceBuffer(DeviceBuffer &&o) noexcept : p_(o.p_), bytes_(o.bytes_), dev_(o.dev_) {
     o.p_     = nullptr;
     o.bytes_ = 0;
   }
@@ -28,6 +37,7 @@ class DeviceBuffer {
       release();
       p_       = o.p_;
       bytes_   = o.bytes_;
+      dev_     = o.dev_;
       o.p_     = nullptr;
       o.bytes_ = 0;
     }
@@ -35,11 +45,11 @@ class DeviceBuffer {
   }
   void resize(size_t bytes) {
     release();
-    if (bytes) MPIR_CUDA(cudaMalloc(&p_, bytes));
+    if (bytes) p_ = device_alloc(bytes, &dev_);
     bytes_ = bytes;
   }
   void release() {
-    if (p_) cudaFree(p_);
+    if (p_) device_free(p_, dev_);
     p_     = nullptr;
     bytes_ = 0;
   }
@@ -52,6 +62,7 @@ class DeviceBuffer {
  private:
   void  *p_     = nullptr;
   size_t bytes_ = 0;
+  int    dev_   = 0;
 };
 
 template <class T>

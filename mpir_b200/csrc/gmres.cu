@@ -100,9 +100,7 @@ void Solver::adopt(std::shared_ptr<Plan> P) {
   if (num_.store_prec == 2) {
     // The 16-bit copy sits beside the float32 panels during factorization;
     // where both do not fit, the solves read the float32 panels instead.
-    size_t free_b = 0, total_b = 0;
-    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess &&
-        Numeric::bytes_for(*plan_, 2) > free_b / 100 * 97)
+    if (Numeric::bytes_for(*plan_, 2) > device_free_bytes(device) / 100 * 97)
       num_.store_prec = 1;
   }
   num_.allocate(*plan_);

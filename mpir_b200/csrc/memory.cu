@@ -1,0 +1,102 @@
+// Device memory of the engine: stream-ordered allocations from each device's
+// default memory pool.
+//
+// cudaFree waits for the whole device; with several host threads each
+// driving its own stream (the serving engine), every free would stall every
+// other thread's work.  Allocations here are cudaMallocAsync on one
+// allocation stream per device, made visible to all streams by a
+// synchronisation of that stream alone; frees are cudaFreeAsync on it and do
+// not wait.  The engine frees a buffer only once the work that used it has
+// completed (its owner synchronised its streams), so the pool may hand the
+// memory out again at once.  Freed memory stays in the pool (release
+// threshold at its maximum); an allocation that does not fit first returns
+// the pool's unused memory to the device and tries once more.
+#include <cstdint>
+#include <mutex>
+
+#include "engine.hpp"
+
+namespace mpir {
+
+namespace {
+constexpr int  kMaxDevices = 64;
+std::once_flag g_once[kMaxDevices];
+cudaStream_t   g_stream[kMaxDevices];
+
+cudaStream_t alloc_stream(int d) {
+  if (d < 0 || d >= kMaxDevices) throw CudaError(cudaErrorInvalidDevice, "allocation stream");
+  std::call_once(g_once[d], [d] {
+    cudaMemPool_t pool;
+    MPIR_CUDA(cudaDeviceGetDefaultMemPool(&pool, d));
+    uint64_t keep = UINT64_MAX;
+    MPIR_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    MPIR_CUDA(cudaStreamCreateWithFlags(&g_stream[d], cudaStreamNonBlocking));
+  });
+  return g_stream[d];
+}
+
+// Makes device d current for the scope.
+struct OnDevice {
+  int prev = -1;
+  explicit OnDevice(int d) {
+    cudaGetDevice(&prev);
+    if (prev != d) cudaSetDevice(d);
+  }
+  ~OnDevice() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+}  // namespace
+
+void *device_alloc(size_t bytes, int *device) {
+  int d = 0;
+  MPIR_CUDA(cudaGetDevice(&d));
+  cudaStream_t s = alloc_stream(d);
+  void        *p = nullptr;
+  cudaError_t  e = cudaMallocAsync(&p, bytes, s);
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    cudaMemPool_t pool;
+    MPIR_CUDA(cudaStreamSynchronize(s));
+    MPIR_CUDA(cudaDeviceGetDefaultMemPool(&pool, d));
+    MPIR_CUDA(cudaMemPoolTrimTo(pool, 0));
+    e = cudaMallocAsync(&p, bytes, s);
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    throw CudaError(e, "cudaMallocAsync");
+  }
+  MPIR_CUDA(cudaStreamSynchronize(s));  // usable from every stream from here on
+  *device = d;
+  return p;
+}
+
+void device_free(void *p, int device) {
+  if (!p) return;
+  OnDevice on(device);
+  // Errors are ignored: a free at process exit may come after the context.
+  if (cudaFreeAsync(p, alloc_stream(device)) != cudaSuccess) cudaGetLastError();
+}
+
+size_t device_free_bytes(int device) {
+  OnDevice on(device);
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  // memory the pool holds but no buffer uses is free for the engine too
+  cudaMemPool_t pool;
+  uint64_t      reserved = 0, used = 0;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess &&
+      cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess &&
+      cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess &&
+      reserved > used)
+    free_b += static_cast<size_t>(reserved - used);
+  cudaGetLastError();
+  return free_b;
+}
+
+}  // namespace mpir

@@ -400,6 +400,7 @@ struct Server::Impl {
         solver->update_engine = cfg.update;
         solver->adopt(plan);
         const int fr = solver->factor(r.Ax);
+        const double sv_factor_ms = solver->last_factor_ms;
         // A resident factor keeps only what the solves read.
         MPIR_CUDA(cudaStreamSynchronize(solver->stream()));
         solver->trim();
@@ -415,6 +416,7 @@ struct Server::Impl {
           patterns[r.pattern_key].factors++;
           st.factorizations++;
           st.factor_ms += 1e3 * (now_s() - tf);
+          st.factor_device_ms += sv_factor_ms;
           st.peak_bytes = std::max<int64_t>(st.peak_bytes, used);
           sv = f.solver.get();
         }
@@ -456,6 +458,7 @@ struct Server::Impl {
         patterns[r.pattern_key].last = f.last;
         st.solves++;
         st.solve_ms += 1e3 * (now_s() - ts);
+        st.solve_device_ms += reps[0].solve_ms;  // a batch reports its whole time in each
         if (nb > 1) {
           st.batched_solves++;
           st.batched_rhs += nb;

@@ -55,6 +55,8 @@ struct ServerStats {
   // the plan build and upload, the factorizations (allocation included) and
   // the solves.
   double analysis_ms = 0, plan_ms = 0, factor_ms = 0, solve_ms = 0;
+  // Device time (CUDA events) of the factorizations and of the solves.
+  double factor_device_ms = 0, solve_device_ms = 0;
 };
 
 class Server {
