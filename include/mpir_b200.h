@@ -413,6 +413,9 @@ typedef struct mpir_server_stats {
    * upload, factorizations (allocation included), solves */
   double analysis_ms, plan_ms, factor_ms, solve_ms;
   double factor_device_ms, solve_device_ms;  /* CUDA-event time of those */
+  double setup_ms, trim_ms;  /* parts of factor_ms: a new factor's solver and
+                                resident buffers; the release of its
+                                factorization scratch afterwards */
 } mpir_server_stats;
 
 int mpir_server_create(mpir_server *out, const mpir_server_config *cfg);

@@ -93,7 +93,8 @@ class ServerStats(C.Structure):
         "batched_solves", "batched_rhs", "evictions", "resident_factors", "resident_patterns",
         "queued", "bytes_in_use", "peak_bytes", "analysis_reuses", "plan_uploads")] + [
         (k, C.c_double) for k in ("analysis_ms", "plan_ms", "factor_ms", "solve_ms",
-                                  "factor_device_ms", "solve_device_ms")]
+                                  "factor_device_ms", "solve_device_ms", "setup_ms",
+                                  "trim_ms")]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -1083,6 +1083,8 @@ int mpir_server_get_stats(mpir_server s, mpir_server_stats *out) {
     out->solve_ms          = st.solve_ms;
     out->factor_device_ms  = st.factor_device_ms;
     out->solve_device_ms   = st.solve_device_ms;
+    out->setup_ms          = st.setup_ms;
+    out->trim_ms           = st.trim_ms;
     return MPIR_OK;
   });
 }

@@ -11,7 +11,10 @@
 // memory out again at once.  Freed memory stays in the pool (release
 // threshold at its maximum); an allocation that does not fit first returns
 // the pool's unused memory to the device and tries once more.
+// MPIR_ALLOC=sync selects plain cudaMalloc / cudaFree instead.
 #include <cstdint>
+#include <cstdlib>
+#include <cstring>
 #include <mutex>
 
 #include "engine.hpp"
@@ -48,11 +51,25 @@ struct OnDevice {
     if (prev >= 0 && cur != prev) cudaSetDevice(prev);
   }
 };
+
+bool use_pool() {
+  static const bool pool = [] {
+    const char *e = std::getenv("MPIR_ALLOC");
+    return e == nullptr || std::strcmp(e, "sync") != 0;
+  }();
+  return pool;
+}
 }  // namespace
 
 void *device_alloc(size_t bytes, int *device) {
   int d = 0;
   MPIR_CUDA(cudaGetDevice(&d));
+  *device = d;
+  if (!use_pool()) {
+    void *p = nullptr;
+    MPIR_CUDA(cudaMalloc(&p, bytes));
+    return p;
+  }
   cudaStream_t s = alloc_stream(d);
   void        *p = nullptr;
   cudaError_t  e = cudaMallocAsync(&p, bytes, s);
@@ -69,7 +86,6 @@ void *device_alloc(size_t bytes, int *device) {
     throw CudaError(e, "cudaMallocAsync");
   }
   MPIR_CUDA(cudaStreamSynchronize(s));  // usable from every stream from here on
-  *device = d;
   return p;
 }
 
@@ -77,7 +93,8 @@ void device_free(void *p, int device) {
   if (!p) return;
   OnDevice on(device);
   // Errors are ignored: a free at process exit may come after the context.
-  if (cudaFreeAsync(p, alloc_stream(device)) != cudaSuccess) cudaGetLastError();
+  const cudaError_t e = use_pool() ? cudaFreeAsync(p, alloc_stream(device)) : cudaFree(p);
+  if (e != cudaSuccess) cudaGetLastError();
 }
 
 size_t device_free_bytes(int device) {

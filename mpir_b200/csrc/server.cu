@@ -399,11 +399,14 @@ struct Server::Impl {
         solver->tol        = cfg.tolerance;
         solver->update_engine = cfg.update;
         solver->adopt(plan);
+        const double t_setup = now_s();
         const int fr = solver->factor(r.Ax);
         const double sv_factor_ms = solver->last_factor_ms;
         // A resident factor keeps only what the solves read.
         MPIR_CUDA(cudaStreamSynchronize(solver->stream()));
+        const double t_trim = now_s();
         solver->trim();
+        const double t_end = now_s();
         {
           std::lock_guard<std::mutex> lk(mu);
           Factor &f = factors[k];
@@ -417,6 +420,8 @@ struct Server::Impl {
           st.factorizations++;
           st.factor_ms += 1e3 * (now_s() - tf);
           st.factor_device_ms += sv_factor_ms;
+          st.setup_ms += 1e3 * (t_setup - tf);
+          st.trim_ms += 1e3 * (t_end - t_trim);
           st.peak_bytes = std::max<int64_t>(st.peak_bytes, used);
           sv = f.solver.get();
         }

@@ -57,6 +57,9 @@ struct ServerStats {
   double analysis_ms = 0, plan_ms = 0, factor_ms = 0, solve_ms = 0;
   // Device time (CUDA events) of the factorizations and of the solves.
   double factor_device_ms = 0, solve_device_ms = 0;
+  // Parts of factor_ms: a new factor's setup (solver, resident buffers) and
+  // the release of its factorization scratch afterwards.
+  double setup_ms = 0, trim_ms = 0;
 };
 
 class Server {
