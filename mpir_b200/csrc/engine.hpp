@@ -11,14 +11,16 @@
 
 namespace mpir {
 
-// Stream-ordered device memory (memory.cu): an allocation on the current
-// device (its device returned in *device), usable from every stream once
-// this returns; a free that does not wait for the device (the caller's work
-// on the buffer has completed); the device's free memory counting what the
-// pool holds unused.
-void  *device_alloc(size_t bytes, int *device);
-void   device_free(void *p, int device);
+// Device memory (memory.cu): an allocation on the current device (its
+// device returned in *device; *pooled: from the stream-ordered pool rather
+// than cudaMalloc), usable from every stream once this returns; its free,
+// which for pool memory does not wait for the device (the caller's work on
+// the buffer has completed); the device's free memory counting what the
+// pool holds unused; the calling thread's choice of allocator.
+void  *device_alloc(size_t bytes, int *device, bool *pooled);
+void   device_free(void *p, int device, bool pooled);
 size_t device_free_bytes(int device);
+void   set_thread_pool(bool pool);
 
 // Owning device allocation.
 class DeviceBuffer {
@@ -28,7 +30,8 @@ class DeviceBuffer {
   ~DeviceBuffer() { release(); }
   DeviceBuffer(const DeviceBuffer &)            = delete;
   DeviceBuffer &operator=(const DeviceBuffer &) = delete;
-  DeviceBuffer(DeviceBuffer &&o) noexcept : p_(o.p_), bytes_(o.bytes_), dev_(o.dev_) {
+  DeviceBuffer(DeviceBuffer &&o) noexcept
+      : p_(o.p_), bytes_(o.bytes_), dev_(o.dev_), pooled_(o.pooled_) {
     o.p_     = nullptr;
     o.bytes_ = 0;
   }
@@ -38,6 +41,7 @@ class DeviceBuffer {
       p_       = o.p_;
       bytes_   = o.bytes_;
       dev_     = o.dev_;
+      pooled_  = o.pooled_;
       o.p_     = nullptr;
       o.bytes_ = 0;
     }
@@ -45,11 +49,11 @@ class DeviceBuffer {
   }
   void resize(size_t bytes) {
     release();
-    if (bytes) p_ = device_alloc(bytes, &dev_);
+    if (bytes) p_ = device_alloc(bytes, &dev_, &pooled_);
     bytes_ = bytes;
   }
   void release() {
-    if (p_) device_free(p_, dev_);
+    if (p_) device_free(p_, dev_, pooled_);
     p_     = nullptr;
     bytes_ = 0;
   }
@@ -62,7 +66,8 @@ class DeviceBuffer {
  private:
   void  *p_     = nullptr;
   size_t bytes_ = 0;
-  int    dev_   = 0;
+  int    dev_    = 0;
+  bool   pooled_ = false;
 };
 
 template <class T>

@@ -11,7 +11,13 @@
 // memory out again at once.  Freed memory stays in the pool (release
 // threshold at its maximum); an allocation that does not fit first returns
 // the pool's unused memory to the device and tries once more.
-// MPIR_ALLOC=sync selects plain cudaMalloc / cudaFree instead.
+//
+// The serving engine's worker threads allocate with plain cudaMalloc /
+// cudaFree instead (set_thread_pool(false)): with eight workers holding the
+// device near its capacity, pool allocations that had to grow the pool took
+// several times longer than cudaMalloc (measured: 40 s against 6 s of the
+// workers' time setting up new factors on a 160-request stream).
+// MPIR_ALLOC=sync makes cudaMalloc / cudaFree the default of every thread.
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
@@ -52,20 +58,25 @@ struct OnDevice {
   }
 };
 
+thread_local int t_pool = -1;  // -1: the process default
+
 bool use_pool() {
   static const bool pool = [] {
     const char *e = std::getenv("MPIR_ALLOC");
     return e == nullptr || std::strcmp(e, "sync") != 0;
   }();
-  return pool;
+  return t_pool < 0 ? pool : t_pool != 0;
 }
 }  // namespace
 
-void *device_alloc(size_t bytes, int *device) {
+void set_thread_pool(bool pool) { t_pool = pool ? 1 : 0; }
+
+void *device_alloc(size_t bytes, int *device, bool *pooled) {
   int d = 0;
   MPIR_CUDA(cudaGetDevice(&d));
   *device = d;
-  if (!use_pool()) {
+  *pooled = use_pool();
+  if (!*pooled) {
     void *p = nullptr;
     MPIR_CUDA(cudaMalloc(&p, bytes));
     return p;
@@ -89,11 +100,11 @@ void *device_alloc(size_t bytes, int *device) {
   return p;
 }
 
-void device_free(void *p, int device) {
+void device_free(void *p, int device, bool pooled) {
   if (!p) return;
   OnDevice on(device);
   // Errors are ignored: a free at process exit may come after the context.
-  const cudaError_t e = use_pool() ? cudaFreeAsync(p, alloc_stream(device)) : cudaFree(p);
+  const cudaError_t e = pooled ? cudaFreeAsync(p, alloc_stream(device)) : cudaFree(p);
   if (e != cudaSuccess) cudaGetLastError();
 }
 

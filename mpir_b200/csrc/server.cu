@@ -498,6 +498,7 @@ struct Server::Impl {
 
   void worker_main() {
     cudaSetDevice(cfg.device);
+    set_thread_pool(false);  // see memory.cu
     for (;;) {
       Job job;
       {
