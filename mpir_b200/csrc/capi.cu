@@ -448,7 +448,7 @@ static int qdldl_solve_phases(int64_t n, const int64_t *Lp, const int64_t *Li, c
     int32_t wait_err = 0;
     MPIR_CUDA(cudaMemcpy(&wait_err, E->ws->err.as<void>(), sizeof wait_err, cudaMemcpyDeviceToHost));
     if (wait_err != 0) {
-      MPIR_CUDA(cudaMemset(E->ws->err.as<void>(), 0, sizeof wait_err));
+      device_zero(E->ws->err.as<void>(), sizeof wait_err);
       g_err = "a bounded device wait of the triangular solves ran out";
       return MPIR_ERR_TIMEOUT;
     }

@@ -11,16 +11,28 @@
 
 namespace mpir {
 
-// Device memory (memory.cu): an allocation on the current device (its
-// device returned in *device; *pooled: from the stream-ordered pool rather
-// than cudaMalloc), usable from every stream once this returns; its free,
-// which for pool memory does not wait for the device (the caller's work on
-// the buffer has completed); the device's free memory counting what the
-// pool holds unused; the calling thread's choice of allocator.
-void  *device_alloc(size_t bytes, int *device, bool *pooled);
-void   device_free(void *p, int device, bool pooled);
+// Device memory (memory.cu).  An allocation on the current device, usable
+// from every stream once device_alloc returns; m records its device, its
+// source (the stream-ordered pool, or cudaMalloc with a cache of idle
+// blocks) and its capacity.  A free waits for nothing (the caller's work on
+// the buffer has completed).  device_free_bytes counts what the pool and
+// the cache hold idle as free; device_cache_flush returns the cache's blocks
+// of a device; set_thread_pool chooses the calling thread's source.
+struct DevMem {
+  int    device = 0;
+  bool   pooled = false;
+  size_t cap    = 0;
+};
+void  *device_alloc(size_t bytes, DevMem *m);
+void   device_free(void *p, const DevMem &m);
 size_t device_free_bytes(int device);
+void   device_cache_flush(int device);
+// Zeroes a buffer of the current device, complete for every stream on return.
+void   device_zero(void *p, size_t bytes);
 void   set_thread_pool(bool pool);
+// Pinned host memory with a cache of freed blocks (by size).
+void  *pinned_alloc(size_t bytes);
+void   pinned_free(void *p, size_t bytes);
 
 // Owning device allocation.
 class DeviceBuffer {
@@ -30,8 +42,7 @@ class DeviceBuffer {
   ~DeviceBuffer() { release(); }
   DeviceBuffer(const DeviceBuffer &)            = delete;
   DeviceBuffer &operator=(const DeviceBuffer &) = delete;
-  DeviceBuffer(DeviceBuffer &&o) noexcept
-      : p_(o.p_), bytes_(o.bytes_), dev_(o.dev_), pooled_(o.pooled_) {
+  DeviceBuffer(DeviceBuffer &&o) noexcept : p_(o.p_), bytes_(o.bytes_), m_(o.m_) {
     o.p_     = nullptr;
     o.bytes_ = 0;
   }
@@ -40,8 +51,7 @@ class DeviceBuffer {
       release();
       p_       = o.p_;
       bytes_   = o.bytes_;
-      dev_     = o.dev_;
-      pooled_  = o.pooled_;
+      m_       = o.m_;
       o.p_     = nullptr;
       o.bytes_ = 0;
     }
@@ -49,11 +59,11 @@ class DeviceBuffer {
   }
   void resize(size_t bytes) {
     release();
-    if (bytes) p_ = device_alloc(bytes, &dev_, &pooled_);
+    if (bytes) p_ = device_alloc(bytes, &m_);
     bytes_ = bytes;
   }
   void release() {
-    if (p_) device_free(p_, dev_, pooled_);
+    if (p_) device_free(p_, m_);
     p_     = nullptr;
     bytes_ = 0;
   }
@@ -66,8 +76,7 @@ class DeviceBuffer {
  private:
   void  *p_     = nullptr;
   size_t bytes_ = 0;
-  int    dev_    = 0;
-  bool   pooled_ = false;
+  DevMem m_;
 };
 
 template <class T>

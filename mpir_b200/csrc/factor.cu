@@ -1367,8 +1367,8 @@ void Numeric::ensure_scratch(const Plan &P) {
   bconv.resize(std::max<int64_t>(P.bconv_elems, 1) * sizeof(float));
   pack.resize(std::max<int64_t>(P.pk_elems, 1) * sizeof(float));
   packd.resize(std::max<int64_t>(2 * P.pd_elems, 1) * sizeof(float));
-  MPIR_CUDA(cudaMemset(pack.as<void>(), 0, pack.bytes()));
-  MPIR_CUDA(cudaMemset(packd.as<void>(), 0, packd.bytes()));
+  device_zero(pack.as<void>(), pack.bytes());
+  device_zero(packd.as<void>(), packd.bytes());
   Axs.resize(std::max<int64_t>(S.nnz, 1) * sizeof(double));
   Ax.resize(std::max<int64_t>(S.nnz, 1) * sizeof(double));
   has_scratch = true;

@@ -60,7 +60,7 @@ Solver::~Solver() {
   cudaSetDevice(device);
   if (own_stream_) cudaStreamSynchronize(own_stream_);
   if (stream_ && stream_ != own_stream_) cudaStreamSynchronize(stream_);
-  if (hpin_) cudaFreeHost(hpin_);
+  if (hpin_) pinned_free(hpin_, hpin_bytes_);
   if (ev0_) cudaEventDestroy(ev0_);
   if (ev1_) cudaEventDestroy(ev1_);
   plan_.reset();
@@ -451,7 +451,7 @@ int Solver::solve_device(const double *d_b, double *d_x, Report *rep) {
   int32_t wait_err = 0;
   MPIR_CUDA(cudaMemcpy(&wait_err, ws_.err.as<void>(), sizeof wait_err, cudaMemcpyDeviceToHost));
   if (wait_err != 0) {
-    MPIR_CUDA(cudaMemset(ws_.err.as<void>(), 0, sizeof wait_err));
+    device_zero(ws_.err.as<void>(), sizeof wait_err);
     st.status = -5;
     if (rep) *rep = st;
     return -5;
@@ -545,7 +545,7 @@ int Solver::luir_device(const double *d_b, double *d_x, int maxiter, Report *rep
   int32_t wait_err = 0;
   MPIR_CUDA(cudaMemcpy(&wait_err, ws_.err.as<void>(), sizeof wait_err, cudaMemcpyDeviceToHost));
   if (wait_err != 0) {
-    MPIR_CUDA(cudaMemset(ws_.err.as<void>(), 0, sizeof wait_err));
+    device_zero(ws_.err.as<void>(), sizeof wait_err);
     st.status = -5;
     if (rep) *rep = st;
     return -5;

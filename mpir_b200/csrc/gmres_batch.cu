@@ -54,13 +54,13 @@ void Solver::ensure_batch(int width) {
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   vecb_.allocate(n, sms, width);
-  if (hpin_) cudaFreeHost(hpin_);
+  if (hpin_) pinned_free(hpin_, hpin_bytes_);
   hpin_ = nullptr;
   // Pinned staging: kStageSlots slots of (width scale factors, width flags)
   // used in turn without waiting (every inner step synchronises once, and
   // takes fewer uploads than slots), then the counts and the coefficients.
-  MPIR_CUDA(cudaMallocHost(&hpin_, sizeof(double) * (kStageSlots * 2 * width + width +
-                                                     (m + 1) * width)));
+  hpin_bytes_ = sizeof(double) * (kStageSlots * 2 * width + width + (m + 1) * width);
+  hpin_       = static_cast<double *>(pinned_alloc(hpin_bytes_));
   stage_next_ = 0;
   bw_ = width;
   bm_ = m;
@@ -93,8 +93,8 @@ void Solver::precond_device(int nrhs, double *d_X) {
   MPIR_CUDA(cudaMemcpy(&e0, ws_.err.as<void>(), sizeof e0, cudaMemcpyDeviceToHost));
   if (mws_.nr) MPIR_CUDA(cudaMemcpy(&e1, mws_.err.as<void>(), sizeof e1, cudaMemcpyDeviceToHost));
   if (e0 || e1) {
-    MPIR_CUDA(cudaMemset(ws_.err.as<void>(), 0, sizeof(int32_t)));
-    if (mws_.nr) MPIR_CUDA(cudaMemset(mws_.err.as<void>(), 0, sizeof(int32_t)));
+    device_zero(ws_.err.as<void>(), sizeof(int32_t));
+    if (mws_.nr) device_zero(mws_.err.as<void>(), sizeof(int32_t));
     throw WaitTimeout();
   }
 }
@@ -439,7 +439,7 @@ int Solver::solve_batch_device(int nrhs, const double *d_B, double *d_X, Report 
   int32_t wait_err = 0;
   MPIR_CUDA(cudaMemcpy(&wait_err, mws_.err.as<void>(), sizeof wait_err, cudaMemcpyDeviceToHost));
   const int rc = wait_err != 0 ? -5 : kOk;
-  if (wait_err != 0) MPIR_CUDA(cudaMemset(mws_.err.as<void>(), 0, sizeof wait_err));
+  if (wait_err != 0) device_zero(mws_.err.as<void>(), sizeof wait_err);
   for (int k = 0; k < nb; k++) {
     if (rc != kOk) st[k].status = rc;
     if (reps) reps[k] = st[k];

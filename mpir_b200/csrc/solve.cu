@@ -661,7 +661,7 @@ void SolveWorkspace::allocate(const Plan &P) {
   sync.resize(std::max<int64_t>(P.sync_elems, 1) * sizeof(int32_t));
   ready.resize(std::max<int64_t>(kReadyCopies * P.S.n, 1) * sizeof(double));
   err.resize(sizeof(SolveCtl));
-  MPIR_CUDA(cudaMemset(err.as<void>(), 0, sizeof(SolveCtl)));
+  device_zero(err.as<void>(), sizeof(SolveCtl));
   xbuf.resize(std::max<int64_t>(P.S.n, 1) * sizeof(double));
 }
 

@@ -643,14 +643,14 @@ void MultiSolveWorkspace::allocate(const Plan &P, int width) {
   nr = width;
   graph.reset();
   xbuf.resize(std::max<int64_t>(S.n, 1) * width * sizeof(double));
-  MPIR_CUDA(cudaMemset(xbuf.as<void>(), 0, xbuf.bytes()));
+  device_zero(xbuf.as<void>(), xbuf.bytes());
   zbuf.resize(std::max<int64_t>(S.z_elems, 1) * width * sizeof(double));
   part.resize(std::max<int64_t>(P.spart_elems, 1) * width * sizeof(double));
   sync.resize(std::max<int64_t>(P.sync_elems, 1) * sizeof(int32_t));
   ready.resize(std::max<int64_t>(static_cast<int64_t>(kMultiCopies) * width * S.n, 1) *
                sizeof(double));
   err.resize(sizeof(SolveCtl));
-  MPIR_CUDA(cudaMemset(err.as<void>(), 0, sizeof(SolveCtl)));
+  device_zero(err.as<void>(), sizeof(SolveCtl));
 }
 
 size_t MultiSolveWorkspace::bytes_for(const Plan &P, int width) {

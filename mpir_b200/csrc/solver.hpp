@@ -158,6 +158,7 @@ class Solver {
   DeviceBuffer          bV_, bbs_, bbp_, bx_, br_, bt_, bd_, bhd_, by_, bfac_, bact_, bkq_, bin_,
                         bout_, bpre_;
   double               *hpin_ = nullptr;  // pinned host scalars (fac, y, act, kq)
+  size_t                hpin_bytes_ = 0;
   static constexpr int  kStageSlots = 16;
   int                   stage_next_ = 0;
   // The next staging slot (2 * bw_ doubles) for an upload of per-vector

@@ -414,7 +414,7 @@ void VecOps::allocate(int64_t n_, int sms, int batch_) {
   part.resize(sizeof(double) * 2048 * batch);
   count.resize(sizeof(unsigned int) * batch);
   infbits.resize(sizeof(unsigned long long) * 8 * batch);
-  MPIR_CUDA(cudaMemset(count.as<void>(), 0, sizeof(unsigned int) * batch));
+  device_zero(count.as<void>(), sizeof(unsigned int) * batch);
 }
 
 // Zeroes slots [first, first + cnt) of banks 0 .. nb-1.
