@@ -204,6 +204,7 @@ class Numeric {
   double          graph_eps      = 0;
   int             graph_mode     = -2;
   int64_t         graph_launches = 0;
+  bool            ran_plain      = false;  // a plain factorization since the graph was released
   // Trailing-update engine: -1 float32 SIMT, 0 bfloat16 tensor cores,
   // 1 3xTF32 tensor cores, 2 float16 tensor cores, 3 3xBF16 tensor cores.
   // The panel solves run on the tensor cores (3xTF32) with every tensor-core

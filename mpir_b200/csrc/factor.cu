@@ -1419,7 +1419,8 @@ __global__ void k_status_reset(FactorStatus *st) {
 
 void Numeric::release_graph() {
   if (graph) cudaGraphExecDestroy(graph);
-  graph = nullptr;
+  graph     = nullptr;
+  ran_plain = false;
 }
 
 cudaGraph_t Numeric::record(const Plan &P, const double *d_Ax, double eps,
@@ -1447,7 +1448,18 @@ void Numeric::run_graph(const Plan &P, const double *d_Ax, double eps, cudaStrea
     run(P, d_Ax, eps, s);
     return;
   }
-  if (!graph || graph_ax != d_Ax || graph_eps != eps || graph_mode != update_mode) {
+  const bool current = graph && graph_ax == d_Ax && graph_eps == eps && graph_mode == update_mode;
+  // A factorization that may be the only one of these buffers (a new factor
+  // of the serving engine, a drop-in Compute) runs its launches directly: a
+  // recording pays the capture and the instantiation for a single replay.
+  // The second one records the graph that every later one replays.
+  if (!current && !ran_plain) {
+    release_graph();
+    run(P, d_Ax, eps, s);
+    ran_plain = true;
+    return;
+  }
+  if (!current) {
     release_graph();
     cudaGraph_t g = record(P, d_Ax, eps, capture_stream, &graph_launches);
     const cudaError_t e = cudaGraphInstantiate(&graph, g, 0);
