@@ -165,16 +165,29 @@ struct GemmProb {
 };
 constexpr int kConvGroups = 8;   // K-groups per conversion CTA (4 per thread)
 
-// Extend-add task: add the lower triangle of child C's update matrix into
-// its parent's front, CTA-chunked by columns of U_C.
+// Extend-add: the update matrix U_C of a child C (|R_C| x |R_C|, lower
+// triangle, column-major with leading dimension |R_C|) is added into its
+// parent's front through the child's relative row map (increasing).
 struct EaTask {
   int64_t child_u;     // U_C offset in the update arena
-  int64_t parent_panel;
-  int64_t parent_u;    // -1 when the parent has no update matrix
   int64_t rel;         // offset of the child's relative row map in srel
   int32_t rc;          // |R_C|
+  int32_t pad;
+};
+// One extend-add CTA: parent columns [c0, c0 + nc), all in the parent's
+// panel (c0 + nc <= wp) or all in its update matrix (c0 >= wp), and the
+// children that add to them, hits [hit0, hit1) in child order.
+struct EaChunk {
+  int64_t parent_panel;
+  int64_t parent_u;    // -1 when the parent has no update matrix
   int32_t hp, wp;      // parent front height and width
-  int32_t chunk0;      // first column chunk of this task within the launch
+  int32_t c0, nc;
+  int32_t hit0, hit1;
+};
+// Columns [ulo, uhi) of task `task`'s U_C land in the chunk (at most
+// kEaChunk of them).
+struct EaHit {
+  int32_t task, ulo, uhi, pad;
 };
 
 
@@ -194,10 +207,7 @@ struct FactorStatus {
 constexpr int kSmallThreads = 256;
 constexpr int kDiagThreads  = 512;
 constexpr int kGemmThreads  = 256;
-constexpr int kEaChunk      = 8;     // U_C columns per extend-add CTA
-// A parent whose children's update matrices hold at most kEaSeqWork entries
-// in all is extended by one CTA (its children in order) instead of rounds.
-constexpr int64_t kEaSeqWork = int64_t{1} << 16;
+constexpr int kEaChunk      = 8;     // parent columns per extend-add CTA
 constexpr int kSolveRows = 128;        // rows per forward-solve CTA
 constexpr int kSolveChunk = 128;       // rows per backward-solve CTA
 constexpr int kSolveThreads = 512;     // 4 column quarters x 128 rows

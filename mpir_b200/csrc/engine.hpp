@@ -92,13 +92,11 @@ DeviceBuffer upload(const std::vector<T> &v, cudaStream_t s) {
 struct LevelPlan {
   int32_t small_begin = 0, small_count = 0;  // into small list
   int32_t large_begin = 0, large_count = 0;  // into large list
-  struct Round {
-    int32_t begin, count, chunks;
-  };
-  std::vector<Round> ea_rounds;
-  // Parents extended by one CTA each: [ea_seq_begin, + ea_seq_count) of the
-  // plan's ea_seq (task begin, task end) pairs.
-  int32_t ea_seq_begin = 0, ea_seq_count = 0;
+  // Extend-add CTAs (EaChunk) of the level's large parents: the columns of
+  // their panels [ea_begin[0], + ea_count[0]) before the fronts are
+  // factored, those of their update matrices [ea_begin[1], + ea_count[1])
+  // after the products that define them.
+  int32_t ea_begin[2] = {0, 0}, ea_count[2] = {0, 0};
   struct Step {
     int32_t begin, count, trsm_tiles, upd_tiles;
     // left-looking update of this block column before its diagonal block
@@ -136,7 +134,7 @@ class Plan {
   DeviceBuffer amap, arow, acol, diag_pos, Kp, Kj, Ksrc;
   DeviceBuffer sfirst, srowptr, srows, srel, slofs, uofs, zofs, child_ptr,
       child_list, perm;
-  DeviceBuffer ea_seq;  // int32 pairs, see LevelPlan::ea_seq_begin
+  DeviceBuffer ea_chunks, ea_hits;  // EaChunk / EaHit, see LevelPlan::ea_begin
   DeviceBuffer small_list, large_list, steps, ea_tasks, linv_ofs_d, gemm_probs,
       solve_fronts, swarp_list, sblock_list, gp, gsrc, fwd_item, chunk_map, own_item;
   int64_t      ws_elems = 0;  // split-K partial tiles (floats)
@@ -163,7 +161,9 @@ class Plan {
   struct HostArrays {
     std::vector<StepDesc>   descs;
     std::vector<EaTask>     tasks;
-    std::vector<int32_t>    seq, chunk_map;
+    std::vector<EaChunk>    chunks;
+    std::vector<EaHit>      hits;
+    std::vector<int32_t>    chunk_map;
     std::vector<GemmProb>   probs;
     std::vector<SolveFront> sfronts;
     std::vector<int64_t>    gp, gsrc;

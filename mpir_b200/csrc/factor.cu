@@ -154,105 +154,52 @@ __global__ void __launch_bounds__(kSmallThreads)
 // ---------------------------------------------------------------------------
 // Zero the update matrices of the level's large fronts.
 
-// Extend-add of children's update matrices into large parents.
-// phase 1: only the columns that go to the parent's panel (before the parent
-// is factored); phase 2: only those that go to its update matrix (after the
-// product that defines it).
-__global__ void k_extend_add(const EaTask *tasks, int ntasks,
-                             const int32_t *srel, float *panel,
-                             float *uarena, int phase) {
-  const int t  = blockIdx.x;
-  int       lo = 0, hi = ntasks - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) / 2;
-    if (tasks[mid].chunk0 <= t) lo = mid; else hi = mid - 1;
-  }
-  const EaTask   tk = tasks[lo];
-  const int      b0 = (t - tk.chunk0) * kEaChunk;
-  const int      nb = min(kEaChunk, tk.rc - b0);
-  const int32_t *rl = srel + tk.rel;
-  const float   *U  = uarena + tk.child_u;
-  const int      rp = tk.hp - tk.wp;
-  // Column b0 + u of U_C goes to column rl[b0 + u] of the parent: in its
-  // panel (rows from 0) or in its update matrix (rows from wp).
-  __shared__ float *dst_s[kEaChunk];
-  __shared__ int    off_s[kEaChunk];
-  __shared__ int    act_s[kEaChunk];
-  if (threadIdx.x < kEaChunk) {
-    const int u  = threadIdx.x;
-    const int cb = u < nb ? rl[b0 + u] : 0;
-    dst_s[u]     = cb < tk.wp ? panel + tk.parent_panel + (int64_t)cb * tk.hp
-                              : uarena + tk.parent_u + (int64_t)(cb - tk.wp) * rp;
-    off_s[u]     = cb < tk.wp ? 0 : tk.wp;
-    act_s[u]     = u < nb && (phase == 1 ? cb < tk.wp : cb >= tk.wp);
-  }
-  // The row map is increasing, so a chunk's columns all belong to one phase
-  // except at the panel / update-matrix boundary: leave if none is active.
-  if (!__syncthreads_or(threadIdx.x < kEaChunk && act_s[threadIdx.x])) return;
-  // Each thread takes one row at a time across all the chunk's columns: the
-  // row map entry is loaded one row ahead, so the values of U_C and of the
-  // parent are loaded together, all before any store (the source and the
-  // destination may both lie in the update arena, so the compiler would not
-  // reorder them itself).
-  int a  = b0 + threadIdx.x;
-  int ra = a < tk.rc ? rl[a] : -1;
-  for (; a < tk.rc; a += blockDim.x) {
-    const int an     = a + blockDim.x;
-    const int ra_nxt = an < tk.rc ? rl[an] : -1;
-    float     v[kEaChunk], o[kEaChunk];
-#pragma unroll
-    for (int u = 0; u < kEaChunk; u++) {
-      const bool ok = act_s[u] && a >= b0 + u;
-      v[u]          = ok ? U[a + (int64_t)(b0 + u) * tk.rc] : 0.0f;
-      o[u]          = ok ? dst_s[u][ra - off_s[u]] : 0.0f;
-    }
+// Extend-add of the children's update matrices into a level's large parents,
+// one CTA per chunk of at most kEaChunk parent columns (EaChunk): the
+// children that add to those columns, in child order with a barrier between
+// them (siblings may add to the same entries), each child's columns of the
+// chunk by all threads over the child's rows.  Every parent entry receives
+// its children's contributions in child order.  Within a child each thread
+// takes one row at a time across the chunk's columns: the row map entry is
+// loaded one row ahead and all values of U_C and of the parent are loaded
+// before any store (the source and the destination may both lie in the
+// update arena, so the compiler would not reorder them itself).
+__global__ void __launch_bounds__(256)
+    k_extend_add(const EaChunk *chunks, const EaHit *hits, const EaTask *tasks,
+                 const int32_t *srel, float *panel, float *uarena) {
+  const EaChunk ck   = chunks[blockIdx.x];
+  const bool    in_u = ck.c0 >= ck.wp;
+  // Parent entry (row ra, column cb) at base + (cb - cbase) * ld + ra: in the
+  // panel (rows from 0) or in the update matrix (rows from wp).
+  float *const  base  = in_u ? uarena + ck.parent_u - ck.wp : panel + ck.parent_panel;
+  const int64_t ld    = in_u ? ck.hp - ck.wp : ck.hp;
+  const int     cbase = in_u ? ck.wp : 0;
+  for (int hh = ck.hit0; hh < ck.hit1; hh++) {
+    const EaHit    hit = hits[hh];
+    const EaTask   tk  = tasks[hit.task];
+    const int32_t *rl  = srel + tk.rel;
+    const float   *U   = uarena + tk.child_u;
+    const int      nb  = hit.uhi - hit.ulo, u0 = hit.ulo;
+    float         *dst[kEaChunk];
 #pragma unroll
     for (int u = 0; u < kEaChunk; u++)
-      if (act_s[u] && a >= b0 + u) dst_s[u][ra - off_s[u]] = o[u] + v[u];
-    ra = ra_nxt;
-  }
-}
-
-// Extend-add for parents with only small children: CTA p takes parent p's
-// tasks (children) in order, a barrier between them (siblings may add to the
-// same entries; the order is the rounds' order, child order).  Within a
-// task warp v takes the 8-column chunks v, v + 8, ..., its lanes the rows.
-__global__ void __launch_bounds__(256)
-    k_extend_add_seq(const int32_t *seq, const EaTask *tasks, const int32_t *srel,
-                     float *panel, float *uarena, int phase) {
-  const int t0 = seq[2 * blockIdx.x], t1 = seq[2 * blockIdx.x + 1];
-  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-  for (int ti = t0; ti < t1; ti++) {
-    const EaTask   tk = tasks[ti];
-    const int32_t *rl = srel + tk.rel;
-    const float   *U  = uarena + tk.child_u;
-    const int      rp = tk.hp - tk.wp;
-    for (int b0 = warp * kEaChunk; b0 < tk.rc; b0 += 8 * kEaChunk) {
-      const int nb = min(kEaChunk, tk.rc - b0);
-      float    *dst[kEaChunk];
-      int       off[kEaChunk];
-      bool      act[kEaChunk];
+      dst[u] = base + static_cast<int64_t>((u < nb ? rl[u0 + u] : cbase) - cbase) * ld;
+    int a  = u0 + threadIdx.x;
+    int ra = a < tk.rc ? rl[a] : 0;
+    for (; a < tk.rc; a += blockDim.x) {
+      const int an     = a + blockDim.x;
+      const int ra_nxt = an < tk.rc ? rl[an] : 0;
+      float     v[kEaChunk], o[kEaChunk];
 #pragma unroll
       for (int u = 0; u < kEaChunk; u++) {
-        const int cb = u < nb ? rl[b0 + u] : 0;
-        dst[u]       = cb < tk.wp ? panel + tk.parent_panel + (int64_t)cb * tk.hp
-                                  : uarena + tk.parent_u + (int64_t)(cb - tk.wp) * rp;
-        off[u]       = cb < tk.wp ? 0 : tk.wp;
-        act[u]       = u < nb && (phase == 1 ? cb < tk.wp : cb >= tk.wp);
+        const bool ok = u < nb && a >= u0 + u;
+        v[u]          = ok ? U[a + static_cast<int64_t>(u0 + u) * tk.rc] : 0.0f;
+        o[u]          = ok ? dst[u][ra] : 0.0f;
       }
-      for (int a = b0 + lane; a < tk.rc; a += 32) {
-        const int ra = rl[a];
-        float     v[kEaChunk], o[kEaChunk];
 #pragma unroll
-        for (int u = 0; u < kEaChunk; u++) {
-          const bool ok = act[u] && a >= b0 + u;
-          v[u]          = ok ? U[a + (int64_t)(b0 + u) * tk.rc] : 0.0f;
-          o[u]          = ok ? dst[u][ra - off[u]] : 0.0f;
-        }
-#pragma unroll
-        for (int u = 0; u < kEaChunk; u++)
-          if (act[u] && a >= b0 + u) dst[u][ra - off[u]] = o[u] + v[u];
-      }
+      for (int u = 0; u < kEaChunk; u++)
+        if (u < nb && a >= u0 + u) dst[u][ra] = o[u] + v[u];
+      ra = ra_nxt;
     }
     __syncthreads();
   }
@@ -961,7 +908,8 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
   h_large.clear();
   std::vector<StepDesc> descs;
   std::vector<EaTask>   tasks;
-  std::vector<int32_t>  seq_h;
+  std::vector<EaChunk>  chunks_h;
+  std::vector<EaHit>    hits_h;
   std::vector<GemmProb> probs;
   ws_elems    = 0;
   bconv_elems = 0;
@@ -1047,58 +995,74 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
     }
     L.small_count = static_cast<int32_t>(h_small.size()) - L.small_begin;
     L.large_count = static_cast<int32_t>(h_large.size()) - L.large_begin;
-    // Extend-add: parents with only small children get one CTA each (their
-    // children in order); the others go by rounds (round q = q-th child).
-    auto ea_task = [&](int64_t P, int64_t C) {
-      EaTask tk;
-      tk.child_u      = S.uofs[C];
-      tk.parent_panel = S.slofs[P];
-      tk.parent_u     = S.uofs[P];
-      tk.rel          = S.srowptr[C] + S.w(C);
-      tk.rc           = static_cast<int32_t>(S.h(C) - S.w(C));
-      tk.hp           = static_cast<int32_t>(S.h(P));
-      tk.wp           = static_cast<int32_t>(S.w(P));
-      tk.chunk0       = 0;
-      return tk;
-    };
-    std::vector<char> seq_parent(L.large_count, 0);
-    L.ea_seq_begin = static_cast<int32_t>(seq_h.size() / 2);
+    // Extend-add: per phase (the parents' panel columns, then their update
+    // matrices' columns) one CTA per chunk of kEaChunk parent columns that a
+    // child adds to, with those children's hits in child order.
+    std::vector<int32_t> task0(L.large_count);
     for (int32_t q = L.large_begin; q < L.large_begin + L.large_count; q++) {
-      const int64_t P    = h_large[q];
-      int64_t       work = 0;
+      const int64_t P = h_large[q];
+      task0[q - L.large_begin] = static_cast<int32_t>(tasks.size());
       for (int64_t c = S.child_ptr[P]; c < S.child_ptr[P + 1]; c++) {
-        const int64_t rc = S.h(S.child_list[c]) - S.w(S.child_list[c]);
-        work += rc * (rc + 1) / 2;
-      }
-      if (S.child_ptr[P + 1] - S.child_ptr[P] < 2 || work > kEaSeqWork) continue;
-      seq_parent[q - L.large_begin] = 1;
-      seq_h.push_back(static_cast<int32_t>(tasks.size()));
-      for (int64_t c = S.child_ptr[P]; c < S.child_ptr[P + 1]; c++)
-        tasks.push_back(ea_task(P, S.child_list[c]));
-      seq_h.push_back(static_cast<int32_t>(tasks.size()));
-    }
-    L.ea_seq_count = static_cast<int32_t>(seq_h.size() / 2) - L.ea_seq_begin;
-    int64_t maxkids = 0;
-    for (int32_t q = L.large_begin; q < L.large_begin + L.large_count; q++) {
-      const int64_t J = h_large[q];
-      if (!seq_parent[q - L.large_begin])
-        maxkids = std::max(maxkids, S.child_ptr[J + 1] - S.child_ptr[J]);
-    }
-    for (int64_t round = 0; round < maxkids; round++) {
-      LevelPlan::Round R{static_cast<int32_t>(tasks.size()), 0, 0};
-      int32_t          ch = 0;
-      for (int32_t q = L.large_begin; q < L.large_begin + L.large_count; q++) {
-        const int64_t P = h_large[q];
-        if (seq_parent[q - L.large_begin]) continue;
-        if (S.child_ptr[P] + round >= S.child_ptr[P + 1]) continue;
-        EaTask tk = ea_task(P, S.child_list[S.child_ptr[P] + round]);
-        tk.chunk0 = ch;
-        ch += (tk.rc + kEaChunk - 1) / kEaChunk;
+        const int64_t C = S.child_list[c];
+        EaTask        tk;
+        tk.child_u = S.uofs[C];
+        tk.rel     = S.srowptr[C] + S.w(C);
+        tk.rc      = static_cast<int32_t>(S.h(C) - S.w(C));
+        tk.pad     = 0;
         tasks.push_back(tk);
       }
-      R.count  = static_cast<int32_t>(tasks.size()) - R.begin;
-      R.chunks = ch;
-      if (R.count > 0) L.ea_rounds.push_back(R);
+    }
+    for (int ph = 0; ph < 2; ph++) {
+      L.ea_begin[ph] = static_cast<int32_t>(chunks_h.size());
+      for (int32_t q = L.large_begin; q < L.large_begin + L.large_count; q++) {
+        const int64_t P  = h_large[q];
+        const int64_t nk = S.child_ptr[P + 1] - S.child_ptr[P];
+        const int32_t hp = static_cast<int32_t>(S.h(P)), wp = static_cast<int32_t>(S.w(P));
+        const int32_t lo = ph == 0 ? 0 : wp, hi = ph == 0 ? wp : hp;
+        if (nk == 0 || hi <= lo) continue;
+        const int32_t nch = (hi - lo + kEaChunk - 1) / kEaChunk;
+        // Hits per chunk (counted, then placed), children in order: a child's
+        // columns in one chunk are consecutive (its row map increases).
+        std::vector<int32_t> cnt(nch + 1, 0);
+        auto walk = [&](auto &&emit) {
+          for (int64_t k = 0; k < nk; k++) {
+            const int32_t  tix = task0[q - L.large_begin] + static_cast<int32_t>(k);
+            const EaTask  &tk  = tasks[tix];
+            const int32_t *rl  = S.srel.data() + tk.rel;
+            int32_t        u   = 0;
+            while (u < tk.rc && rl[u] < lo) u++;
+            while (u < tk.rc && rl[u] < hi) {
+              const int32_t ch = (rl[u] - lo) / kEaChunk, end = lo + (ch + 1) * kEaChunk;
+              int32_t       v  = u;
+              while (v < tk.rc && rl[v] < std::min(end, hi)) v++;
+              emit(ch, tix, u, v);
+              u = v;
+            }
+          }
+        };
+        walk([&](int32_t ch, int32_t, int32_t, int32_t) { cnt[ch + 1]++; });
+        for (int32_t c = 0; c < nch; c++) cnt[c + 1] += cnt[c];
+        const int32_t        hbase = static_cast<int32_t>(hits_h.size());
+        std::vector<int32_t> fill(cnt.begin(), cnt.end() - 1);
+        hits_h.resize(hits_h.size() + cnt[nch]);
+        walk([&](int32_t ch, int32_t tix, int32_t u, int32_t v) {
+          hits_h[hbase + fill[ch]++] = EaHit{tix, u, v, 0};
+        });
+        for (int32_t c = 0; c < nch; c++) {
+          if (cnt[c + 1] == cnt[c]) continue;  // no child adds to these columns
+          EaChunk ck;
+          ck.parent_panel = S.slofs[P];
+          ck.parent_u     = S.uofs[P];
+          ck.hp           = hp;
+          ck.wp           = wp;
+          ck.c0           = lo + c * kEaChunk;
+          ck.nc           = std::min(kEaChunk, hi - ck.c0);
+          ck.hit0         = hbase + cnt[c];
+          ck.hit1         = hbase + cnt[c + 1];
+          chunks_h.push_back(ck);
+        }
+      }
+      L.ea_count[ph] = static_cast<int32_t>(chunks_h.size()) - L.ea_begin[ph];
     }
     // Blocked steps.  Step kb: the left-looking update of block column kb
     // by the columns before it, then its diagonal block and panel solve;
@@ -1275,7 +1239,8 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
   // the device without being built again.
   host_.descs       = std::move(descs);
   host_.tasks       = std::move(tasks);
-  host_.seq         = std::move(seq_h);
+  host_.chunks      = std::move(chunks_h);
+  host_.hits        = std::move(hits_h);
   host_.probs       = std::move(probs);
   host_.sfronts     = std::move(sfronts);
   host_.gp          = std::move(gp_h);
@@ -1308,7 +1273,8 @@ void Plan::upload_all(cudaStream_t s) {
   large_list = upload(h_large, s);
   steps      = upload(host_.descs, s);
   ea_tasks   = upload(host_.tasks, s);
-  ea_seq     = upload(host_.seq, s);
+  ea_chunks  = upload(host_.chunks, s);
+  ea_hits    = upload(host_.hits, s);
   gemm_probs = upload(host_.probs, s);
   linv_ofs_d = upload(linv_ofs, s);
   solve_fronts = upload(host_.sfronts, s);
@@ -1326,7 +1292,7 @@ void Plan::upload_all(cudaStream_t s) {
 void Plan::release_device() {
   for (DeviceBuffer *d :
        {&amap, &arow, &acol, &diag_pos, &Kp, &Kj, &Ksrc, &sfirst, &srowptr, &srows, &srel,
-        &slofs, &uofs, &zofs, &child_ptr, &child_list, &perm, &ea_seq, &small_list,
+        &slofs, &uofs, &zofs, &child_ptr, &child_list, &perm, &ea_chunks, &ea_hits, &small_list,
         &large_list, &steps, &ea_tasks, &linv_ofs_d, &gemm_probs, &solve_fronts, &swarp_list,
         &sblock_list, &gp, &gsrc, &fwd_item, &chunk_map, &own_item})
     d->release();
@@ -1402,7 +1368,7 @@ size_t Plan::device_bytes() const {
   size_t b = 0;
   for (const DeviceBuffer *d :
        {&amap, &arow, &acol, &diag_pos, &Kp, &Kj, &Ksrc, &sfirst, &srowptr, &srows, &srel,
-        &slofs, &uofs, &zofs, &child_ptr, &child_list, &perm, &ea_seq, &small_list,
+        &slofs, &uofs, &zofs, &child_ptr, &child_list, &perm, &ea_chunks, &ea_hits, &small_list,
         &large_list, &steps, &ea_tasks, &linv_ofs_d, &gemm_probs, &solve_fronts, &swarp_list,
         &sblock_list, &gp, &gsrc, &fwd_item, &chunk_map, &own_item})
     b += d->bytes();
@@ -1520,18 +1486,14 @@ void Numeric::run(const Plan &P, const double *d_Ax, double eps, cudaStream_t s)
     // Children's update matrices into the fronts' panels (the update
     // matrices' own columns follow after the product that defines them).
     auto extend_add = [&](int phase) {
-      if (L.ea_seq_count > 0) {
+      const int ph = phase - 1;
+      if (L.ea_count[ph] > 0) {
         kt.begin(kKcExtendAdd, s);
-        launch(k_extend_add_seq, L.ea_seq_count, 256, 0, s,
-               P.ea_seq.as<int32_t>() + 2 * L.ea_seq_begin,
+        launch(k_extend_add, L.ea_count[ph], 256, 0, s,
+               P.ea_chunks.as<EaChunk>() + L.ea_begin[ph],
+               static_cast<const EaHit *>(P.ea_hits.as<EaHit>()),
                static_cast<const EaTask *>(P.ea_tasks.as<EaTask>()), P.srel.as<int32_t>(), pan,
-               ua, phase);
-        kt.end(s);
-      }
-      for (const auto &R : L.ea_rounds) {
-        kt.begin(kKcExtendAdd, s);
-        launch(k_extend_add, R.chunks, 256, 0, s, P.ea_tasks.as<EaTask>() + R.begin, R.count,
-               P.srel.as<int32_t>(), pan, ua, phase);
+               ua);
         kt.end(s);
       }
     };
