@@ -110,37 +110,49 @@ struct Server::Impl {
     }
   }
 
+  // The oldest request that can run now, except that one whose pattern needs
+  // its plan (an unknown or evicted pattern) goes first: its host analysis
+  // or upload is the start of the longest chain of work in the queue
+  // (analysis, factorization, solves), and every queued request on that
+  // pattern waits for it.
   bool pick(Job &job) {
-    for (auto it = queue.begin(); it != queue.end(); ++it) {
-      const ServerRequest r = *it;
-      const FKey          k{r.pattern_key, r.values_key};
-      auto                p = patterns.find(r.pattern_key);
-      if (p != patterns.end() && p->second.busy) continue;  // being analysed
-      auto f = factors.find(k);
-      if (f != factors.end() && f->second.busy) continue;   // in use
-      queue.erase(it);
-      job.reqs.clear();
-      job.reqs.push_back(r);
-      take_same(k, static_cast<size_t>(cfg.max_batch), job.reqs);
-      if (p == patterns.end() || !p->second.resident) {
-        if (p == patterns.end()) {
-          Pattern np;
-          np.last = now_s();
-          p       = patterns.emplace(r.pattern_key, std::move(np)).first;
-        }
-        p->second.busy = true;
-        job.kind       = Job::kAnalyse;
-      } else if (f != factors.end() && f->second.valid) {
-        job.kind = Job::kSolve;
-      } else {
-        job.kind = Job::kFactor;
+    auto choice = queue.end();
+    for (int pass = 0; pass < 2 && choice == queue.end(); pass++)
+      for (auto it = queue.begin(); it != queue.end(); ++it) {
+        auto p = patterns.find(it->pattern_key);
+        if (p != patterns.end() && p->second.busy) continue;  // being analysed
+        auto f = factors.find(FKey{it->pattern_key, it->values_key});
+        if (f != factors.end() && f->second.busy) continue;   // in use
+        if (pass == 0 && p != patterns.end() && p->second.resident) continue;
+        choice = it;
+        break;
       }
-      Factor &fe = factors[k];  // placeholder while it is built
-      fe.busy    = true;
-      running++;
-      return true;
+    if (choice == queue.end()) return false;
+    const ServerRequest r = *choice;
+    const FKey          k{r.pattern_key, r.values_key};
+    auto                p = patterns.find(r.pattern_key);
+    auto                f = factors.find(k);
+    queue.erase(choice);
+    job.reqs.clear();
+    job.reqs.push_back(r);
+    take_same(k, static_cast<size_t>(cfg.max_batch), job.reqs);
+    if (p == patterns.end() || !p->second.resident) {
+      if (p == patterns.end()) {
+        Pattern np;
+        np.last = now_s();
+        p       = patterns.emplace(r.pattern_key, std::move(np)).first;
+      }
+      p->second.busy = true;
+      job.kind       = Job::kAnalyse;
+    } else if (f != factors.end() && f->second.valid) {
+      job.kind = Job::kSolve;
+    } else {
+      job.kind = Job::kFactor;
     }
-    return false;
+    Factor &fe = factors[k];  // placeholder while it is built
+    fe.busy    = true;
+    running++;
+    return true;
   }
 
   // Frees room for `need` bytes by evicting idle factors, then idle plans

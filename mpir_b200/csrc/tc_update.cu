@@ -672,10 +672,10 @@ void launch_convert_b(const GemmProb *probs, int nprob, int convs, const float *
 // Shared memory (K-major core-matrix layout, K-group g at g * 2048 bytes,
 // row m at m * 16): B = X diag(Dinv) in tf32 high and low parts for all 128
 // columns of K (2 x 64 KB), A in halves of 64 columns (high and low parts,
-// 2 x 32 KB).  All 256 threads convert: B, then A's first half; one lane
-// issues its 8 x 3 MMAs (M = N = 128, K = 8) and commits; the threads load
-// A's second half into registers meanwhile and write it once the commit
-// shows the first half's MMAs done.  Epilogue: warps w and w + 4 drain
+// 2 x 32 KB).  All 256 threads load A (both halves) and X into registers
+// first, then convert B and A's first half; one lane issues its 8 x 3 MMAs
+// (M = N = 128, K = 8) and commits; the threads write A's second half once
+// the commit shows the first half's MMAs done.  Epilogue: warps w and w + 4 drain
 // tensor-memory lanes 32 (w % 4) .. (rows), columns 0-63 and 64-127.
 namespace tc {
 constexpr uint32_t kTrsmB     = 32 * kGroup;           // one part of B (bytes)
@@ -742,33 +742,27 @@ __global__ void __launch_bounds__(256, 1)
       *reinterpret_cast<uint4 *>(smem + 2 * kTrsmB + kTrsmA + o) = al;
     }
   };
-  float a[32];
+  // Every global load of the CTA is issued before the first is used (one
+  // memory latency instead of one per batch): A's two halves, and B = X
+  // diag(Dinv) by thread (row n = m, K-groups gsel + 2 i, i < 16).
+  const int halves = nbk > 64 ? 2 : 1;
+  float     a[32], a1[32], xv[64];
   load_a(0, a);
-  // B = X diag(Dinv): thread (row n = m, K-groups gsel + 2 i, i < 16), in two
-  // batches of 8 K-groups (all loads of a batch first).
-  {
-    const float dv = m < nbk ? Dinv[static_cast<int64_t>(d.col0) + kb + m] : 0.0f;
+  const float dv = m < nbk ? Dinv[static_cast<int64_t>(d.col0) + kb + m] : 0.0f;
 #pragma unroll
-    for (int bt = 0; bt < 2; bt++) {
-      float xv[32];
+  for (int i = 0; i < 16; i++)
 #pragma unroll
-      for (int i = 0; i < 8; i++)
+    for (int j = 0; j < 4; j++) xv[4 * i + j] = X[m + (4 * (gsel + 2 * i) + j) * kNB];
+  if (halves == 2) load_a(1, a1);
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-          const int k = 4 * (gsel + 2 * (8 * bt + i)) + j;
-          xv[4 * i + j] = X[m + k * kNB];
-        }
-#pragma unroll
-      for (int i = 0; i < 8; i++) {
-        const float bv[4] = {xv[4 * i] * dv, xv[4 * i + 1] * dv, xv[4 * i + 2] * dv,
-                             xv[4 * i + 3] * dv};
-        uint4       bh, bl;
-        split4(bv, bh, bl);
-        const uint32_t o = (gsel + 2 * (8 * bt + i)) * kGroup + m * 16;
-        *reinterpret_cast<uint4 *>(smem + o)          = bh;
-        *reinterpret_cast<uint4 *>(smem + kTrsmB + o) = bl;
-      }
-    }
+  for (int i = 0; i < 16; i++) {
+    const float bv[4] = {xv[4 * i] * dv, xv[4 * i + 1] * dv, xv[4 * i + 2] * dv,
+                         xv[4 * i + 3] * dv};
+    uint4       bh, bl;
+    split4(bv, bh, bl);
+    const uint32_t o = (gsel + 2 * i) * kGroup + m * 16;
+    *reinterpret_cast<uint4 *>(smem + o)          = bh;
+    *reinterpret_cast<uint4 *>(smem + kTrsmB + o) = bl;
   }
   store_a(a);
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -776,7 +770,6 @@ __global__ void __launch_bounds__(256, 1)
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem   = tmem_slot;
-  const int      halves = nbk > 64 ? 2 : 1;
   const uint32_t idesc  = make_idesc(kFmtTF32);
   auto issue = [&](int half) {
     if (tid != 32) return;
@@ -796,10 +789,9 @@ __global__ void __launch_bounds__(256, 1)
   issue(0);
   bool ok = true;
   if (halves == 2) {
-    load_a(1, a);
     ok = wait_bounded(bar, 0);  // the first half's MMAs have read A
     if (ok) {
-      store_a(a);
+      store_a(a1);
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
     ok = __syncthreads_and(ok);
