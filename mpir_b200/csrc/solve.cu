@@ -665,6 +665,33 @@ void SolveWorkspace::allocate(const Plan &P) {
   xbuf.resize(std::max<int64_t>(P.S.n, 1) * sizeof(double));
 }
 
+cudaStream_t SideStream::fork(cudaStream_t s) {
+  if (!st_) {
+    MPIR_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+    MPIR_CUDA(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
+    MPIR_CUDA(cudaEventCreateWithFlags(&join_, cudaEventDisableTiming));
+  }
+  MPIR_CUDA(cudaEventRecord(fork_, s));
+  MPIR_CUDA(cudaStreamWaitEvent(st_, fork_, 0));
+  return st_;
+}
+
+void SideStream::join(cudaStream_t s) {
+  MPIR_CUDA(cudaEventRecord(join_, st_));
+  MPIR_CUDA(cudaStreamWaitEvent(s, join_, 0));
+}
+
+void SideStream::reset() {
+  if (st_) {
+    cudaStreamSynchronize(st_);
+    cudaStreamDestroy(st_);
+  }
+  if (fork_) cudaEventDestroy(fork_);
+  if (join_) cudaEventDestroy(join_);
+  st_   = nullptr;
+  fork_ = join_ = nullptr;
+}
+
 void SolveWorkspace::release_graph() {
   if (graph) cudaGraphExecDestroy(graph);
   graph = nullptr;
@@ -727,10 +754,12 @@ static void ldlt_solve_t(const Plan &P, const Numeric &F, const T *pan, double *
   }
   kt.begin(kKcSolveFwd, s);
   for (int t = 0; t < nl && (phases & kForward); t++) {
-    const LevelPlan &L = P.levels[t];
+    const LevelPlan &L    = P.levels[t];
+    const bool       both = L.sw_count > 0 && L.sf_count > 0;
+    cudaStream_t     ss   = both ? ws.side.fork(s) : s;  // warp fronts beside block fronts
     if (L.sw_count > 0)
       launch(k_fwd_small<T>, (L.sw_count + kWarpsPerCta - 1) / kWarpsPerCta, 32 * kWarpsPerCta, 0,
-             s, P.swarp_list.as<int32_t>() + L.sw_begin, L.sw_count, P.sfirst.as<int64_t>(),
+             ss, P.swarp_list.as<int32_t>() + L.sw_begin, L.sw_count, P.sfirst.as<int64_t>(),
              P.srowptr.as<int64_t>(), P.slofs.as<int64_t>(), P.child_ptr.as<int64_t>(),
              P.child_list.as<int32_t>(), P.srel.as<int32_t>(), P.zofs.as<int64_t>(), pan, x,
              zbuf);
@@ -739,6 +768,7 @@ static void ldlt_solve_t(const Plan &P, const Numeric &F, const T *pan, double *
              P.fwd_item.as<SolveItem>() + L.fwd_map0, pan, lvt, P.gp.as<int64_t>(),
              P.gsrc.as<int64_t>(), x, zbuf, sync + 2 * t, ready, err);
     }
+    if (both) ws.side.join(s);
   }
   if (phases & kDiagonal)
     launch(k_dscale, static_cast<unsigned>((S.n + 255) / 256), 256, 0, s,
@@ -749,10 +779,12 @@ static void ldlt_solve_t(const Plan &P, const Numeric &F, const T *pan, double *
   kt.begin(kKcSolveBwd, s);
   if (block) launch(k_mark_pending, nmark, 256, 0, s, nready, ready);
   for (int t = nl - 1; t >= 0; t--) {
-    const LevelPlan &L = P.levels[t];
+    const LevelPlan &L    = P.levels[t];
+    const bool       both = L.sw_count > 0 && L.sf_count > 0;
+    cudaStream_t     ss   = both ? ws.side.fork(s) : s;
     if (L.sw_count > 0)
       launch(k_bwd_small<T>, (L.sw_count + kWarpsPerCta - 1) / kWarpsPerCta, 32 * kWarpsPerCta, 0,
-             s, P.swarp_list.as<int32_t>() + L.sw_begin, L.sw_count, P.sfirst.as<int64_t>(),
+             ss, P.swarp_list.as<int32_t>() + L.sw_begin, L.sw_count, P.sfirst.as<int64_t>(),
              P.srowptr.as<int64_t>(), P.srows.as<int32_t>(), P.slofs.as<int64_t>(), pan, x);
     if (L.sf_count > 0) {
       if (L.bwd_chunk_items > 0)
@@ -765,6 +797,7 @@ static void ldlt_solve_t(const Plan &P, const Numeric &F, const T *pan, double *
              F.linv64t.as<double>(), x,
              static_cast<const double *>(ws.part.as<double>()), sync + 2 * t + 1, ready, err);
     }
+    if (both) ws.side.join(s);
   }
   kt.end(s);
   MPIR_CHECK_LAUNCH();

@@ -1,10 +1,45 @@
 // Triangular-solve workspace and entry point (solve.cu).
 #pragma once
 #include <string>
+#include <utility>
 
 #include "engine.hpp"
 
 namespace mpir {
+
+// A second stream and two events, created on first use on the current
+// device: a level's warp-solved fronts run on it beside the same level's
+// block fronts (neither reads what the other writes), inside a recorded
+// graph as a parallel branch.
+class SideStream {
+ public:
+  SideStream() = default;
+  SideStream(const SideStream &)            = delete;
+  SideStream &operator=(const SideStream &) = delete;
+  SideStream(SideStream &&o) noexcept { swap(o); }
+  SideStream &operator=(SideStream &&o) noexcept {
+    if (this != &o) {
+      reset();
+      swap(o);
+    }
+    return *this;
+  }
+  ~SideStream() { reset(); }
+  // The side stream, after everything issued to s so far.
+  cudaStream_t fork(cudaStream_t s);
+  // Work issued to s from here on runs after everything issued to the side.
+  void join(cudaStream_t s);
+
+ private:
+  void swap(SideStream &o) {
+    std::swap(st_, o.st_);
+    std::swap(fork_, o.fork_);
+    std::swap(join_, o.join_);
+  }
+  void         reset();
+  cudaStream_t st_   = nullptr;
+  cudaEvent_t  fork_ = nullptr, join_ = nullptr;
+};
 
 struct SolveWorkspace {
   DeviceBuffer zbuf;      // front vectors, zofs layout (doubles)
@@ -17,6 +52,7 @@ struct SolveWorkspace {
   DeviceBuffer xbuf;      // fixed vector the captured solve works on
   cudaGraphExec_t graph = nullptr;  // captured L D L^T solve (all phases)
   int64_t graph_launches = 0;       // kernels one replay runs
+  SideStream side;
   void allocate(const Plan &P);
   void release_graph();
   ~SolveWorkspace() { release_graph(); }
@@ -66,6 +102,7 @@ struct MultiSolveWorkspace {
   DeviceBuffer xbuf;
   GraphExec    graph;
   int64_t      graph_launches = 0;
+  SideStream   side;
   void         allocate(const Plan &P, int width);
   static size_t bytes_for(const Plan &P, int width);
 };

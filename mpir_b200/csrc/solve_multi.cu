@@ -586,10 +586,12 @@ void solve_multi_nr(const Plan &P, const Numeric &F, const T *pan, double *X,
   if (block && (phases & kForward)) launch(k_mark_pending_m, nmark, 256, 0, s, nready, ready);
   kt.begin(kKcSolveFwd, s);
   for (int t = 0; t < nl && (phases & kForward); t++) {
-    const LevelPlan &L = P.levels[t];
+    const LevelPlan &L    = P.levels[t];
+    const bool       both = L.sw_count > 0 && L.sf_count > 0;
+    cudaStream_t     ss   = both ? ws.side.fork(s) : s;  // warp fronts beside block fronts
     if (L.sw_count > 0)
       launch(k_fwd_small_m<NR, T>, (L.sw_count + kSmallWarpsM - 1) / kSmallWarpsM, 32 * kSmallWarpsM,
-             small_smem, s, P.swarp_list.as<int32_t>() + L.sw_begin, L.sw_count,
+             small_smem, ss, P.swarp_list.as<int32_t>() + L.sw_begin, L.sw_count,
              P.sfirst.as<int64_t>(), P.srowptr.as<int64_t>(), P.slofs.as<int64_t>(),
              P.child_ptr.as<int64_t>(), P.child_list.as<int32_t>(), P.srel.as<int32_t>(),
              P.zofs.as<int64_t>(), pan, X, n, zbuf, zld);
@@ -598,6 +600,7 @@ void solve_multi_nr(const Plan &P, const Numeric &F, const T *pan, double *X,
              fwd_m_smem_doubles<NR>() * sizeof(double), s,
              P.fwd_item.as<SolveItem>() + L.fwd_map0, pan, lvt, P.gp.as<int64_t>(),
              P.gsrc.as<int64_t>(), X, zbuf, zld, sync + 2 * t, ready, err);
+    if (both) ws.side.join(s);
   }
   if (phases & kDiagonal)
     launch(k_dscale_m, static_cast<unsigned>((n * NR + 255) / 256), 256, 0, s, n, NR,
@@ -608,10 +611,12 @@ void solve_multi_nr(const Plan &P, const Numeric &F, const T *pan, double *X,
   kt.begin(kKcSolveBwd, s);
   if (block) launch(k_mark_pending_m, nmark, 256, 0, s, nready, ready);
   for (int t = nl - 1; t >= 0; t--) {
-    const LevelPlan &L = P.levels[t];
+    const LevelPlan &L    = P.levels[t];
+    const bool       both = L.sw_count > 0 && L.sf_count > 0;
+    cudaStream_t     ss   = both ? ws.side.fork(s) : s;
     if (L.sw_count > 0)
       launch(k_bwd_small_m<NR, T>, (L.sw_count + kSmallWarpsM - 1) / kSmallWarpsM, 32 * kSmallWarpsM,
-             small_smem, s, P.swarp_list.as<int32_t>() + L.sw_begin, L.sw_count,
+             small_smem, ss, P.swarp_list.as<int32_t>() + L.sw_begin, L.sw_count,
              P.sfirst.as<int64_t>(), P.srowptr.as<int64_t>(), P.srows.as<int32_t>(),
              P.slofs.as<int64_t>(), pan, X, n);
     if (L.sf_count > 0) {
@@ -625,6 +630,7 @@ void solve_multi_nr(const Plan &P, const Numeric &F, const T *pan, double *X,
              static_cast<const double *>(ws.part.as<double>()), pld, sync + 2 * t + 1, ready,
              err);
     }
+    if (both) ws.side.join(s);
   }
   kt.end(s);
   MPIR_CHECK_LAUNCH();
