@@ -883,7 +883,7 @@ def run_stream(args):
                      "worker_seconds": {k: round(stats[k + "_ms"] / 1e3, 2)
                                         for k in ("analysis", "plan", "factor", "solve",
                                                   "factor_device", "solve_device",
-                                                  "setup", "trim")}},
+                                                  "setup", "trim", "plan_upload")}},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
                 "d2h_bytes_per_step": d2h / args.steps,
                 "note": "the served arm is itself end to end: host arrays in through "

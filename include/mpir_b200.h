@@ -416,6 +416,7 @@ typedef struct mpir_server_stats {
   double setup_ms, trim_ms;  /* parts of factor_ms: a new factor's solver and
                                 resident buffers; the release of its
                                 factorization scratch afterwards */
+  double plan_upload_ms;     /* part of plan_ms: plans' arrays to the device */
 } mpir_server_stats;
 
 int mpir_server_create(mpir_server *out, const mpir_server_config *cfg);

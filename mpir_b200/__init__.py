@@ -94,7 +94,7 @@ class ServerStats(C.Structure):
         "queued", "bytes_in_use", "peak_bytes", "analysis_reuses", "plan_uploads")] + [
         (k, C.c_double) for k in ("analysis_ms", "plan_ms", "factor_ms", "solve_ms",
                                   "factor_device_ms", "solve_device_ms", "setup_ms",
-                                  "trim_ms")]
+                                  "trim_ms", "plan_upload_ms")]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

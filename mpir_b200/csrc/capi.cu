@@ -1085,6 +1085,7 @@ int mpir_server_get_stats(mpir_server s, mpir_server_stats *out) {
     out->solve_device_ms   = st.solve_device_ms;
     out->setup_ms          = st.setup_ms;
     out->trim_ms           = st.trim_ms;
+    out->plan_upload_ms    = st.plan_upload_ms;
     return MPIR_OK;
   });
 }

@@ -156,7 +156,8 @@ class Plan {
   // Frees the device arrays (the host arrays stay) / uploads them again.
   void release_device();
   void upload_all(cudaStream_t s);
-  bool on_device = false;
+  bool   on_device = false;
+  double upload_ms = 0;  // host wall time of the last upload_all
   // Host copies of the launch and solve tables that build() computes.
   struct HostArrays {
     std::vector<StepDesc>   descs;

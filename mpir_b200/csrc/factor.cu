@@ -16,6 +16,7 @@
 //     C -= (L D) L^T.
 // D is left on each panel's diagonal and copied to D / Dinv (permuted order).
 #include <atomic>
+#include <chrono>
 
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -1252,6 +1253,7 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
 }
 
 void Plan::upload_all(cudaStream_t s) {
+  const auto t0 = std::chrono::steady_clock::now();
   amap       = upload(S.amap, s);
   arow       = upload(S.arow, s);
   acol       = upload(S.acol, s);
@@ -1286,6 +1288,7 @@ void Plan::upload_all(cudaStream_t s) {
   chunk_map    = upload(host_.chunk_map, s);
   own_item     = upload(host_.own_item, s);
   MPIR_CUDA(cudaStreamSynchronize(s));
+  upload_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   on_device = true;
 }
 

@@ -286,6 +286,7 @@ struct Server::Impl {
           used += p.bytes;
           st.plan_uploads++;
           st.plan_ms += 1e3 * (p.last - tu);
+          st.plan_upload_ms += plan->upload_ms;
           st.peak_bytes = std::max<int64_t>(st.peak_bytes, used);
         }
       }
@@ -351,6 +352,7 @@ struct Server::Impl {
         if (cached) st.analysis_reuses++;
         st.analysis_ms += 1e3 * (tb - ta);
         st.plan_ms += 1e3 * (p.last - tb);
+        st.plan_upload_ms += plan->upload_ms;
         st.peak_bytes = std::max<int64_t>(st.peak_bytes, used);
       } else {
         std::lock_guard<std::mutex> lk(mu);

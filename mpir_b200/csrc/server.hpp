@@ -60,6 +60,8 @@ struct ServerStats {
   // Parts of factor_ms: a new factor's setup (solver, resident buffers) and
   // the release of its factorization scratch afterwards.
   double setup_ms = 0, trim_ms = 0;
+  // Part of plan_ms: copying plans' arrays to the device (builds and uploads).
+  double plan_upload_ms = 0;
 };
 
 class Server {
