@@ -784,6 +784,17 @@ def stream_workload(args, nreq):
             f"10% new pattern; {args.budget_gb:.0f} GB admission budget; bwd err <= 1e-14")
 
 
+def failure_summary(recs):
+    """Failed requests by status and message (count, first request index)."""
+    out = {}
+    for r in recs:
+        if r["status"] != 0:
+            key = f'{r["status"]}: {r.get("message", "")[:120]}'
+            c = out.setdefault(key, {"count": 0, "first": r["index"], "n": r["n"]})
+            c["count"] += 1
+    return out
+
+
 def run_stream(args):
     """The serving stream: the engine against the one-at-a-time drop-in."""
     import torch
@@ -838,7 +849,8 @@ def run_stream(args):
         drop = {"solves_per_s": d_completed / d_seconds, "p50_ms": dsum["p50_ms"],
                 "p99_ms": dsum["p99_ms"], "factor": "f32", "completed": dsum["completed"],
                 "failed": dsum["failed"], "backward_error_max": dsum["backward_error_max"],
-                "forward_error_max": dsum["forward_error_max"]}
+                "forward_error_max": dsum["forward_error_max"],
+                "failures": failure_summary(drecs)}
         if lat_pass:
             # the same service times under the half-capacity arrivals
             t_done, lat = 0.0, []
@@ -875,6 +887,7 @@ def run_stream(args):
         "forward_error_max": summ["forward_error_max"],
         "requests": {"completed": summ["completed"], "failed": summ["failed"],
                      "refused_over_budget": stats["refused"],
+                     "failures": failure_summary(recs),
                      "paths": {p: sum(1 for r in ok if r["path"] == p) for p in (0, 1, 2)},
                      "batched_rhs": stats["batched_rhs"], "evictions": stats["evictions"],
                      "peak_gb": stats["peak_bytes"] / 1e9,
