@@ -110,11 +110,12 @@ struct Server::Impl {
     }
   }
 
-  // The oldest request that can run now, except that one whose pattern needs
-  // its plan (an unknown or evicted pattern) goes first: its host analysis
-  // or upload is the start of the longest chain of work in the queue
-  // (analysis, factorization, solves), and every queued request on that
-  // pattern waits for it.
+  // The oldest request that can run now, except that one on a pattern not
+  // seen before goes first: its host analysis is the start of the longest
+  // chain of work in the queue (analysis, factorization, solves), and every
+  // queued request on that pattern waits for it.  (A pattern whose plan was
+  // evicted keeps its place: preferring those too re-uploaded plans that
+  // evicted others, whose requests were then preferred in turn.)
   bool pick(Job &job) {
     auto choice = queue.end();
     for (int pass = 0; pass < 2 && choice == queue.end(); pass++)
@@ -123,7 +124,7 @@ struct Server::Impl {
         if (p != patterns.end() && p->second.busy) continue;  // being analysed
         auto f = factors.find(FKey{it->pattern_key, it->values_key});
         if (f != factors.end() && f->second.busy) continue;   // in use
-        if (pass == 0 && p != patterns.end() && p->second.resident) continue;
+        if (pass == 0 && p != patterns.end()) continue;
         choice = it;
         break;
       }
