@@ -356,8 +356,9 @@ int mpir_group_destroy(mpir_group g);
  * GmresLDLIR::Compute + Solve, gmres_ir.hpp:323 and :534-634) served on one
  * GPU by worker threads with a stream each.  Requests name their pattern and
  * values by caller-chosen keys; the engine keeps analysed patterns and
- * factors resident (least recently used evicted first when a new factor
- * does not fit the device-memory budget), solves the queued requests on one
+ * factors resident (when a new factor does not fit the device-memory
+ * budget it evicts first what no queued request names, least recently used
+ * first, then what the queue needs last), solves the queued requests on one
  * factor together (up to max_batch right-hand sides in lockstep, as
  * mpir_solver_solve_batch), and runs requests on different factors
  * concurrently.  A request whose factor alone exceeds the budget, or that

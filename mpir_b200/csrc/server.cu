@@ -157,16 +157,40 @@ struct Server::Impl {
   }
 
   // Frees room for `need` bytes by evicting idle factors, then idle plans
-  // without factors, least recently used first.  Returns false when it cannot
-  // (the evicted solvers are handed back to be destroyed outside the lock).
+  // without factors.  The victim is the one whose next use in the queue is
+  // furthest away: first those no queued request names (least recently used
+  // among them), then the rest by the position of their first queued
+  // request.  Returns false when it cannot (the evicted solvers are handed
+  // back to be destroyed outside the lock).
   bool make_room(size_t need, std::vector<std::unique_ptr<Solver>> &graveyard,
                  std::vector<std::shared_ptr<Plan>> &plan_graveyard) {
+    if (used + need <= static_cast<size_t>(cfg.budget_bytes)) return true;
+    constexpr size_t                none = static_cast<size_t>(-1);
+    std::map<FKey, size_t>          next_f;
+    std::map<uint64_t, size_t>      next_p;
+    size_t                          pos = 0;
+    for (const ServerRequest &q : queue) {
+      next_f.emplace(FKey{q.pattern_key, q.values_key}, pos);
+      next_p.emplace(q.pattern_key, pos);
+      pos++;
+    }
+    auto later = [none](size_t a, double la, size_t b, double lb) {
+      // true when a use at a (last used at la) should be evicted before b
+      if (a != b) return a == none || (b != none && a > b);
+      return la < lb;
+    };
     while (used + need > static_cast<size_t>(cfg.budget_bytes)) {
-      auto victim = factors.end();
-      for (auto it = factors.begin(); it != factors.end(); ++it)
-        if (!it->second.busy && it->second.solver &&
-            (victim == factors.end() || it->second.last < victim->second.last))
+      auto   victim = factors.end();
+      size_t vnext  = 0;
+      for (auto it = factors.begin(); it != factors.end(); ++it) {
+        if (it->second.busy || !it->second.solver) continue;
+        const auto   nf = next_f.find(it->first);
+        const size_t nx = nf == next_f.end() ? none : nf->second;
+        if (victim == factors.end() || later(nx, it->second.last, vnext, victim->second.last)) {
           victim = it;
+          vnext  = nx;
+        }
+      }
       if (victim != factors.end()) {
         used -= victim->second.bytes;
         auto p = patterns.find(victim->first.first);
@@ -176,13 +200,20 @@ struct Server::Impl {
         st.evictions++;
         continue;
       }
-      auto pv = patterns.end();
+      auto   pv     = patterns.end();
+      size_t pvnext = 0;
       for (auto it = patterns.begin(); it != patterns.end(); ++it) {
         if (it->second.busy || it->second.factors != 0 || !it->second.resident) continue;
         bool referenced = false;  // by the placeholder factor of a running job
         for (auto &f : factors)
           if (f.first.first == it->first) referenced = true;
-        if (!referenced && (pv == patterns.end() || it->second.last < pv->second.last)) pv = it;
+        if (referenced) continue;
+        const auto   np = next_p.find(it->first);
+        const size_t nx = np == next_p.end() ? none : np->second;
+        if (pv == patterns.end() || later(nx, it->second.last, pvnext, pv->second.last)) {
+          pv     = it;
+          pvnext = nx;
+        }
       }
       if (pv == patterns.end()) return false;
       // The plan leaves the device; its host side (analysis and tables)

@@ -6,8 +6,9 @@
   solutions within 20x of the solo forward error.
 * Requests on one factor queued together are solved in lockstep batches.
 * Admission: a factor larger than the budget is refused with status -4
-  (MPIR_ERR_NOMEM); a budget that holds only a few factors evicts the least
-  recently used ones and still answers every request correctly."""
+  (MPIR_ERR_NOMEM); a budget that holds only a few factors evicts (with
+  nothing queued behind a request: the least recently used first) and still
+  answers every request correctly."""
 import numpy as np
 import pytest
 
