@@ -890,6 +890,10 @@ def run_stream(args):
                      "failures": failure_summary(recs),
                      "paths": {p: sum(1 for r in ok if r["path"] == p) for p in (0, 1, 2)},
                      "batched_rhs": stats["batched_rhs"], "evictions": stats["evictions"],
+                     "jobs": {k: stats[k] for k in ("analyses", "factorizations", "solves",
+                                                    "batched_solves")},
+                     "distinct_factors": len({(r.pattern_key, r.values_key)
+                                              for r in st.requests}),
                      "peak_gb": stats["peak_bytes"] / 1e9,
                      "plans_rebuilt_from_kept_analysis": stats["analysis_reuses"],
                      "plans_uploaded_again": stats["plan_uploads"],
