@@ -48,6 +48,8 @@ import time
 
 import numpy as np
 
+T_START = time.perf_counter()
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -385,6 +387,11 @@ def reference_line(args, value, cores, kind_sample, detail, workload, lat_ms=Non
     if lat_ms is not None:
         line["latency_ms"] = {"p50": float(np.percentile(lat_ms, 50)),
                               "p99": float(np.percentile(lat_ms, 99))}
+    # Whether value and ms_per_step were timed in full in this run, or
+    # extrapolated from timed samples (then ms_per_step is the model's, not
+    # this run's wall clock, which is given beside it).
+    line["measured"] = not bool(isinstance(detail, dict) and detail.get("extrapolated"))
+    line["wall_seconds"] = time.perf_counter() - T_START
     return line
 
 
