@@ -272,7 +272,7 @@ void Solver::precond_gmres(const double *b, double *res, Report &st) {
 
   std::vector<double> H((m + 1) * std::max<int64_t>(m, 1), 0.0), g(m + 1, 0.0),
       c(std::max<int64_t>(m, 1), 0.0), sn(std::max<int64_t>(m, 1), 0.0),
-      col(m + 2, 0.0);
+      col(m + 3, 0.0);
   auto h = [&](int64_t i, int64_t j) -> double & { return H[i * std::max<int64_t>(m, 1) + j]; };
   g[0] = rho;
   int64_t k;
@@ -288,9 +288,9 @@ void Solver::precond_gmres(const double *b, double *res, Report &st) {
     for (int64_t j = 0; j <= k; j++)
       vec_.mgs_pass(w, V + j * n, hd + j, j < k ? V + (j + 1) * n : nullptr, j < k ? 0 : 1,
                     hd + j + 1, s);
-    read(col.data(), 0, static_cast<int>(k + 2));
-    double normav;
-    read(&normav, static_cast<int>(m + 2), 1);
+    // The column's k + 2 entries and normav (at m + 2) in one copy.
+    read(col.data(), 0, static_cast<int>(m + 3));
+    const double normav = col[m + 2];
     for (int64_t j = 0; j <= k + 1; j++) h(j, k) = col[j];
     const double normav2 = h(k + 1, k);
     if (normav + 0.001 * normav2 == normav) {  // Brown/Hindmarsh, gmres_ir.hpp:683
