@@ -943,10 +943,21 @@ def run_stream(args):
         try:
             from mpir_b200 import kkt
             s48 = kkt.grid3d(seed=0)
-            perm = mp.analyze_host(s48.Ap, s48.Ai, s48.Ax)["perm"]
+            # The GPU factor of the system the CPU sample factors: parity of
+            # the leading rows against the reference's QDLDL_factor<float>.
+            g48 = mp.GmresLDLIR(device=local)
+            g48.Compute(s48.Ap, s48.Ai, s48.Ax)
+            perm = g48.symbolic()["perm"]
             counts = {"applies": 11, "spmv": 13}
             _, det = reference_cpu_estimate(s48, perm, counts, args.cpu_budget,
-                                            log=lambda *a: print(*a, file=sys.stderr))
+                                            log=lambda *a: print(*a, file=sys.stderr),
+                                            keep_factor=True)
+            line["parity"] = dict(leading_parity(g48, det),
+                                  system="grid3d-48, n = 138,240: the system the CPU "
+                                         "baseline samples")
+            g48.close()
+            det.pop("factor")
+            det.pop("factor64", None)
             import oracle
             R = oracle.Reference()
             x = np.ones(s48.n)
