@@ -78,7 +78,7 @@ def parse():
     ap.add_argument("--ir-iter", type=int, default=None)
     # serving stream
     ap.add_argument("--requests-per-step", type=int, default=8)
-    ap.add_argument("--workers", type=int, default=8)
+    ap.add_argument("--workers", type=int, default=4)
     ap.add_argument("--budget-gb", type=float, default=150.0)
     ap.add_argument("--no-latency-pass", action="store_true")
     ap.add_argument("--no-dropin", action="store_true")
