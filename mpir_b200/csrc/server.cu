@@ -11,12 +11,13 @@
 //             ordering and symbolic analysis) and its plan uploaded once;
 //   factors   a factor is kept per (pattern, values) while memory allows:
 //             a request on a resident factor is only a solve, one with new
-//             values on a known pattern a refactorization (replayed from the
-//             pattern's captured graph) and a solve;
+//             values on a known pattern a refactorization from the pattern's
+//             plan, and a solve;
 //   admission every plan and factor is charged its device bytes against the
-//             budget; a factor that does not fit evicts the least recently
-//             used idle factors (then idle plans) first (freed before the
-//             job waits or tries again), and a request whose footprint
+//             budget; a factor that does not fit evicts idle factors (then
+//             idle plans): those no queued request names first, least
+//             recently used first, then those the queue needs last (freed
+//             before the job waits or tries again), and a request whose
 //             exceeds the whole budget, or that finds no room while no other
 //             job runs on or within two minutes, is refused with
 //             MPIR_ERR_NOMEM;
