@@ -22,6 +22,23 @@
 
 namespace mpir {
 
+size_t Solver::batch_growth(int width) const {
+  if (!plan_ || width <= 1) return 0;
+  const int64_t n = std::max<int64_t>(plan_->S.n, 1);
+  const int64_t m = std::max<int64_t>(std::min(gmres_iter, n), 1);
+  if (bw_ == width && bm_ == m) return 0;
+  const size_t want = MultiSolveWorkspace::bytes_for(*plan_, width) +
+                      static_cast<size_t>(m + 1 + 8) * n * width * sizeof(double) +
+                      2048 * width * sizeof(double);
+  size_t have = 0;
+  for (const DeviceBuffer *d : {&bV_, &bbs_, &bbp_, &bx_, &br_, &bt_, &bd_, &bhd_, &by_, &bfac_,
+                                &bact_, &bkq_, &bin_, &bout_, &bpre_, &mws_.zbuf, &mws_.part,
+                                &mws_.sync, &mws_.ready, &mws_.err, &mws_.xbuf, &vecb_.part,
+                                &vecb_.count, &vecb_.infbits})
+    have += d->bytes();
+  return want > have ? want - have : 0;
+}
+
 void Solver::ensure_batch(int width) {
   ensure_vectors();
   const int64_t n = plan_->S.n, m = std::max<int64_t>(std::min(gmres_iter, n), 1);

@@ -479,8 +479,23 @@ struct Server::Impl {
           return;
         }
       } else {
-        std::lock_guard<std::mutex> lk(mu);
-        sv = factors.at(k).solver.get();
+        {
+          // A lockstep batch wider than the factor's buffers grows them:
+          // that growth is charged (and room made for it) before the solve.
+          std::lock_guard<std::mutex> lk(mu);
+          sv = factors.at(k).solver.get();
+          if (job.reqs.size() > 1) {
+            const size_t grow = sv->batch_growth(multi_width(static_cast<int>(job.reqs.size())));
+            if (grow > 0) {
+              make_room(grow, graveyard, plan_graveyard);  // best effort
+              used += grow;
+              reserved = grow;
+              st.peak_bytes = std::max<int64_t>(st.peak_bytes, used);
+            }
+          }
+        }
+        graveyard.clear();
+        release_plans(plan_graveyard);
       }
       // Solve the batch: one request alone, several in lockstep.
       const double  ts = now_s();
@@ -502,9 +517,10 @@ struct Server::Impl {
       {
         std::lock_guard<std::mutex> lk(mu);
         Factor &f = factors[k];
-        // the batch buffers may have grown
+        // the batch buffers may have grown (their growth was reserved)
         const size_t b = f.solver->device_bytes();
-        used           = used - f.bytes + b;
+        used           = used - f.bytes - reserved + b;
+        reserved       = 0;
         f.bytes        = b;
         f.last         = now_s();
         patterns[r.pattern_key].last = f.last;

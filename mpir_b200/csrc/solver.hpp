@@ -76,6 +76,9 @@ class Solver {
   // Device memory this solver holds beyond its plan, and what adopt() plus
   // one batch of `width` right-hand sides would take for plan P.
   size_t device_bytes() const;
+  // Device bytes that solving `width` right-hand sides in lockstep would add
+  // to what this solver holds (0 if its batch buffers already fit).
+  size_t batch_growth(int width) const;
   static size_t bytes_for(const Plan &P, int64_t gmres_iter, int width, int uf = kF32);
   int factor(const double *Ax);
   int solve(const double *b, double *x, Report *rep);
