@@ -150,7 +150,10 @@ class Plan {
   std::vector<int64_t> pk_ofs, pd_ofs;
   int64_t              pk_elems = 0, pd_elems = 0;
 
-  void build(Symbolic &&sym, cudaStream_t s);
+  // The host tables and, unless upload is false, their device copies.
+  void build(Symbolic &&sym, cudaStream_t s, bool upload = true);
+  // Device bytes upload_all() takes.
+  size_t upload_bytes() const;
   // Device memory the plan holds.
   size_t device_bytes() const;
   // Frees the device arrays (the host arrays stay) / uploads them again.

@@ -874,7 +874,7 @@ void invert_diag_blocks(const Plan &P, Numeric &F, cudaStream_t s) {
 // ---------------------------------------------------------------------------
 // Plan construction.
 
-void Plan::build(Symbolic &&sym, cudaStream_t s) {
+void Plan::build(Symbolic &&sym, cudaStream_t s, bool upload) {
   S              = std::move(sym);
   const int64_t ns = S.ns;
   nnz_full         = static_cast<int64_t>(S.Kj.size());
@@ -1249,7 +1249,17 @@ void Plan::build(Symbolic &&sym, cudaStream_t s) {
   host_.fwd_item    = std::move(fwd_item_h);
   host_.chunk_map   = std::move(chunk_map_h);
   host_.own_item    = std::move(own_item_h);
-  upload_all(s);
+  if (upload) upload_all(s);
+}
+
+size_t Plan::upload_bytes() const {
+  auto b = [](const auto &v) { return v.size() * sizeof(v[0]); };
+  return b(S.amap) + b(S.arow) + b(S.acol) + b(S.diag_pos) + b(S.Kp) + b(S.Kj) + b(S.Ksrc) +
+         b(S.sfirst) + b(S.srowptr) + b(S.srows) + b(S.srel) + b(S.slofs) + b(S.uofs) +
+         b(S.zofs) + b(S.child_ptr) + b(S.child_list) + b(S.perm) + b(h_small) + b(h_large) +
+         b(host_.descs) + b(host_.tasks) + b(host_.chunks) + b(host_.hits) + b(host_.probs) +
+         b(linv_ofs) + b(host_.sfronts) + b(h_swarp) + b(h_sblock) + b(host_.gp) +
+         b(host_.gsrc) + b(host_.fwd_item) + b(host_.chunk_map) + b(host_.own_item);
 }
 
 void Plan::upload_all(cudaStream_t s) {

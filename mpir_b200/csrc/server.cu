@@ -230,6 +230,40 @@ struct Server::Impl {
     return true;
   }
 
+  // Charges `need` bytes once they fit the budget (lk held on entry and on
+  // return): evicts as make_room does, frees what it evicted before waiting
+  // or trying again, and waits while other jobs run on.  Returns "" when
+  // admitted, else why the job is refused (no other job runs on that could
+  // free memory, or the wait passed kAdmitWaitSeconds).
+  std::string admit(size_t need, std::unique_lock<std::mutex> &lk,
+                    std::vector<std::unique_ptr<Solver>> &graveyard,
+                    std::vector<std::shared_ptr<Plan>> &plan_graveyard) {
+    const double t_wait = now_s();
+    for (;;) {
+      if (make_room(need, graveyard, plan_graveyard)) {
+        used += need;
+        st.peak_bytes = std::max<int64_t>(st.peak_bytes, used);
+        return "";
+      }
+      if (!graveyard.empty() || !plan_graveyard.empty()) {
+        // What was evicted leaves the device before this job waits or tries
+        // again (the budget already counts it as free).
+        lk.unlock();
+        graveyard.clear();
+        release_plans(plan_graveyard);
+        lk.lock();
+        continue;
+      }
+      // Memory comes free only from jobs that run on: none other than those
+      // waiting for room themselves (or the wait ran too long).
+      if (running - waiting_room <= 1) return "admission budget held by resident plans";
+      if (now_s() - t_wait > kAdmitWaitSeconds) return "admission wait exceeded";
+      waiting_room++;
+      cv_done.wait_for(lk, std::chrono::milliseconds(20));
+      waiting_room--;
+    }
+  }
+
   // ---- work (outside mu) ------------------------------------------------------
   // Frees the device arrays of plans evicted by make_room and clears their
   // patterns' busy flags.
@@ -284,6 +318,40 @@ struct Server::Impl {
     auto fail_all = [&](int code, const std::string &msg) {
       for (const ServerRequest &q : job.reqs) finish(q, code, path, 1, t0, Report{}, msg);
     };
+    // A plan's device arrays are admitted like a factor before they are
+    // uploaded (fresh: the pattern was not known before this job).
+    auto load_plan = [&](const std::shared_ptr<Plan> &pl, bool fresh) -> bool {
+      const size_t pb = pl->upload_bytes();
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        const std::string why = admit(pb, lk, graveyard, plan_graveyard);
+        if (!why.empty()) {
+          if (fresh)
+            patterns.erase(r.pattern_key);
+          else
+            patterns[r.pattern_key].busy = false;
+          factors.erase(k);
+          lk.unlock();
+          fail_all(-4, why);
+          std::lock_guard<std::mutex> lk2(mu);
+          st.refused += static_cast<int64_t>(job.reqs.size());
+          return false;
+        }
+        reserved = pb;
+      }
+      graveyard.clear();
+      release_plans(plan_graveyard);
+      cudaStream_t s = nullptr;
+      MPIR_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+      try {
+        pl->upload_all(s);
+      } catch (...) {
+        cudaStreamDestroy(s);
+        throw;
+      }
+      cudaStreamDestroy(s);
+      return true;
+    };
     try {
       MPIR_CUDA(cudaSetDevice(cfg.device));
       if (job.kind == Job::kAnalyse) {
@@ -299,24 +367,16 @@ struct Server::Impl {
         }
         if (kept) {
           const double tu = now_s();
-          cudaStream_t s  = nullptr;
-          MPIR_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-          try {
-            kept->upload_all(s);
-          } catch (...) {
-            cudaStreamDestroy(s);
-            throw;
-          }
-          cudaStreamDestroy(s);
+          if (!load_plan(kept, false)) return;
           plan = kept;
           std::lock_guard<std::mutex> lk(mu);
-          make_room(plan->device_bytes(), graveyard, plan_graveyard);  // best effort
           Pattern &p = patterns[r.pattern_key];
           p.busy     = false;
           p.resident = true;
           p.bytes    = plan->device_bytes();
           p.last     = now_s();
-          used += p.bytes;
+          used       = used - reserved + p.bytes;
+          reserved   = 0;
           st.plan_uploads++;
           st.plan_ms += 1e3 * (p.last - tu);
           st.plan_upload_ms += plan->upload_ms;
@@ -360,27 +420,18 @@ struct Server::Impl {
           return;
         }
         plan = std::make_shared<Plan>();
-        {
-          cudaStream_t s = nullptr;
-          MPIR_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-          try {
-            plan->build(std::move(S), s);
-          } catch (...) {
-            cudaStreamDestroy(s);
-            throw;
-          }
-          cudaStreamDestroy(s);
-        }
+        plan->build(std::move(S), nullptr, false);  // host tables; uploaded once admitted
+        if (!load_plan(plan, true)) return;
         std::lock_guard<std::mutex> lk(mu);
         const size_t pb = plan->device_bytes();
-        make_room(pb, graveyard, plan_graveyard);  // best effort: plans are small
         Pattern &p = patterns[r.pattern_key];
         p.plan     = plan;
         p.busy     = false;
         p.resident = true;
         p.bytes    = pb;
         p.last     = now_s();
-        used += p.bytes;
+        used       = used - reserved + pb;
+        reserved   = 0;
         st.analyses++;
         if (cached) st.analysis_reuses++;
         st.analysis_ms += 1e3 * (tb - ta);
@@ -405,37 +456,16 @@ struct Server::Impl {
             st.refused += static_cast<int64_t>(job.reqs.size());
             return;
           }
-          const double t_wait = now_s();
-          for (;;) {
-            if (make_room(need, graveyard, plan_graveyard)) break;
-            if (!graveyard.empty() || !plan_graveyard.empty()) {
-              // What was evicted leaves the device before this job waits or
-              // tries again (the budget already counts it as free).
-              lk.unlock();
-              graveyard.clear();
-              release_plans(plan_graveyard);
-              lk.lock();
-              continue;
-            }
-            // Memory comes free only from jobs that run on: none other than
-            // those waiting for room themselves (or the wait ran too long).
-            const bool none_active = running - waiting_room <= 1;
-            if (none_active || now_s() - t_wait > kAdmitWaitSeconds) {
-              factors.erase(k);
-              lk.unlock();
-              fail_all(-4, none_active ? "admission budget held by resident plans"
-                                       : "admission wait exceeded");
-              std::lock_guard<std::mutex> lk2(mu);
-              st.refused += static_cast<int64_t>(job.reqs.size());
-              return;
-            }
-            waiting_room++;
-            cv_done.wait_for(lk, std::chrono::milliseconds(20));
-            waiting_room--;
+          const std::string why = admit(need, lk, graveyard, plan_graveyard);
+          if (!why.empty()) {
+            factors.erase(k);
+            lk.unlock();
+            fail_all(-4, why);
+            std::lock_guard<std::mutex> lk2(mu);
+            st.refused += static_cast<int64_t>(job.reqs.size());
+            return;
           }
-          used += need;  // reserved; corrected to the measured bytes below
-          reserved = need;
-          st.peak_bytes = std::max<int64_t>(st.peak_bytes, used);
+          reserved = need;  // charged; corrected to the measured bytes below
         }
         graveyard.clear();
         release_plans(plan_graveyard);
@@ -481,16 +511,22 @@ struct Server::Impl {
       } else {
         {
           // A lockstep batch wider than the factor's buffers grows them:
-          // that growth is charged (and room made for it) before the solve.
-          std::lock_guard<std::mutex> lk(mu);
+          // that growth is admitted like a factor before the solve.
+          std::unique_lock<std::mutex> lk(mu);
           sv = factors.at(k).solver.get();
           if (job.reqs.size() > 1) {
             const size_t grow = sv->batch_growth(multi_width(static_cast<int>(job.reqs.size())));
             if (grow > 0) {
-              make_room(grow, graveyard, plan_graveyard);  // best effort
-              used += grow;
+              const std::string why = admit(grow, lk, graveyard, plan_graveyard);
+              if (!why.empty()) {
+                factors.at(k).busy = false;
+                lk.unlock();
+                fail_all(-4, why);
+                std::lock_guard<std::mutex> lk2(mu);
+                st.refused += static_cast<int64_t>(job.reqs.size());
+                return;
+              }
               reserved = grow;
-              st.peak_bytes = std::max<int64_t>(st.peak_bytes, used);
             }
           }
         }
