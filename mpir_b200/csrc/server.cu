@@ -13,8 +13,9 @@
 //             a request on a resident factor is only a solve, one with new
 //             values on a known pattern a refactorization from the pattern's
 //             plan, and a solve;
-//   admission every plan and factor is charged its device bytes against the
-//             budget; a factor that does not fit evicts idle factors (then
+//   admission every plan, factor and batch-buffer growth is charged its
+//             device bytes against the budget before it reaches the device;
+//             what does not fit evicts idle factors (then
 //             idle plans): those no queued request names first, least
 //             recently used first, then those the queue needs last (freed
 //             before the job waits or tries again), and a request whose
