@@ -308,7 +308,7 @@ struct Server::Impl {
     Solver                    *sv = nullptr;
     std::vector<std::unique_ptr<Solver>> graveyard;
     std::vector<std::shared_ptr<Plan>>   plan_graveyard;
-    size_t                               reserved = 0;  // admitted bytes not yet a factor's
+    size_t                               reserved = 0;  // admitted bytes not yet counted as a plan's or factor's
     // Plans evicted on this job's behalf leave the device however the job
     // ends (after every lock of this function is released).
     struct ReleaseAtExit {
