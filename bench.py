@@ -817,7 +817,7 @@ def run_stream(args):
     gmres_iter = args.gmres_iter or (30 if low else 10)
     nreq = args.requests_per_step * args.steps
     srv_kw = dict(uf=uf, workers=args.workers, max_batch=16, update=args.update or "default",
-                  budget_bytes=int(args.budget_gb * (1 << 30)), ir_iter=ir_iter,
+                  budget_bytes=int(args.budget_gb * 1e9), ir_iter=ir_iter,
                   gmres_iter=gmres_iter, tol=1e-10, device=local)
     st = smod.Stream(nreq, rate=1e4, seed=replica_seed(args.seed, rank))
     arrays = replay.materialise(st)
@@ -902,6 +902,7 @@ def run_stream(args):
                      "distinct_factors": len({(r.pattern_key, r.values_key)
                                               for r in st.requests}),
                      "peak_gb": stats["peak_bytes"] / 1e9,
+                     "budget_gb": args.budget_gb,
                      "plans_rebuilt_from_kept_analysis": stats["analysis_reuses"],
                      "plans_uploaded_again": stats["plan_uploads"],
                      "worker_seconds": {k: round(stats[k + "_ms"] / 1e3, 2)

@@ -572,7 +572,7 @@ class Server:
     returns an id at once; ``wait`` returns that request's solution and
     result.  Arrays are kept referenced until the request is done."""
 
-    def __init__(self, uf="f32", ur="f64", workers=4, max_batch=16, budget_bytes=150 << 30,
+    def __init__(self, uf="f32", ur="f64", workers=4, max_batch=16, budget_bytes=150 * 10 ** 9,
                  ir_iter=10, gmres_iter=10, tol=1e-10, device=0, update="default"):
         cfg = ServerConfig(device=device, uf=_PREC[uf], ur=_PREC[ur], workers=workers,
                            max_batch=max_batch, update=UPDATE[update],

@@ -14,8 +14,9 @@
 //             values on a known pattern a refactorization from the pattern's
 //             plan, and a solve;
 //   admission every plan, factor and batch-buffer growth is charged its
-//             device bytes against the budget before it reaches the device;
-//             what does not fit evicts idle factors (then
+//             device bytes against the budget before it reaches the device
+//             (plans and batch growth best effort, factors strictly); what
+//             does not fit evicts idle factors (then
 //             idle plans): those no queued request names first, least
 //             recently used first, then those the queue needs last (freed
 //             before the job waits or tries again), and a request whose
@@ -319,26 +320,18 @@ struct Server::Impl {
     auto fail_all = [&](int code, const std::string &msg) {
       for (const ServerRequest &q : job.reqs) finish(q, code, path, 1, t0, Report{}, msg);
     };
-    // A plan's device arrays are admitted like a factor before they are
-    // uploaded (fresh: the pattern was not known before this job).
-    auto load_plan = [&](const std::shared_ptr<Plan> &pl, bool fresh) -> bool {
+    // A plan's device arrays are charged before they are uploaded, after
+    // evicting what makes room for them if anything can go (best effort: a
+    // plan is small, and waiting for room here would hold every queued
+    // request on its pattern).
+    auto load_plan = [&](const std::shared_ptr<Plan> &pl) -> bool {
       const size_t pb = pl->upload_bytes();
       {
-        std::unique_lock<std::mutex> lk(mu);
-        const std::string why = admit(pb, lk, graveyard, plan_graveyard);
-        if (!why.empty()) {
-          if (fresh)
-            patterns.erase(r.pattern_key);
-          else
-            patterns[r.pattern_key].busy = false;
-          factors.erase(k);
-          lk.unlock();
-          fail_all(-4, why);
-          std::lock_guard<std::mutex> lk2(mu);
-          st.refused += static_cast<int64_t>(job.reqs.size());
-          return false;
-        }
-        reserved = pb;
+        std::lock_guard<std::mutex> lk(mu);
+        make_room(pb, graveyard, plan_graveyard);
+        used += pb;
+        reserved      = pb;
+        st.peak_bytes = std::max<int64_t>(st.peak_bytes, used);
       }
       graveyard.clear();
       release_plans(plan_graveyard);
@@ -368,7 +361,7 @@ struct Server::Impl {
         }
         if (kept) {
           const double tu = now_s();
-          if (!load_plan(kept, false)) return;
+          if (!load_plan(kept)) return;
           plan = kept;
           std::lock_guard<std::mutex> lk(mu);
           Pattern &p = patterns[r.pattern_key];
@@ -422,7 +415,7 @@ struct Server::Impl {
         }
         plan = std::make_shared<Plan>();
         plan->build(std::move(S), nullptr, false);  // host tables; uploaded once admitted
-        if (!load_plan(plan, true)) return;
+        if (!load_plan(plan)) return;
         std::lock_guard<std::mutex> lk(mu);
         const size_t pb = plan->device_bytes();
         Pattern &p = patterns[r.pattern_key];
@@ -512,22 +505,17 @@ struct Server::Impl {
       } else {
         {
           // A lockstep batch wider than the factor's buffers grows them:
-          // that growth is admitted like a factor before the solve.
-          std::unique_lock<std::mutex> lk(mu);
+          // that growth is charged before the solve, after evicting what
+          // makes room for it if anything can go (best effort, as plans).
+          std::lock_guard<std::mutex> lk(mu);
           sv = factors.at(k).solver.get();
           if (job.reqs.size() > 1) {
             const size_t grow = sv->batch_growth(multi_width(static_cast<int>(job.reqs.size())));
             if (grow > 0) {
-              const std::string why = admit(grow, lk, graveyard, plan_graveyard);
-              if (!why.empty()) {
-                factors.at(k).busy = false;
-                lk.unlock();
-                fail_all(-4, why);
-                std::lock_guard<std::mutex> lk2(mu);
-                st.refused += static_cast<int64_t>(job.reqs.size());
-                return;
-              }
-              reserved = grow;
+              make_room(grow, graveyard, plan_graveyard);
+              used += grow;
+              reserved      = grow;
+              st.peak_bytes = std::max<int64_t>(st.peak_bytes, used);
             }
           }
         }

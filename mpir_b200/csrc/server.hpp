@@ -15,7 +15,7 @@ struct ServerConfig {
   int     workers    = 4;     // concurrent jobs (host threads, one stream each)
   int     max_batch  = 16;    // right-hand sides solved in lockstep
   int     update     = kUpdateDefault;  // trailing-update engine (float32 factors)
-  int64_t budget_bytes = int64_t{150} << 30;
+  int64_t budget_bytes = int64_t{150} * 1000000000;  // 150 GB
   int64_t max_ir_iterations    = 10;
   int64_t max_gmres_iterations = 10;
   double  tolerance            = 1e-10;
