@@ -10,8 +10,8 @@ configured shapes and value distributions):
            a 2-D or 3-D system with n log-uniform in [1e3, 5e5] and m ~ n1/4,
            60% a new right-hand side on a factor used before, 30% new values
            on a pattern used before, 10% a new pattern; 150 GB admission
-           budget; backward error <= 1e-14.  One step = 16 requests of the
-           stream.  `value` = solves/s of the serving engine
+           budget (150e9 bytes), 4 workers; backward error <= 1e-14.  One
+           step = 8 requests of the stream (--requests-per-step).  `value` = solves/s of the serving engine
            (mpir_server_*) on the stream at a saturating arrival rate;
            `drop_in` = the same requests served one at a time through the
            drop-in GmresLDLIR (Compute + Solve per request, as the
@@ -25,8 +25,9 @@ configured shapes and value distributions):
            delta 1e-4); the reference arm runs its full GMRES-IR here.
   batch2d  64 instances on one 256^2 pattern (H + diag(s), s log-uniform
            in [1e-6, 1e2], 16,384 rows x 4, delta 1e-8), 16 right-hand sides
-           each: one analysis, then per step one instance refactorized and
-           its 16 right-hand sides solved in lockstep.
+           each: one analysis, then per step a group of --group instances
+           refactorized by one graph launch and their 16 right-hand sides
+           each solved in lockstep.
   illcond3d the precision tier: D L3D(grid^3) D + 1e-8 I, D log-uniform in
            [1e-3, 1e3], 8 entries per constraint row, delta 1e-8.
 
