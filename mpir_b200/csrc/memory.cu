@@ -21,7 +21,8 @@
 // would wait for the whole device; an allocation takes the smallest cached
 // block of its device that is at least its size and at most a quarter (plus
 // 2 MiB) larger, else calls cudaMalloc, and one that does not fit first
-// frees the cached blocks.  A refactorization of a pattern seen before finds
+// frees the cached blocks (so does a pool allocation that does not fit, and
+// the serving engine when it is destroyed).  A refactorization of a pattern seen before finds
 // its scratch buffers' sizes there.  MPIR_ALLOC=sync makes cudaMalloc and
 // the cache the default of every thread.
 #include <cstdint>
@@ -156,11 +157,14 @@ void *device_alloc(size_t bytes, DevMem *m) {
   void        *p = nullptr;
   cudaError_t  e = cudaMallocAsync(&p, bytes, s);
   if (e == cudaErrorMemoryAllocation) {
+    // the pool's unused memory and the cache's idle blocks go back to the
+    // device, then one more try
     cudaGetLastError();
     cudaMemPool_t pool;
     MPIR_CUDA(cudaStreamSynchronize(s));
     MPIR_CUDA(cudaDeviceGetDefaultMemPool(&pool, d));
     MPIR_CUDA(cudaMemPoolTrimTo(pool, 0));
+    cache_flush(d);
     e = cudaMallocAsync(&p, bytes, s);
   }
   if (e != cudaSuccess) {

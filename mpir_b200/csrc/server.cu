@@ -624,6 +624,7 @@ Server::~Server() {
   cudaSetDevice(impl_->cfg.device);
   impl_->factors.clear();
   impl_->patterns.clear();
+  device_cache_flush(impl_->cfg.device);  // the workers' idle blocks
 }
 
 int64_t Server::submit(ServerRequest r) {
